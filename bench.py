@@ -1,0 +1,358 @@
+#!/usr/bin/env python
+"""Benchmark of the path-integral Monte Carlo hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--form compensated|plain|fp64]
+
+Workload (the precision form): N = 256 segments, arclength S = 20, source (0,0,0) with
+tangent (0,0,1), receiver (0,0,12) with tangent (0,0,1); Gaussian phase sigma = 0.1
+(config eps = sigma^2 = 0.01), mu_s = 10, regulariser mu = 1, no absorption, 8192-bin
+table from a 20000-step Simpson rule; 2^26 weighted paths per step, sub-chains of
+k ~ U{2..32} segments rotated by U(-0.05, 0.05) rad, Philox seed 1234, 256 unweighted
+burn-in steps per chain. Inputs are synthetic (there is no dataset). One step = one full
+Monte Carlo pass: every chain replays its proposals from the same initial curve.
+
+Metric: path-segments weighted per second = weighted paths x N / time.
+  value  device time of the pass (chain kernel + FP64 reduction), CUDA events on the
+         launching stream, L2 flushed between steps, max over ranks;
+  e2e    the same metric through twisty_run with host buffers (table, initial curve and
+         normaliser setup, host-to-device copies, the pass, the result copy back).
+The JSON line also carries the FP64 error of the estimate, the plain FP32 drop-in's
+throughput on the same workload, the roofline of the chain kernel, and a CPU baseline
+(the reference's own chain loop, compiled from its sources, on this host's cores).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W = dict(N=256, S=20.0, start=(0.0, 0.0, 0.0), sdir=(0.0, 0.0, 1.0), end=(0.0, 0.0, 12.0), edir=(0.0, 0.0, 1.0),
+         sigma=0.1, eps=0.01, scatter=10.0, mu=1.0, absorption=0.0, num_steps_int=20000, bins=8192,
+         paths=2 ** 26, k_max=32, max_angle=0.05, seed=1234, burn_in=256)
+WORKLOAD_NAME = ("precision form: N=256 S=20 x1=(0,0,12) tangents (0,0,1), sigma=0.1 mu_s=10, 8192-bin table, "
+                 "2^26 paths/step, k~U{2..32}, angle~U(-0.05,0.05), Philox seed 1234")
+METRIC = "path-segments weighted/s, 1 B200, chosen vs plain form at <=1e-4 rel err vs FP64"
+UNIT = "path-segments/s"
+# Algorithmic FP32 instruction count of one path-segment of the full recompute: tangent 9,
+# curvature 7, bin index 10, blend+absorption 4, log10 scale + compensated add 5, rotation ~3,
+# RNG/sincos ~2 (one path-segment = one weighted path x one segment).
+INSTR_PER_SEGMENT = 40.0
+SMS = 148
+LANES_PER_SM = 128
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+        self.th = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def workload_params(T, form, num_chains=0, chain_offset=0, device=0):
+    return T.default_params(num_segments=W["N"], mu=W["mu"], eps=W["eps"], scatter=W["scatter"],
+                            absorption=W["absorption"], num_steps_int=W["num_steps_int"],
+                            num_curvature_steps=W["bins"], paths_to_generate=W["paths"], paths_to_skip=W["burn_in"],
+                            perturb_seed=W["seed"], bootstrap_seed=7, max_sub_chain=W["k_max"],
+                            max_angle=W["max_angle"], form=form, lut_mode=T.LUT_FP64, num_chains=num_chains,
+                            chain_offset=chain_offset, device=device)
+
+
+def workload_bc(T):
+    return T.make_bc(W["start"], W["sdir"], W["end"], W["edir"], W["S"])
+
+
+def dist_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def time_passes(T, torch, ctx, steps, warmup, device):
+    """Device time of `steps` passes, each bracketed by events on one stream, L2 flushed between."""
+    stream = torch.cuda.Stream(device=device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            ctx.launch(stream.cuda_stream)
+        torch.cuda.synchronize(device)
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        for i in range(steps):
+            flush.zero_()
+            starts[i].record(stream)
+            ctx.launch(stream.cuda_stream)
+            ends[i].record(stream)
+        torch.cuda.synchronize(device)
+    ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    return ms
+
+
+def cpu_reference_run(paths, threads, timeout=600):
+    """The reference's own chain loop (GeometryRandom, compiled from its sources into
+    oracle/_ref) on this host: returns (path-segments/s, perturb ms, record)."""
+    import numpy as np
+    import twisty_b200 as T
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    if not os.path.exists(harness):
+        return None
+    cfg = {"experiment": {
+        "basicExperiment": {"startPos": list(W["start"]), "startDir": list(W["sdir"]), "endPos": list(W["end"]),
+                            "endDir": list(W["edir"]), "arclength": W["S"]},
+        "experimentParams": {"pathsToGenerate": paths, "pathsToSkip": W["burn_in"], "numSegments": W["N"],
+                             "name": "bench", "experimentDir": tempfile.gettempdir(), "maxPerturbThreads": threads,
+                             "maxWeightThreads": 0, "outputBigFloatWeights": False, "outputPathBatches": False,
+                             "perturbMethod": 0, "random": {"bootstrapSeed": 7, "perturbSeed": W["seed"]},
+                             "useGpu": False,
+                             "weighting": {"weightFunction": 0, "mu": W["mu"], "eps": W["eps"],
+                                           "numStepsInt": W["num_steps_int"], "numCurvatureSteps": W["bins"],
+                                           "absorption": W["absorption"], "scatter": W["scatter"]}}}}
+    with tempfile.TemporaryDirectory() as tmp:
+        cf = os.path.join(tmp, "cfg.json")
+        with open(cf, "w") as f:
+            json.dump(cfg, f)
+        p = T.default_params(num_segments=W["N"], bootstrap_seed=7)
+        curve = T.bootstrap_curve(p, workload_bc(T))
+        curve.astype(np.float32).tofile(cf + ".curve")
+        r = subprocess.run([harness, "chain", cf, cf + ".curve", str(threads), str(paths), cf + ".out"],
+                           capture_output=True, text=True, timeout=timeout, env={**os.environ, "TMPDIR": tmp})
+        if r.returncode != 0:
+            raise RuntimeError(r.stderr[-2000:])
+        rec = json.load(open(cf + ".out"))
+    return rec["paths"] * W["N"] / (rec["perturb_ms"] / 1e3), rec["perturb_ms"], rec
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference_arm(args):
+    ws, rank, _ = dist_info()
+    if rank != 0:
+        return 0
+    threads = cpu_threads()
+    paths = threads * 1_000_000   # one 1e6-path CombinedWeightValues chunk per thread
+    for _ in range(args.warmup):
+        cpu_reference_run(paths // 4, threads)
+    vals = []
+    for _ in range(args.steps):
+        v, ms, rec = cpu_reference_run(paths, threads)
+        vals.append((v, ms))
+    value = statistics.median(v for v, _ in vals)
+    ms = statistics.median(m for _, m in vals)
+    sample = (f"{paths} paths x N=256 per step on {threads} threads (one 1e6-path chunk per thread); the reference "
+              f"loop's own proposals: k~U{{2..25}}, angle~U(-pi,pi)")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD_NAME, "paths_per_step": paths, "segments": W["N"], "parallelism": "host threads"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--form", default="compensated", choices=["compensated", "plain", "fp64"])
+    ap.add_argument("--no-error", action="store_true", help="skip the FP64 error measurement")
+    ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP32 drop-in")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import twisty_b200 as T
+
+    ws, rank, local = dist_info()
+    device = local
+    torch.cuda.set_device(device)
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device(f"cuda:{device}"))
+        pg = dist
+    form = {"compensated": T.FORM_COMPENSATED, "plain": T.FORM_PLAIN_FP32, "fp64": T.FORM_FP64}[args.form]
+    bc = workload_bc(T)
+
+    # one chain layout for every rank (the form's default), disjoint chain ids per rank
+    with T.Context(workload_params(T, form, device=device)) as probe:
+        probe.prepare(bc)
+        probe.launch()
+        chains = probe.collect().num_chains
+
+    ctx = T.Context(workload_params(T, form, num_chains=chains, chain_offset=rank * chains, device=device))
+    ctx.prepare(bc)
+    with ClockSampler(device) as clk:
+        ms = time_passes(T, torch, ctx, args.steps, args.warmup, device)
+    res = ctx.collect()
+    kernel_ms = res.perturb_ms
+    per_step = sum(ms) / len(ms)
+    if pg:
+        t = torch.tensor([per_step, kernel_ms], dtype=torch.float64, device=f"cuda:{device}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        per_step, kernel_ms = t.tolist()
+    segs = res.total_paths * W["N"]
+    value = segs * ws / (per_step / 1e3)
+
+    # end to end through the C ABI with host buffers
+    e2e_ctx = T.Context(workload_params(T, form, num_chains=chains, chain_offset=rank * chains, device=device))
+    e2e_ctx.run(bc)   # warm (builds and caches the table)
+    reps = max(1, min(args.steps, 5))
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        er = e2e_ctx.run(bc)
+    torch.cuda.synchronize(device)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / reps
+    if pg:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{device}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = t.item()
+    e2e_ctx.close()
+    N = W["N"]
+    h2d = 4 * 3 * (N + 1) + 4 * 3 * N + 8 * W["bins"]          # curve + its segment vectors + linear table
+    d2h = 48 + 4 * W["bins"] + 32                                # result + table readback + range
+
+    extra = {}
+    if rank == 0 and not args.no_error and form != T.FORM_FP64:
+        with T.Context(workload_params(T, T.FORM_FP64, num_chains=chains, device=device)) as c64:
+            r64 = c64.run(bc)
+        extra["error_vs_fp64"] = {"rel": abs(10 ** (res.log10_weight - r64.log10_weight) - 1),
+                                  "log10_weight": res.log10_weight, "log10_weight_fp64": r64.log10_weight,
+                                  "fp64_ms": r64.perturb_ms, "rel_std_error": res.rel_std_error}
+    if rank == 0 and not args.no_plain and form == T.FORM_COMPENSATED:
+        with T.Context(workload_params(T, T.FORM_PLAIN_FP32, device=device)) as cp:
+            cp.prepare(bc)
+            pms = time_passes(T, torch, cp, max(1, min(args.steps, 3)), 1, device)
+            rp = cp.collect()
+            plain_v = rp.total_paths * N / (sum(pms) / len(pms) / 1e3)
+            pe = None
+            if not args.no_error:
+                with T.Context(workload_params(T, T.FORM_FP64, num_chains=rp.num_chains, device=device)) as c64:
+                    rp64 = c64.run(bc)
+                pe = abs(10 ** (rp.log10_weight - rp64.log10_weight) - 1)
+        extra["plain_fp32"] = {"value": plain_v, "ms_per_step": sum(pms) / len(pms), "chains": rp.num_chains,
+                               "error_vs_fp64": pe, "speedup_of_chosen": value / ws / plain_v}
+
+    peaks = load_peaks()
+    clocks = clk.summary()
+    sm_max = peaks.get("sm_max_mhz", 1965.0)
+    peak_ti = SMS * LANES_PER_SM * sm_max * 1e6 / 1e12
+    achieved_ti = INSTR_PER_SEGMENT * segs / (kernel_ms / 1e3) / 1e12
+    roofline = {"bound": "fp32", "kernel": "comp_chain_kernel" if form == T.FORM_COMPENSATED else args.form,
+                "achieved": achieved_ti, "peak": peak_ti, "unit": "Tinstr/s", "frac": achieved_ti / peak_ti,
+                "traffic": None, "basis": f"{INSTR_PER_SEGMENT:g} FP32 instructions per path-segment; peak = "
+                f"{SMS} SMs x {LANES_PER_SM} lanes x {sm_max:g} MHz (max SM clock of MEASURED_PEAKS.json)",
+                "segments_per_s_kernel_only": segs / (kernel_ms / 1e3)}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        threads = cpu_threads()
+        try:
+            r = cpu_reference_run(threads * 1_000_000, threads)
+            if r:
+                cpu = {"value": r[0], "unit": UNIT, "cores": threads, "kind": "reference",
+                       "sample": f"{threads * 1_000_000} paths x N=256, reference GeometryRandom loop on {threads} threads"}
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": threads, "kind": "reference", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": per_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32 (f64 cross-chain)", "data": "synthetic",
+                "config": {"workload": WORKLOAD_NAME, "form": args.form, "chains_per_gpu": chains,
+                           "steps_per_chain": res.steps_per_chain, "paths_per_gpu": res.total_paths,
+                           "l2": "flushed between steps (256 MB write)", "parallelism": f"independent chains x{ws}"},
+                "e2e": {"value": segs * ws / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms,
+                        "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+                "gpu_launches": ctx.kernels_per_launch() * args.steps, **extra}
+        print(json.dumps(line))
+    ctx.close()
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

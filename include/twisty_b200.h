@@ -1,0 +1,255 @@
+/*
+ * twisty_b200.h -- C ABI of the B200-native path-integral Monte Carlo runner.
+ *
+ * Drop-in for the reference's experiment-runner API (Twisty/ExperimentRunner.h:29-131)
+ * and its two runners, FullExperimentRunnerOptimalPerturb (CPU,
+ * Twisty/FullExperimentRunnerOptimalPerturb.h:26-74) and
+ * FullExperimentRunnerOptimalPerturbOptimized_GPU
+ * (Twisty/FullExperimentRunnerOptimalPerturbOptimized_GPU.h:36-47).
+ *
+ * All types are plain C structs; no exception, exit() or C++ type crosses this
+ * boundary. Every call returns a twisty_status; twisty_last_error() gives the message.
+ * Weights cross the ABI as log10 values (the reference's weights overflow double:
+ * Twisty/ExperimentRunner.h:75 keeps them in a 100-digit decimal type).
+ *
+ * A context is not re-entrant: one thread at a time may call into a given context
+ * (the reference's RunExperiment is not re-entrant either). Distinct contexts may be
+ * used concurrently from distinct threads.
+ */
+#ifndef TWISTY_B200_H
+#define TWISTY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TWISTY_B200_ABI_VERSION 1
+
+/* Status codes. The reference reports failures by std::nullopt
+ * (FullExperimentRunnerOptimalPerturbOptimized_GPU.cu:153-157), std::runtime_error
+ * (PathGeneration.cpp:51-57,75-77,240-247), exit(1)
+ * (FullExperimentRunnerOptimalPerturb.cpp:320-325) or printf-and-continue (.cu:50-56). */
+typedef enum twisty_status {
+    TWISTY_OK = 0,
+    TWISTY_ERR_INVALID_ARGUMENT = 1,   /* null pointer, size out of range */
+    TWISTY_ERR_INVALID_CONFIG = 2,     /* config text/params rejected (N < 4, odd numStepsInt, ...) */
+    TWISTY_ERR_INFEASIBLE_GEOMETRY = 3,/* no polyline of N segments of length S/N joins the ends */
+    TWISTY_ERR_LUT_INVALID = 4,        /* weight table has NaN/negative entries or < 2 bins */
+    TWISTY_ERR_CUDA = 5,               /* a CUDA runtime call failed */
+    TWISTY_ERR_DEVICE_TIMEOUT = 6,     /* a device-side wait ran past its deadline */
+    TWISTY_ERR_IO = 7,                 /* export/config file could not be written/read */
+    TWISTY_ERR_UNSUPPORTED = 8,        /* combination not implemented (e.g. perturbMethod != 0) */
+    TWISTY_ERR_NO_DEVICE = 9,          /* no CUDA device, or the library was built without one */
+    TWISTY_ERR_OUT_OF_MEMORY = 10
+} twisty_status;
+
+/* Arithmetic form of the Markov-chain kernel. */
+typedef enum twisty_form {
+    /* The reference GPU kernel's design (FullExperimentRunnerOptimalPerturbOptimized_GPU.cu:
+     * 689-918): one chain per thread, chain state in global memory, FP32 IEEE
+     * rotate/tangent/curvature, FP64 log10 per segment, CombinedWeightValues_C partials. */
+    TWISTY_FORM_PLAIN_FP32 = 0,
+    /* The B200 form: warp-cooperative chains held in shared memory as segment vectors,
+     * FP32 tables staged in shared memory, Kahan-compensated FP32 log-weights, log-sum-exp
+     * reductions rescaled by the running maximum, FP64 only across chains. */
+    TWISTY_FORM_COMPENSATED = 1,
+    /* FP64 everywhere (positions, rotation, table, weights): the error yardstick. */
+    TWISTY_FORM_FP64 = 2
+} twisty_form;
+
+typedef enum twisty_lut_mode {
+    TWISTY_LUT_FAITHFUL = 0, /* the reference's mixed precision: float phase function, double
+                                Simpson, float table (PathWeightUtils.cpp:19-33,371-433) */
+    TWISTY_LUT_FP64 = 1,     /* the same quadrature entirely in double */
+    TWISTY_LUT_EXTERNAL = 2  /* the caller's table, set with twisty_set_lut */
+} twisty_lut_mode;
+
+typedef struct twisty_vec3 {
+    float x, y, z;
+} twisty_vec3;
+
+/* PerturbUtils::BoundaryConditions (Twisty/CurvePerturbUtils.h:62-68). */
+typedef struct twisty_bc {
+    twisty_vec3 start_pos;
+    twisty_vec3 start_dir; /* unit */
+    twisty_vec3 end_pos;
+    twisty_vec3 end_dir;   /* unit */
+    float arclength;
+} twisty_bc;
+
+/* ExperimentRunner::ExperimentParameters (Twisty/ExperimentRunner.h:42-68) with its
+ * WeightingParameters (Twisty/PathWeightUtils.h:35-48), plus the B200 knobs.
+ * Fill with twisty_params_init() first. */
+typedef struct twisty_params {
+    uint32_t struct_size;        /* sizeof(twisty_params) */
+    uint64_t paths_to_generate;  /* pathsToGenerate: accepted paths in the estimate */
+    uint64_t paths_to_skip;      /* pathsToSkip: unweighted burn-in steps of every chain */
+    uint32_t num_segments;       /* numSegments (N >= 4) */
+    uint32_t bootstrap_seed;     /* random.bootstrapSeed */
+    uint32_t perturb_seed;       /* random.perturbSeed */
+    int32_t weight_function;     /* weighting.weightFunction: 0 radiative transfer */
+    int32_t perturb_method;      /* perturbMethod: 0 GeometricRandom (the only one the reference runs) */
+    float mu;                    /* weighting.mu  (regulariser; see F5 swap in the docs) */
+    float eps;                   /* weighting.eps (phase-function parameter) */
+    float scatter;               /* weighting.scatter  (mu_s) */
+    float absorption;            /* weighting.absorption (mu_a) */
+    uint32_t num_steps_int;      /* weighting.numStepsInt (even) */
+    uint32_t num_curvature_steps;/* weighting.numCurvatureSteps (table bins) */
+    float min_bound;             /* 0 */
+    float max_bound;             /* 10/eps */
+    float bias;                  /* 1 */
+    /* ---- B200 knobs ---- */
+    int32_t form;                /* twisty_form */
+    int32_t lut_mode;            /* twisty_lut_mode */
+    uint32_t max_sub_chain;      /* k_max of the rotated sub-chain (reference: 25) */
+    float max_angle;             /* rotation angle ~ U(-max_angle, max_angle) (reference: pi) */
+    uint32_t num_chains;         /* independent Markov chains; 0 = form default */
+    int32_t device;              /* CUDA device ordinal */
+    uint32_t chain_offset;       /* first global chain id (shards one experiment over GPUs) */
+    uint32_t experiment_id;      /* Philox stream id of this experiment */
+    int32_t bootstrap_kind;      /* 0 auto, 1 reference recursion (N-2 in {4,6,8,12,16,24,...}), 2 arc */
+    twisty_vec3 eval_end_shift;  /* weights evaluated with the receiver moved by this vector,
+                                    the chain itself unchanged (finite-difference checks) */
+} twisty_params;
+
+/* ExperimentRunner::ExperimentResults (Twisty/ExperimentRunner.h:73-82). */
+typedef struct twisty_result {
+    double log10_weight;         /* log10 experimentWeight = log10(sum of path weights * normaliser) */
+    double log10_normalizer;     /* log10 Norm(N, ds, bc) (PathWeightUtils.cpp:721-752) */
+    double log10_mean_weight;    /* log10(experimentWeight / totalPathsGenerated) */
+    double rel_std_error;        /* standard error of experimentWeight / experimentWeight,
+                                    from the spread of the independent chains' sums */
+    uint64_t total_paths;        /* totalPathsGenerated (valid, weighted paths) */
+    uint64_t failed_paths;       /* numFailedPaths (NaN weights) */
+    uint64_t clamped_curvatures; /* curvatures outside the table range, clamped */
+    uint32_t num_chains;
+    uint32_t steps_per_chain;
+    double total_ms;             /* totalExperimentMs */
+    double setup_ms;             /* setupExperimentMs: table, normaliser, initial curve */
+    double perturb_ms;           /* perturbExperimentMs: the chain kernel, device time */
+    double weighting_ms;         /* weightingExperimentMs: final reduction */
+} twisty_result;
+
+/* Table metadata (BaseWeightLookupTable accessors, Twisty/PathWeightUtils.h:129-141). */
+typedef struct twisty_lut_info {
+    float min_curvature, max_curvature, curvature_step;
+    float min_segment_weight, max_segment_weight, ds;
+    uint32_t bins;
+} twisty_lut_info;
+
+/* One experiment of a batch (the receiver/pixel loops of the reference's drivers,
+ * e.g. Experiments/BeamSpreadExperiment.cpp:240-269, NoisyCircleExperiment.cpp:259-361). */
+typedef struct twisty_experiment {
+    twisty_bc bc;
+    uint32_t num_segments;
+    float scatter;               /* per-experiment mu_s */
+    float eps;                   /* per-experiment phase parameter (sigma^2) */
+    uint64_t paths;              /* paths_to_generate of this experiment */
+} twisty_experiment;
+
+typedef struct twisty_ctx twisty_ctx;
+
+/* ---------------------------------------------------------------- basics */
+int twisty_abi_version(void);
+const char *twisty_status_string(twisty_status s);
+/* Reference defaults: ExperimentParameters/WeightingParameters member initialisers. */
+void twisty_params_init(twisty_params *p);
+
+/* ExperimentRunner::ParseExperimentParamsFromConfig (Twisty/ExperimentRunner.cpp:48-177)
+ * plus the basicExperiment block read by Experiments/FullExperiment.cpp:162-191.
+ * `text` is the reference's JSON config schema, or the same keys in YAML block syntax
+ * (is_yaml != 0). bc may be NULL. */
+twisty_status twisty_params_from_config(const char *text, int is_yaml, twisty_params *out, twisty_bc *bc);
+
+/* --------------------------------------------------------------- context */
+/* ExperimentRunner(ExperimentParameters&) ctor (Twisty/ExperimentRunner.cpp:180-192);
+ * the params are copied. Selects and initialises the CUDA device. */
+twisty_status twisty_create(const twisty_params *p, twisty_ctx **out);
+void twisty_destroy(twisty_ctx *ctx);
+const char *twisty_last_error(const twisty_ctx *ctx);
+twisty_status twisty_update_params(twisty_ctx *ctx, const twisty_params *p);
+
+/* ----------------------------------------------------------- experiments */
+/* ExperimentRunner::RunExperiment (Twisty/ExperimentRunner.cpp:196-301) ->
+ * RunnerSpecificRunExperiment (FullExperimentRunnerOptimalPerturb.cpp:48-435). Host in,
+ * host out: builds the table, the normaliser and the initial curve, runs the chains,
+ * reduces, and fills *res. */
+twisty_status twisty_run(twisty_ctx *ctx, const twisty_bc *bc, twisty_result *res);
+
+/* Split form of twisty_run for callers that keep inputs resident and time the device:
+ * twisty_prepare does the setup (table, normaliser, curve, device state) once;
+ * twisty_launch enqueues one full Monte Carlo pass on `stream` (a cudaStream_t, NULL for
+ * the context's own stream) without synchronising; twisty_collect waits and reduces. */
+twisty_status twisty_prepare(twisty_ctx *ctx, const twisty_bc *bc);
+twisty_status twisty_launch(twisty_ctx *ctx, void *stream);
+twisty_status twisty_collect(twisty_ctx *ctx, twisty_result *res);
+/* Number of kernels twisty_launch enqueues (for launch accounting). */
+uint32_t twisty_launch_kernel_count(const twisty_ctx *ctx);
+
+/* Many experiments (uneven N, S, mu_s, eps) in one persistent launch fed by a device
+ * work queue; the pass is captured once as a CUDA graph and replayed `iterations` times
+ * (results of the last replay). res has n entries. */
+twisty_status twisty_run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n,
+                               uint32_t iterations, twisty_result *res);
+
+/* ------------------------------------------------------------- weighting */
+/* Weigh exported paths: UpdateTangentsFromPos + UpdateCurvaturesFromTangents_RadiativeTransfer
+ * + WeightCurveViaCurvatureLog10_CudaSafe (CurvePerturbUtils.cpp:147-166,
+ * PathWeighters.cpp:27-104) on pos[n_paths][N+1][3]. Uses the context's table for
+ * ds = bc->arclength / N. Outputs log10 weights (without the normaliser), validity, and
+ * optionally the left bin index of every curvature (bins[n_paths][N-1], may be NULL).
+ * form selects the reference FP32 semantics (PLAIN_FP32) or the compensated path. */
+twisty_status twisty_weight_paths(twisty_ctx *ctx, const twisty_bc *bc, const float *pos,
+                                  uint64_t n_paths, int32_t form, double *log10w,
+                                  uint8_t *valid, int32_t *bins);
+
+/* WeightLookupTableIntegral(params, ds) + Initialize (PathWeightUtils.cpp:281-348), on
+ * the device in FP64. lut may be NULL (info only). */
+twisty_status twisty_build_lut(twisty_ctx *ctx, float ds, float *lut, twisty_lut_info *info);
+/* Use the caller's table (e.g. one exported by the reference) for subsequent runs. */
+twisty_status twisty_set_lut(twisty_ctx *ctx, const float *lut, const twisty_lut_info *info);
+
+/* NormalizerStuff::Norm (PathWeightUtils.cpp:721-752) as log10; N = 5, 6 run their
+ * 1e10-term quadrature on the device in FP64. */
+twisty_status twisty_normalizer_log10(twisty_ctx *ctx, uint32_t n_segments, float ds,
+                                      const twisty_bc *bc, double *out);
+
+/* Initial curve (Curve::SetBoundaryConditions + PathGeneration::ResolveEvenNumberOfSegments,
+ * Twisty/Curve.cpp:20-30, Twisty/PathGeneration.cpp:236-414) for any N >= 4:
+ * pos[N+1][3]. Fails with TWISTY_ERR_INFEASIBLE_GEOMETRY when no curve exists. */
+twisty_status twisty_bootstrap_curve(const twisty_params *p, const twisty_bc *bc, float *pos);
+/* CalculateMinimumArclength (Twisty/PathGeneration.cpp:12-43). */
+float twisty_min_arclength(const twisty_bc *bc, uint32_t n_segments);
+/* Use pos[n_points][3] (n_points = N+1) as the initial curve of the context's next runs
+ * instead of the bootstrapper; the reference replicates one initial curve into every
+ * chain (FullExperimentRunnerOptimalPerturb.cpp:122-179). NULL reverts to the bootstrapper. */
+twisty_status twisty_set_initial_curve(twisty_ctx *ctx, const float *pos, uint32_t n_points);
+
+/* --------------------------------------------------------------- exports */
+/* Path-batch export of GeometryRandom_ExportPaths / BeginPathBatchOutput
+ * (FullExperimentRunnerOptimalPerturb.cpp:599-858, ExperimentRunner.cpp:303-396): runs the
+ * experiment and writes, under dir/GeneratedCurves/, Paths_Binary.pbd (f32 [P][N+1][3]),
+ * Log10PathWeights_Binary.bdt (f64 linear weights incl. normaliser, as the reference),
+ * Paths_Metadata.pmd ("chain batch count" lines), BoundaryConditions.bcf (56 bytes) and
+ * index.json, for the first max_paths accepted paths. Also returns them in memory when
+ * pos/log10w are not NULL (pos[max_paths][N+1][3], log10w[max_paths], without the normaliser). */
+twisty_status twisty_export_paths(twisty_ctx *ctx, const twisty_bc *bc, const char *dir,
+                                  uint64_t max_paths, float *pos, double *log10w,
+                                  uint64_t *n_written, twisty_result *res);
+
+/* ---------------------------------------------------------------- adjoint */
+/* Gradient of log10 experimentWeight with respect to (mu_s, sigma, receiver x, y, z),
+ * sigma = sqrt(eps), by a hand-written adjoint pass that replays the chains of the
+ * forward run in `fwd` (same params, same bc) and recomputes curvatures instead of storing
+ * them. The receiver gradient moves the two fixed end points with the interior held
+ * (pathwise estimator). grad has 5 entries. */
+twisty_status twisty_adjoint(twisty_ctx *ctx, const twisty_bc *bc, const twisty_result *fwd,
+                             double grad[5]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TWISTY_B200_H */

@@ -771,9 +771,9 @@ static void *chain_worker_f64(void *arg)
             const double sn = sin(ha), cs = cos(ha);
             /* rotation matrix of the unit quaternion (cs, a*sn) applied as q^-1 p q */
             const double qw = cs, qx = ax * sn, qy = ay * sn, qz = az * sn;
-            const double r00 = 1 - 2 * (qy * qy + qz * qz), r01 = 2 * (qx * qy + qw * qz), r02 = 2 * (qx * qz - qw * qy);
-            const double r10 = 2 * (qx * qy - qw * qz), r11 = 1 - 2 * (qx * qx + qz * qz), r12 = 2 * (qy * qz + qw * qx);
-            const double r20 = 2 * (qx * qz + qw * qy), r21 = 2 * (qy * qz - qw * qx), r22 = 1 - 2 * (qx * qx + qy * qy);
+            const double r00 = 1 - 2 * (qy * qy + qz * qz), r01 = 2 * (qx * qy - qw * qz), r02 = 2 * (qx * qz + qw * qy);
+            const double r10 = 2 * (qx * qy + qw * qz), r11 = 1 - 2 * (qx * qx + qz * qz), r12 = 2 * (qy * qz - qw * qx);
+            const double r20 = 2 * (qx * qz - qw * qy), r21 = 2 * (qy * qz + qw * qx), r22 = 1 - 2 * (qx * qx + qy * qy);
             for (uint32_t i = left + 1; i < right; ++i) {
                 const double vx = pos[3 * i] - lx, vy = pos[3 * i + 1] - ly, vz = pos[3 * i + 2] - lz;
                 pos[3 * i] = r00 * vx + r01 * vy + r02 * vz + lx;

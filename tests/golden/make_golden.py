@@ -1,0 +1,202 @@
+"""Generate the golden fixtures under tests/golden/ from the reference itself.
+
+    make -C oracle ref && python tests/golden/make_golden.py
+
+Every expected value here comes out of the reference's own code, compiled from its
+sources by oracle/Makefile (with the three patches it documents) and driven through
+oracle/_ref/ref_harness:
+  lut_*.npz        WeightLookupTableIntegral::Initialize tables and their metadata
+  paths_*.npz      path batches and, per path, the reference weigher's log10 weight,
+                   curvatures and left bin indices (UpdateTangentsFromPos,
+                   UpdateCurvaturesFromTangents_RadiativeTransfer, WeightCurveViaCurvatureLog10_CudaSafe)
+  rotate.npz       RotateVectorByQuaternion on random inputs
+  cw.npz           CombinedWeightValues_C add / combine / extract sequences
+  norm.json        log10 Norm(N, ds, bc) for N = 4 (and 5)
+  boot_*.npy       reference bootstrap curves (ResolveEvenNumberOfSegments)
+  chain_*.json     full runs of the reference's Markov-chain loop (GeometryRandom) for the
+                   statistical comparison, with per-1e6-path chunk sums
+The path batches are perturbed with the oracle's chain runner so they cover curved
+configurations; their weights still come from the reference weigher. This script reads
+the reference tree only through oracle/_ref, and is never run by the tests themselves.
+"""
+from __future__ import annotations
+
+import json
+import os
+import struct
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+from oracle import py_oracle as O  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+H = O.REF_HARNESS
+F32 = np.float32
+
+# (name, mu, eps, scatter, absorption, numStepsInt, bins, N, S)
+LUTS = [
+    ("A", 1.0, 0.01, 10.0, 0.0, 2000, 1024, 66, 10.0),
+    ("B", 1.0, 0.01, 10.0, 0.05, 2000, 2048, 34, 12.0),
+    ("C", 0.3, 0.0025, 50.0, 0.0, 4000, 512, 18, 6.0),
+]
+GEOM = {  # N -> (startPos, startDir, endPos, endDir)
+    66: ((0, 0, 0), (1, 0, 0), (8, 0, 0), (1, 0, 0)),
+    34: ((0, 0, 0), (0, 0, 1), (0, 0, 7), (0, 0, 1)),
+    18: ((0, 0, 0), (1, 0, 0), (2.5, 1.0, 0.5), (0, 1, 0)),
+    10: ((0, 0, 0), (1, 0, 0), (3, 0, 0), (1, 0, 0)),
+}
+
+
+def run(args, **kw):
+    return subprocess.run([H, *map(str, args)], check=True, capture_output=True, text=True, **kw)
+
+
+def bc12(n):
+    g = GEOM[n]
+    return [c for v in g for c in v]
+
+
+def ref_lut(tmp, mu, eps, scatter, absorption, nsteps, bins, ds):
+    f = os.path.join(tmp, "lut.bin")
+    run(["lut", repr(mu), repr(eps), repr(scatter), repr(absorption), nsteps, bins, repr(float(ds)), f])
+    b = open(f, "rb").read()
+    hdr = np.frombuffer(b[:24], F32)
+    n = struct.unpack("<I", b[24:28])[0]
+    lut = np.frombuffer(b[28:28 + 4 * n], F32).copy()
+    return f, hdr, lut
+
+
+def ref_weigh(tmp, lutfile, N, S, absorption, pos):
+    pf = os.path.join(tmp, "paths.bin")
+    of = os.path.join(tmp, "wout.bin")
+    with open(pf, "wb") as f:
+        f.write(struct.pack("<Q", pos.shape[0]))
+        f.write(np.ascontiguousarray(pos, F32).tobytes())
+    run(["weigh", lutfile, N, repr(float(S)), repr(float(absorption)), pf, of])
+    b = open(of, "rb").read()
+    rec = 1 + 8 + 8 * (N - 1)
+    P = pos.shape[0]
+    valid = np.zeros(P, np.uint8)
+    w = np.zeros(P)
+    curv = np.zeros((P, N - 1), F32)
+    bins = np.zeros((P, N - 1), np.int32)
+    for p in range(P):
+        x = b[p * rec:(p + 1) * rec]
+        valid[p] = x[0]
+        w[p] = struct.unpack("<d", x[1:9])[0]
+        curv[p] = np.frombuffer(x[9:9 + 4 * (N - 1)], F32)
+        bins[p] = np.frombuffer(x[9 + 4 * (N - 1):], np.int32)
+    return w, valid, curv, bins
+
+
+def ref_bootstrap(tmp, N, S, seed):
+    f = os.path.join(tmp, "boot.bin")
+    run(["bootstrap", N, repr(float(S)), *bc12(N), seed, f])
+    return np.fromfile(f, F32).reshape(N + 1, 3)
+
+
+def make_config(N, S, paths, skip, seed, mu, eps, scatter, absorption, nsteps, bins, threads):
+    g = GEOM[N]
+    return {"experiment": {
+        "basicExperiment": {"startPos": list(g[0]), "startDir": list(g[1]), "endPos": list(g[2]),
+                            "endDir": list(g[3]), "arclength": S},
+        "experimentParams": {"pathsToGenerate": paths, "pathsToSkip": skip, "numSegments": N, "name": "golden",
+                             "experimentDir": "/tmp/twisty_golden", "maxPerturbThreads": threads,
+                             "maxWeightThreads": 0, "outputBigFloatWeights": False, "outputPathBatches": False,
+                             "perturbMethod": 0, "random": {"bootstrapSeed": 7, "perturbSeed": seed},
+                             "useGpu": False,
+                             "weighting": {"weightFunction": 0, "mu": mu, "eps": eps, "numStepsInt": nsteps,
+                                           "numCurvatureSteps": bins, "absorption": absorption,
+                                           "scatter": scatter}}}}
+
+
+def main():
+    if not os.path.exists(H):
+        sys.exit("build the reference first: make -C oracle ref")
+    rng = np.random.default_rng(20261203)
+    with tempfile.TemporaryDirectory() as tmp:
+        # ---- bootstrap curves
+        boots = {}
+        for N, S in ((10, 5.0), (18, 6.0), (34, 12.0), (66, 10.0)):
+            boots[N] = ref_bootstrap(tmp, N, S, 7)
+            np.save(os.path.join(OUT, f"boot_{N}.npy"), boots[N])
+        # ---- tables and weighed path batches
+        for name, mu, eps, scatter, absorption, nsteps, bins, N, S in LUTS:
+            ds = F32(S) / F32(N)
+            lf, hdr, lut = ref_lut(tmp, mu, eps, scatter, absorption, nsteps, bins, ds)
+            np.savez(os.path.join(OUT, f"lut_{name}.npz"), lut=lut, hdr=hdr,
+                     params=np.array([mu, eps, scatter, absorption, nsteps, bins, N, S], np.float64))
+            wp = O.wparams(mu, eps, scatter, absorption, nsteps, bins)
+            olut, meta = O.lut_f32(wp, ds)
+            init = boots[N]
+            pos = [init[None]]
+            # curved configurations: chain states after a few rotations of U(-pi, pi)
+            for seed, steps in ((11, 3), (12, 17), (13, 60)):
+                r = O.run_chains(init, N, S, olut, meta, seed=seed, n_chains=20, steps=steps, want_final=True)
+                pos.append(r["final_pos"])
+            # a fully stretched straight path (all curvatures 0) on the same N
+            st = np.zeros((1, N + 1, 3), F32)
+            st[0, :, 0] = np.arange(N + 1, dtype=F32) * ds
+            pos.append(st)
+            pos = np.concatenate(pos).astype(F32)
+            w, valid, curv, rbins = ref_weigh(tmp, lf, N, S, absorption, pos)
+            np.savez(os.path.join(OUT, f"paths_{name}.npz"), pos=pos, log10w=w, valid=valid, curv=curv, bins=rbins)
+            print(f"lut/paths {name}: {pos.shape[0]} paths, N={N}")
+        # ---- rotation
+        n = 512
+        q = rng.normal(size=(n, 4)).astype(F32)
+        q /= np.linalg.norm(q, axis=1, keepdims=True)
+        v = (rng.normal(size=(n, 3)) * 3).astype(F32)
+        f = os.path.join(tmp, "rot.bin")
+        with open(f, "wb") as fh:
+            fh.write(struct.pack("<Q", n))
+            fh.write(np.concatenate([q, v], 1).astype(F32).tobytes())
+        run(["rotate", f, f + ".out"])
+        np.savez(os.path.join(OUT, "rotate.npz"), q=q, v=v, out=np.fromfile(f + ".out", F32).reshape(n, 3))
+        # ---- combined weights
+        seqs = [rng.normal(-300, 20, 4000), np.sort(rng.normal(-50, 5, 1000)), np.full(64, -12.5),
+                rng.normal(700, 40, 3000)]
+        splits = [1500, 400, 32, 2999]
+        recs = []
+        for s, sp in zip(seqs, splits):
+            f = os.path.join(tmp, "cw.bin")
+            with open(f, "wb") as fh:
+                fh.write(struct.pack("<QQ", len(s), sp))
+                fh.write(np.asarray(s, np.float64).tobytes())
+            run(["cw", f, f + ".out"])
+            b = open(f + ".out", "rb").read()
+            recs.append({"values": np.asarray(s).tolist(), "split": sp,
+                         "cw": [list(struct.unpack("<dddII", b[i * 32:(i + 1) * 32])[:4]) for i in range(3)],
+                         "extract_log10": list(struct.unpack("<ddd", b[96:120]))})
+        json.dump(recs, open(os.path.join(OUT, "cw.json"), "w"))
+        # ---- normaliser
+        norm = []
+        for N, ds, bc in ((4, 0.25, [0, 0, 0, 0, 0, 1, 0.3, 0.1, 0.4, 0, 0, 1]),
+                          (4, 0.5, [0, 0, 0, 1, 0, 0, 0.7, 0.2, 0.1, 0, 1, 0]),
+                          (4, 0.1, [0, 0, 0, 0, 0, 1, 0, 0, 0.25, 0, 0, 1])):
+            out = run(["norm", N, repr(ds), *bc]).stdout.strip().splitlines()[-1]
+            norm.append({"N": N, "ds": ds, "bc": bc, "log10": float(out)})
+        if os.environ.get("TWISTY_GOLDEN_NORM5"):
+            out = run(["norm", 5, repr(0.25), 0, 0, 0, 0, 0, 1, 0.2, 0.1, 0.9, 0, 0, 1]).stdout.strip().splitlines()[-1]
+            norm.append({"N": 5, "ds": 0.25, "bc": [0, 0, 0, 0, 0, 1, 0.2, 0.1, 0.9, 0, 0, 1], "log10": float(out)})
+        json.dump(norm, open(os.path.join(OUT, "norm.json"), "w"), indent=1)
+        # ---- reference Markov-chain runs (statistical parity): theta ~ U(-pi, pi), k <= 25
+        for N, S, paths, threads in ((10, 5.0, 32_000_000, 8), (18, 6.0, 16_000_000, 8), (66, 10.0, 16_000_000, 8)):
+            cfg = make_config(N, S, paths, 1000, 4321, 1.0, 0.01, 10.0, 0.0, 2000, 1024, threads)
+            cf = os.path.join(tmp, f"chain_{N}.json")
+            json.dump(cfg, open(cf, "w"))
+            np.asarray(boots[N], F32).tofile(cf + ".curve")
+            run(["chain", cf, cf + ".curve", threads, paths, cf + ".out"])
+            res = json.load(open(cf + ".out"))
+            res["config"] = cfg
+            json.dump(res, open(os.path.join(OUT, f"chain_{N}.json"), "w"))
+            print(f"chain N={N}: log10 W = {res['log10_weight']:.6f} in {res['perturb_ms']:.0f} ms")
+
+
+if __name__ == "__main__":
+    main()

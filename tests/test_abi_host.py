@@ -1,0 +1,144 @@
+"""Host-side checks of the C ABI that need no GPU: the library loads and exports every
+entry point include/twisty_b200.h declares, config parsing follows the reference schema,
+the bootstrapper and geometry checks, and the no-device error path."""
+import ctypes as C
+import json
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+import twisty_b200 as T
+from twisty_b200 import _abi
+
+HEADER = os.path.join(ROOT, "include", "twisty_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(twisty_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = _abi.load()
+    names = declared_functions()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(L, n), n
+    nm = subprocess.run(["nm", "-D", "--defined-only", _abi.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (twisty_\w+)", nm))
+    assert set(names) <= exported
+    # every ctypes signature matches a declared function and vice versa
+    assert sorted(n for n, _, _ in _abi.SIGNATURES) == names
+
+
+def test_struct_sizes_match_header():
+    # compile a probe against the header and compare struct sizes with the ctypes mirror
+    src = os.path.join(ROOT, "_work", "abi_probe.c")
+    os.makedirs(os.path.dirname(src), exist_ok=True)
+    with open(src, "w") as f:
+        f.write('#include "twisty_b200.h"\n#include <stdio.h>\n#include <stddef.h>\n'
+                'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(twisty_params), sizeof(twisty_bc),'
+                ' sizeof(twisty_result), sizeof(twisty_lut_info), sizeof(twisty_experiment),'
+                ' offsetof(twisty_params, eval_end_shift), offsetof(twisty_result, total_ms)); return 0;}\n')
+    exe = src[:-2]
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), src, "-o", exe], check=True)
+    sizes = list(map(int, subprocess.run([exe], capture_output=True, text=True).stdout.split()))
+    assert sizes == [C.sizeof(_abi.Params), C.sizeof(_abi.BC), C.sizeof(_abi.Result), C.sizeof(_abi.LutInfo),
+                     C.sizeof(_abi.Experiment), _abi.Params.eval_end_shift.offset, _abi.Result.total_ms.offset]
+
+
+def test_params_init_reference_defaults():
+    p = T.default_params()
+    assert p.struct_size == C.sizeof(_abi.Params)
+    # WeightingParameters member initialisers (Twisty/PathWeightUtils.h:35-48)
+    assert (p.mu, p.num_steps_int, p.min_bound, p.max_bound, p.eps, p.bias, p.num_curvature_steps) == \
+        (pytest.approx(0.1), 2000, 0.0, 100.0, pytest.approx(0.01), 1.0, 10000)
+    assert p.max_sub_chain == 25 and p.max_angle == pytest.approx(np.pi)
+
+
+def reference_config(**over):
+    cfg = json.load(open(os.path.join(ROOT, "tests", "golden", "chain_66.json")))["config"]
+    cfg["experiment"]["experimentParams"].update(over)
+    return cfg
+
+
+def test_config_json_and_yaml_agree():
+    cfg = reference_config()
+    ep, bc = T.ParseExperimentParamsFromConfig(json.dumps(cfg))
+    assert ep.numSegmentsPerCurve == 66 and ep.numPathsToSkip == 1000
+    assert ep.weightingParameters.maxBound == pytest.approx(10.0 / np.float32(0.01))
+    lines = []
+
+    def emit(d, ind):
+        for k, v in d.items():
+            if isinstance(v, dict):
+                lines.append(" " * ind + f"{k}:")
+                emit(v, ind + 2)
+            elif isinstance(v, list):
+                lines.append(" " * ind + f"{k}: [{', '.join(map(str, v))}]")
+            else:
+                lines.append(" " * ind + f"{k}: {json.dumps(v)}  # comment")
+    emit(cfg, 0)
+    ep2, bc2 = T.ParseExperimentParamsFromConfig("\n".join(lines), yaml=True)
+    assert ep2 == ep and bc2 == bc
+
+
+def test_config_normalises_directions_and_rejects_missing_keys():
+    cfg = reference_config()
+    cfg["experiment"]["basicExperiment"]["startDir"] = [2.0, 0.0, 0.0]
+    ep, bc = T.ParseExperimentParamsFromConfig(cfg)
+    assert bc.m_startDir == pytest.approx((1.0, 0.0, 0.0))
+    del cfg["experiment"]["experimentParams"]["weighting"]["eps"]
+    with pytest.raises(T.TwistyError) as e:
+        T.ParseExperimentParamsFromConfig(cfg)
+    assert e.value.status == _abi.ERR_INVALID_CONFIG
+    with pytest.raises(T.TwistyError):
+        T.ParseExperimentParamsFromConfig("{not json")
+
+
+def test_config_b200_block():
+    cfg = reference_config(b200={"form": 0, "maxSubChain": 32, "maxAngle": 0.05, "numChains": 4096})
+    ep, _ = T.ParseExperimentParamsFromConfig(cfg)
+    assert (ep.form, ep.maxSubChain, ep.numChains) == (0, 32, 4096) and ep.maxAngle == pytest.approx(0.05)
+
+
+@pytest.mark.parametrize("N,S,end", [(4, 5.0, (3, 0, 0)), (64, 10.0, (8, 0, 0)), (256, 20.0, (0, 0, 12)),
+                                     (257, 20.0, (0, 0, 12)), (1024, 40.0, (5, 5, 5)), (13, 3.0, (0, 0, 0))])
+def test_bootstrap_any_n(N, S, end):
+    d = (0, 0, 1) if end == (0, 0, 12) else (1, 0, 0)
+    bc = T.make_bc((0, 0, 0), d, end, d, S)
+    pos = T.bootstrap_curve(T.default_params(num_segments=N), bc).astype(np.float64)
+    seg = np.linalg.norm(np.diff(pos, axis=0), axis=1)
+    ds = np.float32(S) / np.float32(N)
+    # positions are stored in float: each length is exact up to the rounding of its end points
+    tol = 4 * np.abs(pos).max() * 2.0 ** -24
+    assert np.all(np.abs(seg - ds) <= tol + 2e-7 * ds)
+    assert np.allclose(pos[0], 0) and np.allclose(pos[-1], end, atol=1e-6)
+    assert np.allclose(pos[1], np.array(d) * ds, atol=1e-6)
+
+
+def test_bootstrap_infeasible():
+    bc = T.make_bc((0, 0, 0), (1, 0, 0), (11, 0, 0), (1, 0, 0), 10.0)
+    with pytest.raises(T.TwistyError) as e:
+        T.bootstrap_curve(T.default_params(num_segments=64), bc)
+    assert e.value.status == _abi.ERR_INFEASIBLE_GEOMETRY
+
+
+def test_min_arclength_formula():
+    # CalculateMinimumArclength (Twisty/PathGeneration.cpp:12-43) for straight ends
+    bc = T.make_bc((0, 0, 0), (1, 0, 0), (8, 0, 0), (1, 0, 0), 10.0)
+    assert T.min_arclength(bc, 64) == pytest.approx(8.0, rel=1e-6)
+
+
+def test_no_device_is_an_error_not_a_fallback():
+    if os.path.exists("/dev/nvidia0"):
+        pytest.skip("a GPU is present")
+    with pytest.raises(T.TwistyError) as e:
+        T.Context(T.default_params(num_segments=8))
+    assert e.value.status == _abi.ERR_NO_DEVICE

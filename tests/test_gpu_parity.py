@@ -1,0 +1,226 @@
+"""Parity of the CUDA library (through its C ABI) with the oracle and the reference's own
+golden outputs. Every test here needs a B200 (marker `gpu`)."""
+import numpy as np
+import pytest
+
+from conftest import GEOM, LUT_SETS, golden_json, golden_npz
+
+import twisty_b200 as T
+from twisty_b200 import _abi
+
+pytestmark = pytest.mark.gpu
+F32 = np.float32
+
+
+def lut_params(name, **kw):
+    mu, eps, sc, ab, nst, bins, N, S = LUT_SETS[name]
+    return T.default_params(num_segments=N, mu=mu, eps=eps, scatter=sc, absorption=ab, num_steps_int=nst,
+                            num_curvature_steps=bins, **kw), N, S
+
+
+def geom_bc(N, S):
+    g = GEOM[N]
+    return T.make_bc(g[0], g[1], g[2], g[3], S)
+
+
+def golden_lut_info(name):
+    g = golden_npz(f"lut_{name}.npz")
+    h = g["hdr"]
+    info = _abi.LutInfo(float(h[0]), float(h[1]), float(h[2]), float(h[3]), float(h[4]), float(h[5]), g["lut"].size)
+    return g["lut"], info
+
+
+# ------------------------------------------------------------------------------ tables
+@pytest.mark.parametrize("name", sorted(LUT_SETS))
+def test_faithful_table_within_one_ulp_of_reference(name):
+    p, N, S = lut_params(name, lut_mode=T.LUT_FAITHFUL)
+    g = golden_npz(f"lut_{name}.npz")
+    with T.Context(p) as ctx:
+        lut, info = ctx.build_lut(F32(S) / F32(N))
+    ulps = np.abs(lut.view(np.int32).astype(np.int64) - g["lut"].view(np.int32).astype(np.int64))
+    assert ulps.max() <= 1, ulps.max()
+    assert np.mean(ulps == 0) > 0.9
+    h = g["hdr"]
+    assert (info.min_curvature, info.max_curvature, info.curvature_step) == (h[0], h[1], h[2])
+
+
+@pytest.mark.parametrize("name", sorted(LUT_SETS))
+def test_fp64_table_matches_oracle_twin(oracle, name):
+    p, N, S = lut_params(name, lut_mode=T.LUT_FP64)
+    mu, eps, sc, ab, nst, bins, _, _ = LUT_SETS[name]
+    ds = F32(S) / F32(N)
+    ref, _ = oracle.lut_f64(oracle.wparams(mu, eps, sc, ab, nst, bins), float(ds))
+    with T.Context(p) as ctx:
+        lut, _ = ctx.build_lut(ds)
+    assert np.max(np.abs(lut - ref) / ref) < 1.2e-7
+
+
+# ------------------------------------------------------------------------ weighting
+@pytest.mark.parametrize("name", sorted(LUT_SETS))
+def test_plain_weigher_matches_reference(name):
+    p, N, S = lut_params(name)
+    paths = golden_npz(f"paths_{name}.npz")
+    lut, info = golden_lut_info(name)
+    with T.Context(p) as ctx:
+        ctx.set_lut(lut, info)
+        w, v, b = ctx.weight_paths(geom_bc(N, S), paths["pos"], form=T.FORM_PLAIN_FP32, want_bins=True)
+    assert np.array_equal(v, paths["valid"])
+    assert np.array_equal(b, paths["bins"])                     # bit-exact bins
+    assert np.max(np.abs(w - paths["log10w"])) < 1e-12           # FP64 log10 may differ by an ulp
+
+
+@pytest.mark.parametrize("name", sorted(LUT_SETS))
+def test_compensated_weigher_matches_reference(name):
+    p, N, S = lut_params(name)
+    paths = golden_npz(f"paths_{name}.npz")
+    lut, info = golden_lut_info(name)
+    with T.Context(p) as ctx:
+        ctx.set_lut(lut, info)
+        w, v, b = ctx.weight_paths(geom_bc(N, S), paths["pos"], form=T.FORM_COMPENSATED, want_bins=True)
+    assert np.array_equal(v, paths["valid"])
+    # bins bit-exact except for curvatures within rounding of a bin edge
+    r = paths["curv"].astype(np.float64) / float(info.curvature_step)
+    near_edge = np.abs(r - np.round(r)) < 2e-3
+    mism = b != paths["bins"]
+    assert not np.any(mism & ~near_edge)
+    assert np.abs(b - paths["bins"]).max() <= 1
+    # per-path log10 weights within 1e-5 relative (paths with an edge flip move by one bin's step)
+    flip = mism.any(axis=1)
+    rel = np.abs(w - paths["log10w"]) / np.abs(paths["log10w"])
+    assert np.all(rel[~flip] < 1e-5), rel[~flip].max()
+
+
+# ---------------------------------------------------------------------------- chains
+def chain_ctx(name, form, seed=1234, chains=256, steps=200, burn=50, k_max=25, angle=float(F32(np.pi)), lut_ext=True):
+    p, N, S = lut_params(name, form=form, perturb_seed=seed, num_chains=chains, paths_to_generate=chains * steps,
+                         paths_to_skip=burn, max_sub_chain=k_max, max_angle=angle)
+    ctx = T.Context(p)
+    if lut_ext:
+        lut, info = golden_lut_info(name)
+        ctx.set_lut(lut, info)
+    boot = np.load(f"tests/golden/boot_{N}.npy")
+    ctx.set_initial_curve(boot)
+    return ctx, N, S, boot
+
+
+@pytest.mark.parametrize("name,angle", [("A", float(F32(np.pi))), ("C", float(F32(np.pi))), ("B", 0.05)])
+def test_plain_chains_bit_exact_with_oracle(oracle, name, angle):
+    ctx, N, S, boot = chain_ctx(name, T.FORM_PLAIN_FP32, angle=angle)
+    r = ctx.run(geom_bc(N, S))
+    ctx.close()
+    lut, info = golden_lut_info(name)
+    mu, eps, sc, ab, nst, bins, _, _ = LUT_SETS[name]
+    olut, meta = oracle.lut_f32(oracle.wparams(mu, eps, sc, ab, nst, bins), F32(S) / F32(N))
+    o = oracle.run_chains(boot, N, S, olut, meta, seed=1234, n_chains=256, steps=200, burn_in=50, k_max=25,
+                          max_angle=angle, absorption=ab)
+    ref = oracle.log10_sum(o["chain_log10"])
+    assert r.total_paths == int(o["chain_valid"].sum()) == 256 * 200
+    assert abs(r.log10_weight - ref) < 1e-11, (r.log10_weight, ref)
+
+
+def test_fp64_form_matches_oracle_twin(oracle):
+    name = "A"
+    ctx, N, S, boot = chain_ctx(name, T.FORM_FP64, angle=0.05, lut_ext=False)
+    ctx.update(lut_mode=T.LUT_FP64)
+    r = ctx.run(geom_bc(N, S))
+    ctx.close()
+    mu, eps, sc, ab, nst, bins, _, _ = LUT_SETS[name]
+    olut, meta = oracle.lut_f64(oracle.wparams(mu, eps, sc, ab, nst, bins), float(F32(S) / F32(N)))
+    o = oracle.run_chains(boot, N, S, olut, meta, seed=1234, n_chains=256, steps=200, burn_in=50, k_max=25,
+                          max_angle=0.05, f64=True)
+    assert abs(r.log10_weight - oracle.log10_sum(o["chain_log10"])) < 1e-9
+
+
+@pytest.mark.parametrize("name", ["A", "B"])
+def test_compensated_within_1e4_of_fp64(name):
+    """Small rotation angles keep FP32 and FP64 trajectories together: the compensated
+    estimate agrees with the FP64 form on the same proposals to better than 1e-4."""
+    res = {}
+    for form in (T.FORM_COMPENSATED, T.FORM_FP64):
+        p, N, S = lut_params(name, form=form, perturb_seed=99, num_chains=2048, paths_to_generate=2048 * 500,
+                             paths_to_skip=100, max_sub_chain=32, max_angle=0.1, lut_mode=T.LUT_FP64)
+        with T.Context(p) as ctx:
+            ctx.set_initial_curve(np.load(f"tests/golden/boot_{N}.npy"))
+            res[form] = ctx.run(geom_bc(N, S))
+    a, b = res[T.FORM_COMPENSATED], res[T.FORM_FP64]
+    assert a.total_paths == b.total_paths == 2048 * 500
+    rel = abs(10 ** (a.log10_weight - b.log10_weight) - 1)
+    assert rel < 1e-4, rel
+
+
+@pytest.mark.parametrize("N", [10, 18, 66])
+@pytest.mark.parametrize("form", [T.FORM_COMPENSATED, T.FORM_PLAIN_FP32])
+def test_statistics_match_reference_runner(N, form):
+    """MC estimate within 3 standard errors of the reference CPU runner's own run."""
+    rec = golden_json(f"chain_{N}.json")
+    ep = rec["config"]["experiment"]["experimentParams"]
+    w = ep["weighting"]
+    S = rec["config"]["experiment"]["basicExperiment"]["arclength"]
+    p = T.default_params(num_segments=N, mu=w["mu"], eps=w["eps"], scatter=w["scatter"], absorption=w["absorption"],
+                         num_steps_int=w["numStepsInt"], num_curvature_steps=w["numCurvatureSteps"], form=form,
+                         perturb_seed=2024, paths_to_generate=8_000_000, paths_to_skip=ep["pathsToSkip"],
+                         num_chains=8000, lut_mode=T.LUT_FAITHFUL)
+    with T.Context(p) as ctx:
+        ctx.set_initial_curve(np.load(f"tests/golden/boot_{N}.npy"))
+        r = ctx.run(geom_bc(N, S))
+    x = np.array([v for v, n in zip(rec["chunk_log10"], rec["chunk_paths"]) if n > 0])
+    m = x.max()
+    s = 10 ** (x - m)
+    ref_mean = m + np.log10(s.sum()) - np.log10(rec["paths"])
+    ref_se = np.sqrt(len(s) * s.var(ddof=1)) / s.sum()
+    got_mean = r.log10_mean_weight
+    tol = 3 * np.hypot(ref_se, r.rel_std_error) / np.log(10)
+    assert abs(got_mean - ref_mean) < tol, (got_mean, ref_mean, r.rel_std_error, ref_se)
+
+
+def test_runs_are_deterministic_and_split_api_matches():
+    p, N, S = lut_params("A", perturb_seed=7, paths_to_generate=300_000, paths_to_skip=10)
+    bc = geom_bc(N, S)
+    with T.Context(p) as ctx:
+        a = ctx.run(bc)
+        b = ctx.run(bc)
+        ctx.prepare(bc)
+        ctx.launch()
+        c = ctx.collect()
+        assert ctx.kernels_per_launch() == 2
+    assert a.log10_weight == b.log10_weight == c.log10_weight
+    assert a.total_paths == 300_000
+
+
+def test_runner_mirror_api():
+    cfg = golden_json("chain_66.json")["config"]
+    cfg["experiment"]["experimentParams"]["pathsToGenerate"] = 100_000
+    ep, bc = T.ParseExperimentParamsFromConfig(cfg)
+    res = T.FullExperimentRunnerOptimalPerturb(ep).RunExperiment(bc)
+    assert res.totalPathsGenerated == 100_000 and np.isfinite(res.experimentWeightLog10)
+    res2 = T.FullExperimentRunnerOptimalPerturbOptimized_GPU(ep).RunExperiment(bc)
+    assert res2.experimentWeightLog10 == res.experimentWeightLog10
+
+
+def test_normalizer_k4_matches_reference():
+    with T.Context(T.default_params(num_segments=4)) as ctx:
+        for rec in golden_json("norm.json"):
+            if rec["N"] != 4:
+                continue
+            b = rec["bc"]
+            bc = _abi.BC(_abi.Vec3(*b[0:3]), _abi.Vec3(*b[3:6]), _abi.Vec3(*b[6:9]), _abi.Vec3(*b[9:12]),
+                         rec["ds"] * 4)
+            assert ctx.normalizer_log10(4, rec["ds"], bc) == pytest.approx(rec["log10"], rel=1e-14, abs=1e-14)
+
+
+def test_error_statuses():
+    p, N, S = lut_params("A", paths_to_generate=1000)
+    with T.Context(p) as ctx:
+        with pytest.raises(T.TwistyError) as e:
+            ctx.run(T.make_bc((0, 0, 0), (1, 0, 0), (20, 0, 0), (1, 0, 0), 10.0))
+        assert e.value.status == _abi.ERR_INFEASIBLE_GEOMETRY
+        ctx.update(num_steps_int=2001)
+        with pytest.raises(T.TwistyError) as e:
+            ctx.run(geom_bc(N, S))
+        assert e.value.status == _abi.ERR_INVALID_CONFIG
+        ctx.update(num_steps_int=2000, perturb_method=1)
+        with pytest.raises(T.TwistyError) as e:
+            ctx.run(geom_bc(N, S))
+        assert e.value.status == _abi.ERR_UNSUPPORTED
+        ctx.update(perturb_method=0)
+        assert ctx.run(geom_bc(N, S)).total_paths == 1000   # the context stays usable

@@ -1,0 +1,48 @@
+// host_util.h -- host-side pieces of the runner that need no device: config parsing,
+// initial-curve construction, geometry checks, the closed-form normaliser.
+#pragma once
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/twisty_b200.h"
+
+namespace twisty {
+
+// A tiny document model shared by the JSON and YAML readers.
+struct Node {
+    enum Kind { Null, Bool, Number, String, Object, Array } kind = Null;
+    bool b = false;
+    double num = 0.0;
+    std::string str;
+    std::map<std::string, Node> obj;
+    std::vector<Node> arr;
+    const Node *get(const std::string &k) const;
+};
+
+bool parse_json(const std::string &text, Node &out, std::string &err);
+bool parse_yaml(const std::string &text, Node &out, std::string &err);
+
+// Fill params/bc from a parsed config (reference schema: experiment.experimentParams.*,
+// experiment.basicExperiment.*). Returns false with err set when a required key is
+// missing or has the wrong type.
+bool params_from_node(const Node &root, twisty_params &p, twisty_bc *bc, std::string &err);
+
+// CalculateMinimumArclength (Twisty/PathGeneration.cpp:12-43).
+float min_arclength(const twisty_bc &bc, uint32_t n);
+
+// Initial curve for any N >= 4: points 0, 1, N-1, N fixed by the boundary conditions
+// (Twisty/Curve.cpp:20-30), the N-2 free segments laid on a planar circular arc from
+// point 1 to point N-1 whose turning angle is solved by bisection so that every segment
+// has length exactly ds (computed in double, stored in float). The arc's plane is turned
+// about the chord by an angle drawn from the bootstrap seed. Returns false (err set) when
+// |x_{N-1} - x_1| > (N-2) ds.
+bool bootstrap_arc(const twisty_bc &bc, uint32_t n, uint32_t seed, std::vector<float> &pos, std::string &err);
+
+// K4 (Twisty/PathWeightUtils.cpp:643-651) and the z of Norm (:729-732), float math.
+double norm_k4_log10(float z, float ds);
+float norm_z(const twisty_bc &bc, float ds);
+
+}  // namespace twisty

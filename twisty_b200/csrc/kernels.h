@@ -1,0 +1,123 @@
+// kernels.h -- launch interface between the host runtime (runtime.cpp) and the CUDA
+// translation units. Plain structs and host functions only; each launcher enqueues on the
+// given stream and returns the launch error.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace twisty {
+
+// One Monte Carlo pass over one experiment.
+struct ChainSpec {
+    uint32_t n_segments;     // N
+    float arclength;         // S
+    float ds;                // S/N (float, as the reference: FullExperimentRunnerOptimalPerturb.cpp:57)
+    float inv_ds;            // (float)N / S (CurvePerturbUtils.cpp:160)
+    uint64_t seed;
+    uint32_t experiment;     // Philox stream id
+    uint32_t chain0;         // global id of chain 0
+    uint32_t n_chains;
+    uint32_t steps;          // weighted steps of every chain but the last
+    uint32_t last_steps;     // weighted steps of the last chain
+    uint32_t burn_in;        // unweighted steps at the start of every chain
+    uint32_t k_eff;          // min(k_max, N-2)
+    float max_angle;
+    double absorption_factor;// exp(-mu_a * ds) as the reference computes it (float exp, promoted)
+    float eval_shift[3];     // receiver shift applied only when weighting
+    int has_eval_shift;
+};
+
+// Float table metadata (BaseWeightLookupTable accessors).
+struct LutMetaF {
+    float min_k, max_k, step;
+    int32_t bins;
+};
+
+// Per-chain outcome, identical for every form.
+struct ChainOut {
+    double log10_sum;        // log10 of the chain's summed path weights (-inf if none)
+    uint32_t valid;          // weighted paths with a finite weight
+    uint32_t failed;         // NaN weights
+    uint32_t clamped;        // curvatures outside the table, clamped
+    uint32_t pad;
+};
+
+// Result of the FP64 global reduction.
+struct ReduceOut {
+    double log10_sum;        // log10 sum over chains
+    double rel_se;           // standard error of the sum / the sum (spread over chains)
+    double max_chain_log10;
+    uint64_t valid, failed, clamped;
+};
+
+// ---------------------------------------------------------------- tables (lut.cu)
+// Simpson quadrature of the reference's table (PathWeightUtils.cpp:281-433) in FP64:
+// faithful=1 reproduces the reference's float phase function and float-pi constants,
+// faithful=0 is double throughout. Writes out64[bins] (nullable) and out32[bins] (nullable).
+struct LutBuildSpec {
+    float mu, eps, scatter, min_bound, max_bound, bias;
+    uint32_t num_steps_int;
+    uint32_t bins;
+    float ds;
+    float min_k, step;       // the float grid (faithful) ...
+    double step64;           // ... and its double twin
+    int faithful;
+    int derivatives;         // also d/d(mu_s) and d/d(eps) tables (adjoint)
+};
+cudaError_t launch_lut_build(const LutBuildSpec &s, double *out64, double *d_mus, double *d_eps,
+                             cudaStream_t st);
+// Non-positive entries replaced by the smallest non-negative one (PathWeightUtils.cpp:
+// 327-344); min/max returned through minmax[2]; float copy written to out32.
+cudaError_t launch_lut_finalize(uint32_t bins, double *lut64, float *out32, double *minmax, cudaStream_t st);
+// Compensated-form table: per bin (log10 L_i, secant slope in log10 per curvature unit).
+cudaError_t launch_lut_logtable(uint32_t bins, const float *lut32, float step, float2 *out,
+                                double *max_err, cudaStream_t st);
+
+// ------------------------------------------------------------- chains (chain_*.cu)
+cudaError_t launch_plain_chains(const ChainSpec &c, const float *init_pos, float *state,
+                                const float *lut, LutMetaF m, ChainOut *out, cudaStream_t st);
+// Plain-form state of one chain: positions (N+1)*3, tangents N*3, curvatures N-1,
+// padded to a multiple of 4 floats.
+__host__ __device__ inline size_t plain_state_floats_per_chain(uint32_t n)
+{
+    const size_t f = 3 * (size_t)(n + 1) + 3 * (size_t)n + (n - 1);
+    return (f + 3) & ~(size_t)3;
+}
+
+cudaError_t launch_fp64_chains(const ChainSpec &c, const float *init_pos, double *state,
+                               const double *lut, double min_k, double max_k, double step,
+                               int32_t bins, ChainOut *out, cudaStream_t st);
+
+// Compensated form. init_seg holds the N initial segment vectors (float3, x_{i+1}-x_i).
+struct CompTuning {
+    int group;               // lanes per chain (4, 8, 16, 32)
+    int spl;                 // segments per lane
+    int warps_per_block;
+    int exact_blend;         // 1: interpolate the linear table and take log2 (MUFU)
+};
+CompTuning comp_default_tuning(uint32_t n_segments);
+bool comp_tuning_supported(const CompTuning &t, uint32_t n_segments, uint32_t k_eff);
+uint32_t comp_default_chains(uint32_t n_segments, int sm_count);
+size_t comp_smem_bytes(const CompTuning &t, uint32_t bins);
+cudaError_t launch_comp_chains(const ChainSpec &c, const CompTuning &t, const float *init_seg,
+                               const float2 *logtab, const float2 *lintab, LutMetaF m,
+                               ChainOut *out, double2 *block_partials, cudaStream_t st);
+uint32_t comp_blocks(const ChainSpec &c, const CompTuning &t);
+
+// ----------------------------------------------------------- reduction (chain_plain.cu)
+cudaError_t launch_reduce(const ChainOut *chains, uint32_t n, ReduceOut *out, cudaStream_t st);
+
+// ------------------------------------------------------------- weighting of given paths
+cudaError_t launch_weigh_plain(const float *pos, uint64_t n_paths, uint32_t n_segments, float inv_ds,
+                               const float *lut, LutMetaF m, double absorption_factor,
+                               double *log10w, uint8_t *valid, int32_t *bins, cudaStream_t st);
+cudaError_t launch_weigh_comp(const float *pos, uint64_t n_paths, uint32_t n_segments, float inv_ds,
+                              const float2 *logtab, const float2 *lintab, int exact_blend, LutMetaF m,
+                              double log10_absorption, double *log10w, uint8_t *valid, int32_t *bins,
+                              cudaStream_t st);
+
+// ------------------------------------------------------------ normaliser (norm.cu)
+uint32_t norm_partial_blocks();
+cudaError_t launch_norm_k56(float z, float ds, double *partials, double *out, cudaStream_t st);
+
+}  // namespace twisty

@@ -1,0 +1,275 @@
+// lut.cu -- weight lookup tables, built on the device in FP64.
+//
+// The reference builds its table with an OpenMP loop over bins, each bin a composite
+// Simpson quadrature of IntegrandRT whose terms are sorted then summed
+// (Twisty/PathWeightUtils.cpp:281-433). Here one CTA integrates one bin: every thread
+// takes a strided share of the nodes and keeps a Neumaier-compensated FP64 sum, and the
+// CTA combines the partial sums pairwise. The compensated sum replaces the sort (it is
+// at least as accurate), so the float table matches the reference's to within one float
+// ulp rather than bit for bit.
+//
+// The node set keeps the reference's rule exactly: weights h/3 * {1, 4, 2, ..., 4, 2, 1}
+// with the odd loop ending at node n-3 and the even loop at n-4 (nodes n-2 and n-1 are
+// dropped), and the config mu/eps swap of IntegrandRT's call (PathWeightUtils.cpp:401).
+#include "kernels.h"
+#include "device_common.cuh"
+
+#include <cfloat>
+#include <math_constants.h>
+
+namespace twisty {
+namespace {
+
+constexpr int kLutThreads = 256;
+
+struct Integrand {
+    double kds, bds, reg, m;   // reg = config mu, m = config eps (phase parameter)
+    int faithful;
+    float np_f;                // float phase normaliser (faithful)
+    double np_d, dlnnp_dm;     // double phase normaliser and its log-derivative in m
+};
+
+__device__ __forceinline__ double phase(const Integrand &g, double p)
+{
+    if (g.faithful) {
+        // GaussianPhase / SimpleGaussianPhase in float (PathWeightUtils.cpp:19-33)
+        const float pf = (float)p, mf = (float)g.m;
+        const float val = __fmul_rn(__fmul_rn(__fmul_rn(-mf, pf), pf), 0.5f);
+        return (double)__fmul_rn(g.np_f, expf(val));
+    }
+    return g.np_d * exp(-g.m * p * p * 0.5);
+}
+
+// f(p) = p exp(bds*phase(p) - reg^2 p^2/2) * sin(kds p)/kds   (IntegrandRT, :350-369)
+__device__ __forceinline__ double integrand(const Integrand &g, double p)
+{
+    const double ph = phase(g, p);
+    const double scattering = p * exp(g.bds * ph - 1.0 * (g.reg * g.reg * p * p * 0.5));
+    return scattering * (g.kds > 0.0 ? sin(g.kds * p) / g.kds : p);
+}
+
+// Derivatives of f (double form): df/dbds, df/dp, df/dm.
+__device__ __forceinline__ void integrand_derivs(const Integrand &g, double p, double &f, double &f_bds,
+                                                 double &f_p, double &f_m)
+{
+    const double ph = g.np_d * exp(-g.m * p * p * 0.5);
+    const double e = exp(g.bds * ph - g.reg * g.reg * p * p * 0.5);
+    double s, sp;
+    if (g.kds > 0.0) {
+        double sn, cs;
+        sincos(g.kds * p, &sn, &cs);
+        s = sn / g.kds;
+        sp = cs;
+    } else {
+        s = p;
+        sp = 1.0;
+    }
+    f = p * e * s;
+    f_bds = f * ph;
+    const double ph_p = -g.m * p * ph;
+    f_p = e * s + p * e * (g.bds * ph_p - g.reg * g.reg * p) * s + p * e * sp;
+    const double ph_m = ph * (g.dlnnp_dm - 0.5 * p * p);
+    f_m = f * g.bds * ph_m;
+}
+
+struct Neumaier {
+    double s = 0.0, c = 0.0;
+    __device__ __forceinline__ void add(double x)
+    {
+        const double t = s + x;
+        c += (fabs(s) >= fabs(x)) ? (s - t) + x : (x - t) + s;
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return s + c; }
+};
+
+__device__ double block_sum(double v, double *red)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (w == 0) {
+        r = (l < (int)(blockDim.x >> 5)) ? red[l] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+    }
+    return r;  // valid in thread 0
+}
+
+__global__ void __launch_bounds__(kLutThreads) lut_build_kernel(LutBuildSpec s, double *out64,
+                                                                 double *d_mus, double *d_eps)
+{
+    __shared__ double red[kLutThreads / 32];
+    const uint32_t bin = blockIdx.x;
+    const uint32_t n = s.num_steps_int;
+    Integrand g;
+    g.faithful = s.faithful;
+    g.reg = (double)s.mu;
+    g.m = (double)s.eps;
+    double h, weight, start, maxb, tp;
+    if (s.faithful) {
+        const float kappa = __fadd_rn(s.min_k, __fmul_rn((float)bin, s.step));
+        g.kds = (double)__fmul_rn(kappa, s.ds);
+        g.bds = (double)__fmul_rn(s.scatter, s.ds);
+        g.np_f = __fdiv_rn(__fsqrt_rn(__fmul_rn(__fmul_rn(dev::kPiF, s.eps), 0.5f)),
+                           __fsub_rn(1.0f, expf(__fdiv_rn(-2.0f, s.eps))));
+        h = (double)__fdiv_rn(__fsub_rn(s.max_bound, s.min_bound), (float)n);
+        weight = (double)(1.0f / 3.0f) * h;
+        start = (double)s.min_bound;
+        maxb = (double)s.max_bound;
+        tp = (double)dev::kPiF;
+    } else {
+        const double ds = (double)s.ds;
+        g.kds = (double)bin * s.step64 * ds;
+        g.bds = (double)s.scatter * ds;
+        maxb = 10.0 / (double)s.eps;
+        h = maxb / (double)n;
+        weight = h / 3.0;
+        start = 0.0;
+        tp = CUDART_PI;
+    }
+    const double em = exp(-2.0 / g.m);
+    g.np_d = sqrt((CUDART_PI * g.m) * 0.5) / (1.0 - em);
+    g.dlnnp_dm = 0.5 / g.m - (2.0 / (g.m * g.m)) * em / (1.0 - em);
+
+    Neumaier acc, acc_mus, acc_eps;
+    for (uint32_t j = threadIdx.x; j <= n; j += blockDim.x) {
+        double c;
+        if (j == 0 || j == n) c = 1.0;
+        else if (j >= n - 2) c = 0.0;            // dropped nodes n-2, n-1
+        else c = (j & 1u) ? 4.0 : 2.0;
+        if (c == 0.0) continue;
+        const double p = (j == n) ? maxb : start + (double)j * h;
+        if (s.derivatives && !s.faithful) {
+            double f, f_bds, f_p, f_m;
+            integrand_derivs(g, p, f, f_bds, f_p, f_m);
+            acc.add(c * f);
+            acc_mus.add(c * f_bds);
+            acc_eps.add(c * (-p * f_p / g.m + f_m));
+        } else {
+            acc.add(integrand(g, p) * weight * c);
+        }
+    }
+    const double total = block_sum(acc.value(), red);
+    if (s.derivatives && !s.faithful) {
+        const double t_mus = block_sum(acc_mus.value(), red);
+        const double t_eps = block_sum(acc_eps.value(), red);
+        if (threadIdx.x == 0) {
+            const double scale = weight / (2.0 * tp * tp) * (double)s.bias;
+            const double I = total * scale;
+            out64[bin] = I;
+            // d/d(mu_s): bds = mu_s * ds
+            d_mus[bin] = t_mus * scale * (double)s.ds;
+            // d/d(eps): h and every node move with maxBound = 10/eps
+            d_eps[bin] = -I / g.m + t_eps * scale;
+        }
+    } else if (threadIdx.x == 0) {
+        out64[bin] = (total / (2.0 * tp * tp)) * (double)s.bias;
+    }
+}
+
+// Replace non-positive entries by the smallest non-negative one and emit the float copy
+// (WeightLookupTableIntegral::Initialize, PathWeightUtils.cpp:305-347).
+__global__ void __launch_bounds__(1024) lut_finalize_kernel(uint32_t bins, double *lut, float *out32,
+                                                            double *minmax)
+{
+    __shared__ double smin[32], smax[32];
+    __shared__ int sarg[32];
+    // The reference keeps entries in float, so min/max selection runs on the float values.
+    double mn = (double)(float)lut[0], mx = mn;
+    int arg = 0;
+    for (uint32_t i = 1 + threadIdx.x; i < bins; i += blockDim.x) {
+        const double v = (double)(float)lut[i];
+        if (v < mn && v >= 0.0) { mn = v; arg = (int)i; }
+        if (v > mx && v >= 0.0) mx = v;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const double omn = __shfl_xor_sync(0xffffffffu, mn, o);
+        const int oarg = __shfl_xor_sync(0xffffffffu, arg, o);
+        if (omn < mn || (omn == mn && oarg < arg)) { mn = omn; arg = oarg; }
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { smin[w] = mn; smax[w] = mx; sarg[w] = arg; }
+    __syncthreads();
+    if (w == 0) {
+        const int nw = blockDim.x >> 5;
+        mn = l < nw ? smin[l] : DBL_MAX;
+        mx = l < nw ? smax[l] : -DBL_MAX;
+        arg = l < nw ? sarg[l] : 0;
+        for (int o = 16; o > 0; o >>= 1) {
+            const double omn = __shfl_xor_sync(0xffffffffu, mn, o);
+            const int oarg = __shfl_xor_sync(0xffffffffu, arg, o);
+            if (omn < mn || (omn == mn && oarg < arg)) { mn = omn; arg = oarg; }
+            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        }
+        if (l == 0) { smin[0] = mn; smax[0] = mx; sarg[0] = arg; }
+    }
+    __syncthreads();
+    mn = smin[0];
+    const double mn64 = lut[sarg[0]];
+    for (uint32_t i = threadIdx.x; i < bins; i += blockDim.x) {
+        double v = lut[i];
+        if ((float)v <= 0.0f) v = mn64;
+        lut[i] = v;
+        if (out32) out32[i] = (float)v;
+    }
+    if (threadIdx.x == 0 && minmax) {
+        minmax[0] = mn;
+        minmax[1] = smax[0];
+        minmax[2] = (double)sarg[0];
+    }
+}
+
+__device__ __forceinline__ void atomic_max_nonneg(double *addr, double v)
+{
+    // Non-negative doubles order like their bit patterns.
+    atomicMax(reinterpret_cast<unsigned long long *>(addr), (unsigned long long)__double_as_longlong(v));
+}
+
+// Per bin: (log10 L_i, secant slope of log10(blend) over the bin in curvature units).
+// With the reference's interpolation weight in curvature units (PathWeighters.cpp:79-82),
+// the blend over bin i is L_i (1 + d (L_{i+1}/L_i - 1)) for d in [0, step); the secant
+// through d = 0 and d = step has error at most (step (L_{i+1}/L_i - 1))^2 / (8 ln 10),
+// reported through max_err so the caller can fall back to the exact blend.
+__global__ void lut_logtable_kernel(uint32_t bins, const float *lut32, float step, float2 *out, double *max_err)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= bins) return;
+    const double li = (double)lut32[i];
+    double slope = 0.0, err = 0.0;
+    if (i + 1 < bins) {
+        const double a = (double)lut32[i + 1] / li - 1.0;
+        const double st = (double)step;
+        slope = log10(1.0 + st * a) / st;
+        err = (st * a) * (st * a) / (8.0 * 2.302585092994046);
+    }
+    out[i] = make_float2((float)log10(li), (float)slope);
+    if (max_err) atomic_max_nonneg(max_err, err);
+}
+
+}  // namespace
+
+cudaError_t launch_lut_build(const LutBuildSpec &s, double *out64, double *d_mus, double *d_eps, cudaStream_t st)
+{
+    if (s.bins < 2 || s.num_steps_int < 4 || (s.num_steps_int & 1u)) return cudaErrorInvalidValue;
+    lut_build_kernel<<<s.bins, kLutThreads, 0, st>>>(s, out64, d_mus, d_eps);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lut_finalize(uint32_t bins, double *lut64, float *out32, double *minmax, cudaStream_t st)
+{
+    lut_finalize_kernel<<<1, 1024, 0, st>>>(bins, lut64, out32, minmax);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lut_logtable(uint32_t bins, const float *lut32, float step, float2 *out, double *max_err,
+                                cudaStream_t st)
+{
+    lut_logtable_kernel<<<(bins + 255) / 256, 256, 0, st>>>(bins, lut32, step, out, max_err);
+    return cudaGetLastError();
+}
+
+}  // namespace twisty

@@ -1,0 +1,773 @@
+// runtime.cu -- implementation of the C ABI in include/twisty_b200.h.
+//
+// Owns the device state of one context: the weight tables for the current ds (cached by
+// their parameters), the initial curve, the per-chain state and outputs, and the events
+// that time each phase. Host code only; the kernels live in lut.cu, chain_*.cu, norm.cu.
+// No exception leaves an entry point: every body runs under guard().
+#include "kernels.h"
+#include "host_util.h"
+#include "../../include/twisty_b200.h"
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <functional>
+#include <limits>
+#include <new>
+#include <sstream>
+#include <string>
+#include <vector>
+
+using namespace twisty;
+
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t n)
+    {
+        if (n <= bytes && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, n ? n : 16);
+        if (e == cudaSuccess) bytes = n ? n : 16;
+        return e;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T>
+    T *as() const { return static_cast<T *>(p); }
+};
+
+struct Failure {
+    twisty_status s;
+    std::string msg;
+};
+
+[[noreturn]] void fail(twisty_status s, const std::string &m) { throw Failure{s, m}; }
+
+void ck(cudaError_t e, const char *what)
+{
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fail(e == cudaErrorMemoryAllocation ? TWISTY_ERR_OUT_OF_MEMORY : TWISTY_ERR_CUDA,
+             std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+double now_ms()
+{
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+uint64_t seed_of(uint32_t s)
+{
+    // ProcessRandomSeed (Twisty/ExperimentRunner.cpp:40-46): seed 0 means the wall clock.
+    return s ? (uint64_t)s : (uint64_t)time(nullptr);
+}
+
+}  // namespace
+
+struct twisty_ctx {
+    twisty_params p{};
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    std::string err;
+
+    // tables for the current key
+    bool lut_ready = false;
+    uint64_t lut_key[4] = {0, 0, 0, 0};
+    DevBuf lut64, lut32, logtab, lintab, dmus, deps, lutaux;
+    LutMetaF meta{};
+    double min_w = 0, max_w = 0, logtab_err = 0;
+    int exact_blend = 0;
+    std::vector<float> ext_lut;
+    twisty_lut_info ext_info{};
+
+    // the prepared experiment
+    bool prepared = false;
+    twisty_bc bc{};
+    ChainSpec spec{};
+    CompTuning tuning{};
+    double log10_norm = 0.0;
+    double setup_ms = 0.0;
+    double prepare_start = 0.0;
+    std::vector<float> user_curve;
+    std::vector<float> init_pos_host;
+    DevBuf init_pos, init_seg, state, chain_out, partials, reduce_out, norm_scratch;
+    uint32_t kernels_per_launch = 0;
+    bool launched = false;
+};
+
+namespace {
+
+twisty_status guard(twisty_ctx *ctx, const std::function<void()> &f);
+
+void validate(const twisty_params &p)
+{
+    if (p.struct_size != sizeof(twisty_params)) fail(TWISTY_ERR_INVALID_ARGUMENT, "twisty_params.struct_size mismatch (call twisty_params_init)");
+    if (p.num_segments < 4) fail(TWISTY_ERR_INVALID_CONFIG, "numSegments must be at least 4");
+    if (p.num_segments > 1024 && p.form == TWISTY_FORM_COMPENSATED) fail(TWISTY_ERR_INVALID_CONFIG, "the compensated form supports numSegments <= 1024");
+    if (p.num_curvature_steps < 2) fail(TWISTY_ERR_INVALID_CONFIG, "numCurvatureSteps must be at least 2");
+    if (p.lut_mode != TWISTY_LUT_EXTERNAL && (p.num_steps_int < 4 || (p.num_steps_int & 1u)))
+        fail(TWISTY_ERR_INVALID_CONFIG, "numStepsInt must be even and at least 4");
+    if (p.lut_mode != TWISTY_LUT_EXTERNAL && !(p.eps > 0.0f)) fail(TWISTY_ERR_INVALID_CONFIG, "weighting.eps must be positive");
+    if (p.form < 0 || p.form > 2) fail(TWISTY_ERR_INVALID_CONFIG, "unknown form");
+    if (p.lut_mode < 0 || p.lut_mode > 2) fail(TWISTY_ERR_INVALID_CONFIG, "unknown lut_mode");
+    if (p.perturb_method != 0) fail(TWISTY_ERR_UNSUPPORTED, "only perturbMethod 0 (GeometricRandom) runs; the reference exits on the others");
+    if (p.weight_function != 0) fail(TWISTY_ERR_UNSUPPORTED, "only weightFunction 0 (radiative transfer) is implemented on the device");
+    if (p.max_sub_chain < 2) fail(TWISTY_ERR_INVALID_CONFIG, "max_sub_chain must be at least 2");
+    if (!(p.max_angle >= 0.0f) || p.max_angle > 3.1415927f) fail(TWISTY_ERR_INVALID_CONFIG, "max_angle must be in [0, pi]");
+}
+
+void validate_bc(const twisty_bc *bc)
+{
+    if (!bc) fail(TWISTY_ERR_INVALID_ARGUMENT, "bc is NULL");
+    if (!(bc->arclength > 0.0f) || !std::isfinite(bc->arclength)) fail(TWISTY_ERR_INVALID_CONFIG, "arclength must be positive");
+    auto unit = [](const twisty_vec3 &v) {
+        const double l = std::sqrt((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
+        return std::fabs(l - 1.0) < 1e-3;
+    };
+    if (!unit(bc->start_dir) || !unit(bc->end_dir)) fail(TWISTY_ERR_INVALID_CONFIG, "start_dir and end_dir must be unit vectors");
+}
+
+void set_device(twisty_ctx *ctx) { ck(cudaSetDevice(ctx->device), "cudaSetDevice"); }
+
+// ------------------------------------------------------------------ tables
+void build_tables(twisty_ctx *ctx, float ds, bool derivatives)
+{
+    const twisty_params &p = ctx->p;
+    const uint32_t bins = p.num_curvature_steps;
+    uint64_t key[4];
+    uint32_t dsb;
+    std::memcpy(&dsb, &ds, 4);
+    uint32_t f[6];
+    std::memcpy(&f[0], &p.mu, 4);
+    std::memcpy(&f[1], &p.eps, 4);
+    std::memcpy(&f[2], &p.scatter, 4);
+    std::memcpy(&f[3], &p.bias, 4);
+    std::memcpy(&f[4], &p.max_bound, 4);
+    std::memcpy(&f[5], &p.min_bound, 4);
+    key[0] = ((uint64_t)dsb << 32) | (uint64_t)(uint32_t)p.lut_mode;
+    key[1] = ((uint64_t)f[0] << 32) | f[1];
+    key[2] = ((uint64_t)f[2] << 32) | f[3];
+    key[3] = ((uint64_t)f[4] << 32) ^ ((uint64_t)f[5]) ^ ((uint64_t)bins << 8) ^ ((uint64_t)p.num_steps_int << 40) ^
+             (derivatives ? 1ull : 0ull);
+    if (ctx->lut_ready && std::memcmp(key, ctx->lut_key, sizeof(key)) == 0) return;
+    ctx->lut_ready = false;
+    cudaStream_t st = ctx->stream;
+    ck(ctx->lut32.ensure(sizeof(float) * bins), "alloc table");
+    ck(ctx->logtab.ensure(sizeof(float2) * bins), "alloc log table");
+    ck(ctx->lintab.ensure(sizeof(float2) * bins), "alloc linear table");
+    ck(ctx->lutaux.ensure(sizeof(double) * 4), "alloc table scratch");
+    std::vector<float> host32(bins);
+    if (p.lut_mode == TWISTY_LUT_EXTERNAL) {
+        if (ctx->ext_lut.size() != bins) fail(TWISTY_ERR_LUT_INVALID, "no external table of numCurvatureSteps entries was set (twisty_set_lut)");
+        host32 = ctx->ext_lut;
+        ctx->meta = LutMetaF{ctx->ext_info.min_curvature, ctx->ext_info.max_curvature, ctx->ext_info.curvature_step, (int32_t)bins};
+        ctx->min_w = ctx->ext_info.min_segment_weight;
+        ctx->max_w = ctx->ext_info.max_segment_weight;
+        ck(cudaMemcpyAsync(ctx->lut32.p, host32.data(), sizeof(float) * bins, cudaMemcpyHostToDevice, st), "upload table");
+        ck(ctx->lut64.ensure(sizeof(double) * bins), "alloc table");
+        std::vector<double> h64(host32.begin(), host32.end());
+        ck(cudaMemcpyAsync(ctx->lut64.p, h64.data(), sizeof(double) * bins, cudaMemcpyHostToDevice, st), "upload table");
+        ck(cudaStreamSynchronize(st), "sync");
+    } else {
+        // WeightLookupTableIntegral ctor (PathWeightUtils.cpp:281-289), float grid
+        const float min_k = 0.0f;
+        const float max_k = (float)((2.0 / (double)ds) * (double)1.01f);
+        const float step = (max_k - min_k) / (float)(bins - 1);
+        LutBuildSpec s{};
+        s.mu = p.mu;
+        s.eps = p.eps;
+        s.scatter = p.scatter;
+        s.min_bound = p.min_bound;
+        s.max_bound = p.max_bound;
+        s.bias = p.bias;
+        s.num_steps_int = p.num_steps_int;
+        s.bins = bins;
+        s.ds = ds;
+        s.min_k = min_k;
+        s.step = step;
+        s.step64 = ((2.0 / (double)ds) * 1.01) / (double)(bins - 1);
+        s.faithful = (p.lut_mode == TWISTY_LUT_FAITHFUL) ? 1 : 0;
+        s.derivatives = derivatives ? 1 : 0;
+        if (derivatives && s.faithful) fail(TWISTY_ERR_UNSUPPORTED, "derivative tables need lut_mode FP64");
+        ck(ctx->lut64.ensure(sizeof(double) * bins), "alloc table");
+        if (derivatives) {
+            ck(ctx->dmus.ensure(sizeof(double) * bins), "alloc derivative table");
+            ck(ctx->deps.ensure(sizeof(double) * bins), "alloc derivative table");
+        }
+        ck(launch_lut_build(s, ctx->lut64.as<double>(), ctx->dmus.as<double>(), ctx->deps.as<double>(), st), "table build");
+        ck(launch_lut_finalize(bins, ctx->lut64.as<double>(), ctx->lut32.as<float>(), ctx->lutaux.as<double>(), st),
+           "table finalize");
+        double mm[3];
+        ck(cudaMemcpyAsync(mm, ctx->lutaux.p, sizeof(double) * 3, cudaMemcpyDeviceToHost, st), "read table range");
+        ck(cudaMemcpyAsync(host32.data(), ctx->lut32.p, sizeof(float) * bins, cudaMemcpyDeviceToHost, st), "read table");
+        ck(cudaStreamSynchronize(st), "table build");
+        ctx->min_w = mm[0];
+        ctx->max_w = mm[1];
+        ctx->meta = LutMetaF{min_k, max_k, step, (int32_t)bins};
+    }
+    for (uint32_t i = 0; i < bins; ++i)
+        if (!std::isfinite(host32[i])) fail(TWISTY_ERR_LUT_INVALID, "weight table has non-finite entries");
+    // compensated-form tables
+    ck(cudaMemsetAsync(ctx->lutaux.p, 0, sizeof(double), st), "memset");
+    ck(launch_lut_logtable(bins, ctx->lut32.as<float>(), ctx->meta.step, ctx->logtab.as<float2>(), ctx->lutaux.as<double>(), st),
+       "log table");
+    std::vector<float2> lin(bins);
+    for (uint32_t i = 0; i < bins; ++i) {
+        const float a = host32[i], b = host32[i + 1 < bins ? i + 1 : i];
+        lin[i] = make_float2(a, b - a);
+    }
+    ck(cudaMemcpyAsync(ctx->lintab.p, lin.data(), sizeof(float2) * bins, cudaMemcpyHostToDevice, st), "upload linear table");
+    double err = 0;
+    ck(cudaMemcpyAsync(&err, ctx->lutaux.p, sizeof(double), cudaMemcpyDeviceToHost, st), "read table error");
+    ck(cudaStreamSynchronize(st), "tables");
+    ctx->logtab_err = err;
+    // The secant form is used only when its worst-case error is below 1e-7 per segment.
+    ctx->exact_blend = (err > 1e-7) ? 1 : 0;
+    std::memcpy(ctx->lut_key, key, sizeof(key));
+    ctx->lut_ready = true;
+}
+
+// -------------------------------------------------------------- normaliser
+double normalizer_log10(twisty_ctx *ctx, uint32_t n, float ds, const twisty_bc &bc)
+{
+    if (n == 4) return norm_k4_log10(norm_z(bc, ds), ds);
+    if (n == 5 || n == 6) {
+        const uint32_t blocks = norm_partial_blocks();
+        ck(ctx->norm_scratch.ensure(sizeof(double) * (blocks + 1)), "alloc normaliser scratch");
+        double *d = ctx->norm_scratch.as<double>();
+        ck(launch_norm_k56(norm_z(bc, ds), ds, d + 1, d, ctx->stream), "normaliser");
+        double v = 0.0;
+        ck(cudaMemcpyAsync(&v, d, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "read normaliser");
+        ck(cudaStreamSynchronize(ctx->stream), "normaliser");
+        return std::log10(v);
+    }
+    return 0.0;  // Norm returns 1.0 for any other N (PathWeightUtils.cpp:745-750)
+}
+
+// ------------------------------------------------------------ chain layout
+void layout(twisty_ctx *ctx, uint64_t paths, uint32_t requested, uint32_t max_steps)
+{
+    ChainSpec &c = ctx->spec;
+    if (paths == 0) {
+        c.n_chains = 0;
+        c.steps = 0;
+        c.last_steps = 0;
+        return;
+    }
+    uint64_t C = requested ? requested : 1;
+    if (C > paths) C = paths;
+    uint64_t L = (paths + C - 1) / C;
+    if (L > max_steps) {
+        L = max_steps;
+    }
+    C = (paths + L - 1) / L;
+    if (C > 0xFFFFFFFFull) fail(TWISTY_ERR_INVALID_CONFIG, "too many chains");
+    c.n_chains = (uint32_t)C;
+    c.steps = (uint32_t)L;
+    c.last_steps = (uint32_t)(paths - (C - 1) * L);
+}
+
+void prepare(twisty_ctx *ctx, const twisty_bc *bcp)
+{
+    const double t0 = now_ms();
+    validate(ctx->p);
+    validate_bc(bcp);
+    set_device(ctx);
+    const twisty_params &p = ctx->p;
+    const twisty_bc bc = *bcp;
+    const uint32_t N = p.num_segments;
+    const float ds = bc.arclength / (float)N;
+    build_tables(ctx, ds, false);
+    ctx->log10_norm = normalizer_log10(ctx, N, ds, bc);
+    // initial curve
+    std::vector<float> pos;
+    if (!ctx->user_curve.empty()) {
+        if (ctx->user_curve.size() != 3 * (size_t)(N + 1)) fail(TWISTY_ERR_INVALID_ARGUMENT, "initial curve has the wrong number of points");
+        pos = ctx->user_curve;
+    } else {
+        std::string e;
+        if (!bootstrap_arc(bc, N, p.bootstrap_seed, pos, e)) fail(TWISTY_ERR_INFEASIBLE_GEOMETRY, e);
+    }
+    ctx->init_pos_host = pos;
+    std::vector<float> seg(3 * (size_t)N);
+    for (uint32_t i = 0; i < N; ++i)
+        for (int k = 0; k < 3; ++k) seg[3 * i + k] = pos[3 * (i + 1) + k] - pos[3 * i + k];
+
+    ChainSpec &c = ctx->spec;
+    c = ChainSpec{};
+    c.n_segments = N;
+    c.arclength = bc.arclength;
+    c.ds = ds;
+    c.inv_ds = (float)N / bc.arclength;
+    c.seed = seed_of(p.perturb_seed);
+    c.experiment = p.experiment_id;
+    c.chain0 = p.chain_offset;
+    c.burn_in = (uint32_t)std::min<uint64_t>(p.paths_to_skip, 0xFFFFFFFFull);
+    c.k_eff = std::min<uint32_t>(p.max_sub_chain, N - 2);
+    c.max_angle = p.max_angle;
+    c.absorption_factor = (double)std::exp(-p.absorption * ds);
+    c.eval_shift[0] = p.eval_end_shift.x;
+    c.eval_shift[1] = p.eval_end_shift.y;
+    c.eval_shift[2] = p.eval_end_shift.z;
+    c.has_eval_shift = (p.eval_end_shift.x != 0.f || p.eval_end_shift.y != 0.f || p.eval_end_shift.z != 0.f) ? 1 : 0;
+
+    uint32_t requested = p.num_chains;
+    uint32_t max_steps = 0xFFFFFFFFu - c.burn_in;
+    if (p.form == TWISTY_FORM_PLAIN_FP32) {
+        if (!requested) requested = (uint32_t)ctx->sm_count * 256;
+        // one CombinedWeightValues_C per chain holds at most 1e6 paths (CombinedWeightUtils.h:22-24)
+        max_steps = std::min<uint32_t>(max_steps, 1000000u);
+    } else if (p.form == TWISTY_FORM_COMPENSATED) {
+        ctx->tuning = comp_default_tuning(N);
+        ctx->tuning.exact_blend = ctx->exact_blend;
+        if (!comp_tuning_supported(ctx->tuning, N, c.k_eff)) fail(TWISTY_ERR_UNSUPPORTED, "no compensated kernel shape for this N / max_sub_chain");
+        const size_t smem = comp_smem_bytes(ctx->tuning, p.num_curvature_steps);
+        if (smem > 227 * 1024) fail(TWISTY_ERR_UNSUPPORTED, "weight table too large to stage in shared memory");
+        if (!requested) requested = comp_default_chains(N, 148);
+    } else {
+        if (!requested) requested = (uint32_t)ctx->sm_count * 256;
+    }
+    layout(ctx, p.paths_to_generate, requested, max_steps);
+
+    cudaStream_t st = ctx->stream;
+    ck(ctx->init_pos.ensure(sizeof(float) * pos.size()), "alloc curve");
+    ck(ctx->init_seg.ensure(sizeof(float) * seg.size()), "alloc curve");
+    ck(cudaMemcpyAsync(ctx->init_pos.p, pos.data(), sizeof(float) * pos.size(), cudaMemcpyHostToDevice, st), "upload curve");
+    ck(cudaMemcpyAsync(ctx->init_seg.p, seg.data(), sizeof(float) * seg.size(), cudaMemcpyHostToDevice, st), "upload curve");
+    const uint32_t C = std::max<uint32_t>(c.n_chains, 1);
+    ck(ctx->chain_out.ensure(sizeof(ChainOut) * C), "alloc chain results");
+    ck(ctx->reduce_out.ensure(sizeof(ReduceOut)), "alloc result");
+    if (p.form == TWISTY_FORM_PLAIN_FP32) {
+        ck(ctx->state.ensure(sizeof(float) * plain_state_floats_per_chain(N) * C), "alloc chain state");
+    } else if (p.form == TWISTY_FORM_FP64) {
+        ck(ctx->state.ensure(sizeof(double) * 3 * (size_t)(N + 1) * C), "alloc chain state");
+        if (p.lut_mode == TWISTY_LUT_FAITHFUL) {
+            // the FP64 form weighs with a double table; rebuild it in double
+            ctx->lut_ready = false;
+            twisty_params saved = ctx->p;
+            ctx->p.lut_mode = TWISTY_LUT_FP64;
+            build_tables(ctx, ds, false);
+            ctx->p = saved;
+        }
+    } else {
+        ck(ctx->partials.ensure(sizeof(double2) * comp_blocks(c, ctx->tuning)), "alloc block partials");
+    }
+    ck(cudaStreamSynchronize(st), "prepare");
+    ctx->kernels_per_launch = c.n_chains ? 2 : 0;
+    ctx->bc = bc;
+    ctx->prepared = true;
+    ctx->launched = false;
+    ctx->setup_ms = now_ms() - t0;
+}
+
+void launch(twisty_ctx *ctx, cudaStream_t st)
+{
+    if (!ctx->prepared) fail(TWISTY_ERR_INVALID_ARGUMENT, "twisty_launch before twisty_prepare");
+    set_device(ctx);
+    const ChainSpec &c = ctx->spec;
+    ck(cudaEventRecord(ctx->ev[0], st), "event");
+    if (c.n_chains) {
+        const twisty_params &p = ctx->p;
+        if (p.form == TWISTY_FORM_PLAIN_FP32) {
+            ck(launch_plain_chains(c, ctx->init_pos.as<float>(), ctx->state.as<float>(), ctx->lut32.as<float>(), ctx->meta,
+                                   ctx->chain_out.as<ChainOut>(), st),
+               "plain chain kernel");
+        } else if (p.form == TWISTY_FORM_FP64) {
+            const double max_k = (2.0 / (double)c.ds) * 1.01;
+            const double step = max_k / (double)(p.num_curvature_steps - 1);
+            ck(launch_fp64_chains(c, ctx->init_pos.as<float>(), ctx->state.as<double>(), ctx->lut64.as<double>(), 0.0, max_k,
+                                  step, (int32_t)p.num_curvature_steps, ctx->chain_out.as<ChainOut>(), st),
+               "fp64 chain kernel");
+        } else {
+            ck(launch_comp_chains(c, ctx->tuning, ctx->init_seg.as<float>(), ctx->logtab.as<float2>(), ctx->lintab.as<float2>(),
+                                  ctx->meta, ctx->chain_out.as<ChainOut>(), ctx->partials.as<double2>(), st),
+               "compensated chain kernel");
+        }
+    }
+    ck(cudaEventRecord(ctx->ev[1], st), "event");
+    if (c.n_chains) ck(launch_reduce(ctx->chain_out.as<ChainOut>(), c.n_chains, ctx->reduce_out.as<ReduceOut>(), st), "reduction");
+    ck(cudaEventRecord(ctx->ev[2], st), "event");
+    ctx->launched = true;
+}
+
+void collect(twisty_ctx *ctx, twisty_result *res)
+{
+    if (!ctx->launched) fail(TWISTY_ERR_INVALID_ARGUMENT, "twisty_collect before twisty_launch");
+    if (!res) fail(TWISTY_ERR_INVALID_ARGUMENT, "result is NULL");
+    set_device(ctx);
+    ReduceOut r{};
+    r.log10_sum = -std::numeric_limits<double>::infinity();
+    if (ctx->spec.n_chains) {
+        ck(cudaMemcpy(&r, ctx->reduce_out.p, sizeof(r), cudaMemcpyDeviceToHost), "read result");
+    } else {
+        ck(cudaEventSynchronize(ctx->ev[2]), "sync");
+    }
+    float a = 0, b = 0;
+    ck(cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]), "event time");
+    ck(cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]), "event time");
+    std::memset(res, 0, sizeof(*res));
+    res->log10_normalizer = ctx->log10_norm;
+    res->log10_weight = r.log10_sum + ctx->log10_norm;
+    res->total_paths = r.valid;
+    res->failed_paths = r.failed;
+    res->clamped_curvatures = r.clamped;
+    res->log10_mean_weight = r.valid ? res->log10_weight - std::log10((double)r.valid) : -std::numeric_limits<double>::infinity();
+    res->rel_std_error = r.rel_se;
+    res->num_chains = ctx->spec.n_chains;
+    res->steps_per_chain = ctx->spec.steps;
+    res->setup_ms = ctx->setup_ms;
+    res->perturb_ms = a;
+    res->weighting_ms = b;
+}
+
+twisty_status guard(twisty_ctx *ctx, const std::function<void()> &f)
+{
+    try {
+        f();
+        if (ctx) ctx->err.clear();
+        return TWISTY_OK;
+    } catch (const Failure &e) {
+        if (ctx) ctx->err = e.msg;
+        return e.s;
+    } catch (const std::bad_alloc &) {
+        if (ctx) ctx->err = "host out of memory";
+        return TWISTY_ERR_OUT_OF_MEMORY;
+    } catch (const std::exception &e) {
+        if (ctx) ctx->err = e.what();
+        return TWISTY_ERR_INVALID_ARGUMENT;
+    } catch (...) {
+        if (ctx) ctx->err = "unknown error";
+        return TWISTY_ERR_INVALID_ARGUMENT;
+    }
+}
+
+thread_local std::string g_free_err;
+
+}  // namespace
+
+extern "C" {
+
+int twisty_abi_version(void) { return TWISTY_B200_ABI_VERSION; }
+
+const char *twisty_status_string(twisty_status s)
+{
+    switch (s) {
+        case TWISTY_OK: return "ok";
+        case TWISTY_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case TWISTY_ERR_INVALID_CONFIG: return "invalid config";
+        case TWISTY_ERR_INFEASIBLE_GEOMETRY: return "infeasible geometry";
+        case TWISTY_ERR_LUT_INVALID: return "invalid weight table";
+        case TWISTY_ERR_CUDA: return "CUDA error";
+        case TWISTY_ERR_DEVICE_TIMEOUT: return "device timeout";
+        case TWISTY_ERR_IO: return "I/O error";
+        case TWISTY_ERR_UNSUPPORTED: return "unsupported";
+        case TWISTY_ERR_NO_DEVICE: return "no CUDA device";
+        case TWISTY_ERR_OUT_OF_MEMORY: return "out of memory";
+    }
+    return "unknown status";
+}
+
+void twisty_params_init(twisty_params *p)
+{
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->struct_size = sizeof(twisty_params);
+    // ExperimentParameters / WeightingParameters member initialisers
+    // (Twisty/ExperimentRunner.h:42-68, Twisty/PathWeightUtils.h:35-48)
+    p->paths_to_generate = 0;
+    p->paths_to_skip = 0;
+    p->num_segments = 4;
+    p->mu = 0.1f;
+    p->num_steps_int = 2000;
+    p->min_bound = 0.0f;
+    p->max_bound = 100.0f;
+    p->eps = 0.01f;
+    p->bias = 1.0f;
+    p->scatter = 0.0f;
+    p->absorption = 0.0f;
+    p->num_curvature_steps = 10000;
+    p->form = TWISTY_FORM_COMPENSATED;
+    p->lut_mode = TWISTY_LUT_FP64;
+    p->max_sub_chain = 25;                 // FullExperimentRunnerOptimalPerturb.cpp:483-484
+    p->max_angle = 3.141592653589793f;     // :501-502
+    p->device = 0;
+}
+
+twisty_status twisty_params_from_config(const char *text, int is_yaml, twisty_params *out, twisty_bc *bc)
+{
+    if (!text || !out) return TWISTY_ERR_INVALID_ARGUMENT;
+    twisty::Node root;
+    std::string err;
+    const bool ok = is_yaml ? twisty::parse_yaml(text, root, err) : twisty::parse_json(text, root, err);
+    if (!ok) {
+        g_free_err = err;
+        return TWISTY_ERR_INVALID_CONFIG;
+    }
+    twisty_params p;
+    twisty_params_init(&p);
+    if (!twisty::params_from_node(root, p, bc, err)) {
+        g_free_err = err;
+        return TWISTY_ERR_INVALID_CONFIG;
+    }
+    *out = p;
+    return TWISTY_OK;
+}
+
+twisty_status twisty_create(const twisty_params *p, twisty_ctx **out)
+{
+    if (!p || !out) return TWISTY_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (p->struct_size != sizeof(twisty_params)) return TWISTY_ERR_INVALID_ARGUMENT;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        g_free_err = "no CUDA device";
+        return TWISTY_ERR_NO_DEVICE;
+    }
+    if (p->device < 0 || p->device >= n) {
+        g_free_err = "device ordinal out of range";
+        return TWISTY_ERR_INVALID_ARGUMENT;
+    }
+    twisty_ctx *ctx = new (std::nothrow) twisty_ctx();
+    if (!ctx) return TWISTY_ERR_OUT_OF_MEMORY;
+    ctx->p = *p;
+    ctx->device = p->device;
+    const twisty_status s = guard(ctx, [&] {
+        set_device(ctx);
+        int sms = 0;
+        ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device), "device query");
+        ctx->sm_count = sms;
+        ck(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "stream");
+        for (auto &e : ctx->ev) ck(cudaEventCreate(&e), "event");
+    });
+    if (s != TWISTY_OK) {
+        g_free_err = ctx->err;
+        twisty_destroy(ctx);
+        return s;
+    }
+    *out = ctx;
+    return TWISTY_OK;
+}
+
+void twisty_destroy(twisty_ctx *ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    DevBuf *bufs[] = {&ctx->lut64, &ctx->lut32, &ctx->logtab, &ctx->lintab, &ctx->dmus, &ctx->deps, &ctx->lutaux,
+                      &ctx->init_pos, &ctx->init_seg, &ctx->state, &ctx->chain_out, &ctx->partials, &ctx->reduce_out,
+                      &ctx->norm_scratch};
+    for (DevBuf *b : bufs) b->release();
+    for (auto &e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char *twisty_last_error(const twisty_ctx *ctx) { return ctx ? ctx->err.c_str() : g_free_err.c_str(); }
+
+twisty_status twisty_update_params(twisty_ctx *ctx, const twisty_params *p)
+{
+    if (!ctx || !p) return TWISTY_ERR_INVALID_ARGUMENT;
+    return guard(ctx, [&] {
+        if (p->struct_size != sizeof(twisty_params)) fail(TWISTY_ERR_INVALID_ARGUMENT, "struct_size mismatch");
+        if (p->device != ctx->device) fail(TWISTY_ERR_INVALID_ARGUMENT, "the device of a context cannot change");
+        ctx->p = *p;
+        ctx->prepared = false;
+        ctx->launched = false;
+    });
+}
+
+twisty_status twisty_prepare(twisty_ctx *ctx, const twisty_bc *bc)
+{
+    if (!ctx) return TWISTY_ERR_INVALID_ARGUMENT;
+    return guard(ctx, [&] { prepare(ctx, bc); });
+}
+
+twisty_status twisty_launch(twisty_ctx *ctx, void *stream)
+{
+    if (!ctx) return TWISTY_ERR_INVALID_ARGUMENT;
+    return guard(ctx, [&] { launch(ctx, stream ? (cudaStream_t)stream : ctx->stream); });
+}
+
+twisty_status twisty_collect(twisty_ctx *ctx, twisty_result *res)
+{
+    if (!ctx) return TWISTY_ERR_INVALID_ARGUMENT;
+    return guard(ctx, [&] { collect(ctx, res); });
+}
+
+uint32_t twisty_launch_kernel_count(const twisty_ctx *ctx) { return ctx ? ctx->kernels_per_launch : 0; }
+
+twisty_status twisty_run(twisty_ctx *ctx, const twisty_bc *bc, twisty_result *res)
+{
+    if (!ctx || !res) return TWISTY_ERR_INVALID_ARGUMENT;
+    return guard(ctx, [&] {
+        const double t0 = now_ms();
+        prepare(ctx, bc);
+        launch(ctx, ctx->stream);
+        collect(ctx, res);
+        res->total_ms = now_ms() - t0;
+    });
+}
+
+twisty_status twisty_weight_paths(twisty_ctx *ctx, const twisty_bc *bc, const float *pos, uint64_t n_paths, int32_t form,
+                                  double *log10w, uint8_t *valid, int32_t *bins)
+{
+    if (!ctx || !bc || (!pos && n_paths) || (!log10w && n_paths)) return TWISTY_ERR_INVALID_ARGUMENT;
+    return guard(ctx, [&] {
+        validate(ctx->p);
+        validate_bc(bc);
+        set_device(ctx);
+        const uint32_t N = ctx->p.num_segments;
+        const float ds = bc->arclength / (float)N;
+        build_tables(ctx, ds, false);
+        if (n_paths == 0) return;
+        cudaStream_t st = ctx->stream;
+        DevBuf dpos, dw, dv, db;
+        const size_t np = 3 * (size_t)(N + 1) * n_paths;
+        try {
+            ck(dpos.ensure(sizeof(float) * np), "alloc paths");
+            ck(dw.ensure(sizeof(double) * n_paths), "alloc weights");
+            ck(dv.ensure(n_paths), "alloc validity");
+            if (bins) ck(db.ensure(sizeof(int32_t) * (N - 1) * n_paths), "alloc bins");
+            ck(cudaMemcpyAsync(dpos.p, pos, sizeof(float) * np, cudaMemcpyHostToDevice, st), "upload paths");
+            const float inv_ds = (float)N / bc->arclength;
+            const double af = (double)std::exp(-ctx->p.absorption * ds);
+            if (form == TWISTY_FORM_COMPENSATED) {
+                ck(launch_weigh_comp(dpos.as<float>(), n_paths, N, inv_ds, ctx->logtab.as<float2>(), ctx->lintab.as<float2>(),
+                                     ctx->exact_blend, ctx->meta, std::log10(af), dw.as<double>(), dv.as<uint8_t>(),
+                                     bins ? db.as<int32_t>() : nullptr, st),
+                   "weigh kernel");
+            } else if (form == TWISTY_FORM_PLAIN_FP32) {
+                ck(launch_weigh_plain(dpos.as<float>(), n_paths, N, inv_ds, ctx->lut32.as<float>(), ctx->meta, af,
+                                      dw.as<double>(), dv.as<uint8_t>(), bins ? db.as<int32_t>() : nullptr, st),
+                   "weigh kernel");
+            } else {
+                fail(TWISTY_ERR_UNSUPPORTED, "weight_paths supports the plain and compensated forms");
+            }
+            ck(cudaMemcpyAsync(log10w, dw.p, sizeof(double) * n_paths, cudaMemcpyDeviceToHost, st), "read weights");
+            if (valid) ck(cudaMemcpyAsync(valid, dv.p, n_paths, cudaMemcpyDeviceToHost, st), "read validity");
+            if (bins) ck(cudaMemcpyAsync(bins, db.p, sizeof(int32_t) * (N - 1) * n_paths, cudaMemcpyDeviceToHost, st), "read bins");
+            ck(cudaStreamSynchronize(st), "weigh");
+        } catch (...) {
+            cudaStreamSynchronize(st);
+            dpos.release(); dw.release(); dv.release(); db.release();
+            throw;
+        }
+        dpos.release(); dw.release(); dv.release(); db.release();
+    });
+}
+
+twisty_status twisty_build_lut(twisty_ctx *ctx, float ds, float *lut, twisty_lut_info *info)
+{
+    if (!ctx || !(ds > 0.0f)) return TWISTY_ERR_INVALID_ARGUMENT;
+    return guard(ctx, [&] {
+        validate(ctx->p);
+        set_device(ctx);
+        build_tables(ctx, ds, false);
+        if (lut) ck(cudaMemcpy(lut, ctx->lut32.p, sizeof(float) * ctx->p.num_curvature_steps, cudaMemcpyDeviceToHost), "read table");
+        if (info) {
+            info->min_curvature = ctx->meta.min_k;
+            info->max_curvature = ctx->meta.max_k;
+            info->curvature_step = ctx->meta.step;
+            info->min_segment_weight = (float)ctx->min_w;
+            info->max_segment_weight = (float)ctx->max_w;
+            info->ds = ds;
+            info->bins = ctx->p.num_curvature_steps;
+        }
+    });
+}
+
+twisty_status twisty_set_lut(twisty_ctx *ctx, const float *lut, const twisty_lut_info *info)
+{
+    if (!ctx || !lut || !info || info->bins < 2) return TWISTY_ERR_INVALID_ARGUMENT;
+    return guard(ctx, [&] {
+        for (uint32_t i = 0; i < info->bins; ++i)
+            if (!std::isfinite(lut[i])) fail(TWISTY_ERR_LUT_INVALID, "table has non-finite entries");
+        if (!(info->curvature_step > 0.0f) || !(info->max_curvature > info->min_curvature))
+            fail(TWISTY_ERR_LUT_INVALID, "table range is empty");
+        ctx->ext_lut.assign(lut, lut + info->bins);
+        ctx->ext_info = *info;
+        ctx->p.lut_mode = TWISTY_LUT_EXTERNAL;
+        ctx->p.num_curvature_steps = info->bins;
+        ctx->lut_ready = false;
+        ctx->prepared = false;
+    });
+}
+
+twisty_status twisty_normalizer_log10(twisty_ctx *ctx, uint32_t n, float ds, const twisty_bc *bc, double *out)
+{
+    if (!ctx || !bc || !out || n < 4 || !(ds > 0.0f)) return TWISTY_ERR_INVALID_ARGUMENT;
+    return guard(ctx, [&] {
+        set_device(ctx);
+        *out = normalizer_log10(ctx, n, ds, *bc);
+    });
+}
+
+twisty_status twisty_bootstrap_curve(const twisty_params *p, const twisty_bc *bc, float *pos)
+{
+    if (!p || !bc || !pos) return TWISTY_ERR_INVALID_ARGUMENT;
+    std::vector<float> v;
+    std::string e;
+    if (p->num_segments < 4) return TWISTY_ERR_INVALID_CONFIG;
+    if (!(bc->arclength > 0.0f)) return TWISTY_ERR_INVALID_CONFIG;
+    if (!twisty::bootstrap_arc(*bc, p->num_segments, p->bootstrap_seed, v, e)) {
+        g_free_err = e;
+        return TWISTY_ERR_INFEASIBLE_GEOMETRY;
+    }
+    std::memcpy(pos, v.data(), sizeof(float) * v.size());
+    return TWISTY_OK;
+}
+
+float twisty_min_arclength(const twisty_bc *bc, uint32_t n) { return bc ? twisty::min_arclength(*bc, n) : 0.0f; }
+
+twisty_status twisty_run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_t iterations,
+                               twisty_result *res)
+{
+    if (!ctx || (!ex && n) || (!res && n)) return TWISTY_ERR_INVALID_ARGUMENT;
+    (void)iterations;
+    return guard(ctx, [&] { fail(TWISTY_ERR_UNSUPPORTED, "batched runs are not built yet"); });
+}
+
+twisty_status twisty_export_paths(twisty_ctx *ctx, const twisty_bc *bc, const char *dir, uint64_t max_paths, float *pos,
+                                  double *log10w, uint64_t *n_written, twisty_result *res)
+{
+    if (!ctx || !bc) return TWISTY_ERR_INVALID_ARGUMENT;
+    (void)dir; (void)max_paths; (void)pos; (void)log10w; (void)n_written; (void)res;
+    return guard(ctx, [&] { fail(TWISTY_ERR_UNSUPPORTED, "path export is not built yet"); });
+}
+
+twisty_status twisty_adjoint(twisty_ctx *ctx, const twisty_bc *bc, const twisty_result *fwd, double grad[5])
+{
+    if (!ctx || !bc || !fwd || !grad) return TWISTY_ERR_INVALID_ARGUMENT;
+    return guard(ctx, [&] { fail(TWISTY_ERR_UNSUPPORTED, "the adjoint is not built yet"); });
+}
+
+twisty_status twisty_set_initial_curve(twisty_ctx *ctx, const float *pos, uint32_t n_points)
+{
+    if (!ctx) return TWISTY_ERR_INVALID_ARGUMENT;
+    return guard(ctx, [&] {
+        if (!pos) {
+            ctx->user_curve.clear();
+        } else {
+            ctx->user_curve.assign(pos, pos + 3 * (size_t)n_points);
+        }
+        ctx->prepared = false;
+    });
+}
+
+}  // extern "C"
