@@ -32,16 +32,15 @@ def golden_lut_info(name):
 
 # ------------------------------------------------------------------------------ tables
 @pytest.mark.parametrize("name", sorted(LUT_SETS))
-def test_faithful_table_within_one_ulp_of_reference(name):
+def test_faithful_table_bit_exact_with_reference(name):
     p, N, S = lut_params(name, lut_mode=T.LUT_FAITHFUL)
     g = golden_npz(f"lut_{name}.npz")
     with T.Context(p) as ctx:
         lut, info = ctx.build_lut(F32(S) / F32(N))
-    ulps = np.abs(lut.view(np.int32).astype(np.int64) - g["lut"].view(np.int32).astype(np.int64))
-    assert ulps.max() <= 1, ulps.max()
-    assert np.mean(ulps == 0) > 0.9
+    assert np.array_equal(lut.view(np.uint32), g["lut"].view(np.uint32))
     h = g["hdr"]
-    assert (info.min_curvature, info.max_curvature, info.curvature_step) == (h[0], h[1], h[2])
+    assert (info.min_curvature, info.max_curvature, info.curvature_step, info.min_segment_weight,
+            info.max_segment_weight) == (h[0], h[1], h[2], h[3], h[4])
 
 
 @pytest.mark.parametrize("name", sorted(LUT_SETS))

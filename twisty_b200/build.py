@@ -24,7 +24,8 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libtwisty_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-I", os.path.join(ROOT, "include")]
+COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3,-ffp-contract=off", "-I",
+          os.path.join(ROOT, "include")]
 # Translation units whose FP32 arithmetic must keep the reference's exact rounding. Their
 # device code spells every operation with round-to-nearest intrinsics already; the flag
 # also keeps any remaining plain expression from being contracted.
@@ -84,6 +85,17 @@ def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = True) 
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    # drop-in CLI for the reference's Experiments/FullExperiment.cpp, linked to the library
+    cli_src = os.path.join(HERE, "cli", "full_experiment.cpp")
+    cli = os.path.join(HERE, "twisty_full_experiment")
+    hdr = os.path.join(ROOT, "include", "twisty_b200_runner.hpp")
+    if force or not os.path.exists(cli) or os.path.getmtime(cli) < max(os.path.getmtime(cli_src), os.path.getmtime(hdr),
+                                                                       os.path.getmtime(LIB)):
+        gxx = (_host_compiler() or ["", "g++"])[1]
+        r = subprocess.run([gxx, "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), cli_src, "-o", cli,
+                            "-L", HERE, "-ltwisty_b200", "-Wl,-rpath,$ORIGIN"], capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"CLI build failed:\n{r.stderr}")
     if not quiet:
         print(LIB)
     return LIB

@@ -40,6 +40,7 @@ constexpr uint32_t FULL = 0xffffffffu;
 constexpr int kMaxSubChain = 64;            // largest k the rotation rounds cover
 constexpr float kLog2_10 = 3.32192809488736234787f;
 constexpr float kLog10_2 = 0.30102999566398119521f;
+constexpr float kInvLn10 = 0.43429448190325182765f;
 
 struct CompConsts {
     float kscale;        // (N/S) / step : |t_{i+1}-t_i| -> fractional bin index
@@ -170,12 +171,73 @@ struct Layout {
     }
 };
 
-template <int G, int SPL, bool EXACT, int MAXT>
+enum { kModeForward = 0, kModeExport = 1, kModeAdjoint = 2 };
+
+// Receiver-position gradient of one path's log10 weight, computed by one lane from the
+// last three segment vectors: moving the receiver moves points N-1 and N together, so only
+// v_{N-2} changes, hence t_{N-2} and the curvatures kappa_{N-3}, kappa_{N-2}. The table's
+// slope is taken per bin, (L_{i+1} - L_i) / step, the derivative of the curve the table
+// samples (the reference's interpolation weight in curvature units makes its own weight
+// almost piecewise constant within a bin, a slope finite differences do not see).
+__device__ __forceinline__ void receiver_grad(const float *sx, const float *sy, const float *sz, uint32_t a3,
+                                              uint32_t a2, uint32_t a1, const float *__restrict__ lut,
+                                              const CompConsts &k, float inv_ds, float g[3])
+{
+    const float v3x = sx[a3], v3y = sy[a3], v3z = sz[a3];   // v_{N-3}
+    const float v2x = sx[a2], v2y = sy[a2], v2z = sz[a2];   // v_{N-2}
+    const float v1x = sx[a1], v1y = sy[a1], v1z = sz[a1];   // v_{N-1}
+    const float r3 = rsqrtf(fmaf(v3x, v3x, fmaf(v3y, v3y, v3z * v3z)));
+    const float r2 = rsqrtf(fmaf(v2x, v2x, fmaf(v2y, v2y, v2z * v2z)));
+    const float r1 = rsqrtf(fmaf(v1x, v1x, fmaf(v1y, v1y, v1z * v1z)));
+    const float t3[3] = {v3x * r3, v3y * r3, v3z * r3};
+    const float t2[3] = {v2x * r2, v2y * r2, v2z * r2};
+    const float t1[3] = {v1x * r1, v1y * r1, v1z * r1};
+    // d t2 / d v2 = (I - t2 t2^T) * r2
+    g[0] = g[1] = g[2] = 0.f;
+    for (int which = 0; which < 2; ++which) {
+        float d[3];
+        float sign;
+        if (which == 0) { for (int q = 0; q < 3; ++q) d[q] = t2[q] - t3[q]; sign = 1.f; }   // kappa_{N-3}
+        else { for (int q = 0; q < 3; ++q) d[q] = t1[q] - t2[q]; sign = -1.f; }             // kappa_{N-2}
+        const float dn = sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        if (!(dn > 0.f)) continue;
+        float r = fmaf(dn, k.kscale, k.roff);
+        if (r < 0.f) r = 0.f;
+        if (r > k.rmax) continue;  // clamped: flat
+        const int32_t L = min((int32_t)r, k.bins - 1);
+        const int32_t R = min(L + 1, k.bins - 1);
+        const float lv = __ldg(lut + L), rv = __ldg(lut + R);
+        const float dd = (r - (float)L) * k.step;
+        const float blend = fmaf(dd, rv - lv, lv);
+        // d log10(w)/d kappa, per unit curvature
+        const float dlog = (rv - lv) / (k.step * blend) * kInvLn10;
+        const float dk = dlog * inv_ds * sign / dn;  // d kappa / d t = inv_ds * d/|d| (sign per term)
+        // project through (I - t2 t2^T) r2
+        const float dt = d[0] * t2[0] + d[1] * t2[1] + d[2] * t2[2];
+        for (int q = 0; q < 3; ++q) g[q] += dk * (d[q] - dt * t2[q]) * r2;
+    }
+}
+
+struct ModeArgs {
+    // export
+    float *exp_pos;      // [chains][steps][N+1][3]
+    double *exp_w;       // [chains][steps] log10 weights (absorption included, normaliser not)
+    float x0[3];
+    double log10_abs;
+    // adjoint
+    const float *lut;    // float table
+    const float *dmu;    // d table / d mu_s
+    const float *deps;   // d table / d eps
+    float ref_log10;     // log10 of the forward sum of path weights (normaliser excluded)
+    double *grad;        // [chains][6]: d/dmu_s, d/deps, d/dx, d/dy, d/dz (log10 units), sum of weights
+};
+
+template <int G, int SPL, bool EXACT, int MAXT, int MODE>
 __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompConsts kc,
                                                              const float *__restrict__ init_seg,
                                                              const float2 *__restrict__ tab_g,
                                                              ChainOut *__restrict__ out,
-                                                             double2 *__restrict__ block_partials)
+                                                             double2 *__restrict__ block_partials, ModeArgs ma)
 {
     extern __shared__ float4 smem4[];
     const int bins = kc.bins;
@@ -216,6 +278,7 @@ __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompCo
     const uint32_t gchain = c.chain0 + (real_chain ? chain : 0);
     float lse_m = 0.f, lse_s = 0.f, lse_c = 0.f;
     uint32_t valid = 0, failed = 0, clamped = 0;
+    float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 
     auto seg_smem = [&](int m, float &x, float &y, float &z) {
         const uint32_t a = Lay::addr(gbase, j, m);
@@ -280,10 +343,109 @@ __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompCo
             __syncwarp();
             const uint32_t step = base + jj;
             if (step < c.burn_in) continue;
+            const uint32_t wstep = step - c.burn_in;
+            const bool active = wstep < steps_c;
             float hi, lo;
-            path_log10<G, SPL, EXACT>(j, N, s_tab, kc, seg_smem, no_bins, hi, lo, clamped);
-            __syncwarp();
-            if (step - c.burn_in >= steps_c) continue;
+            if (MODE == kModeAdjoint) {
+                // log10 weight and d/d(mu_s), d/d(eps) of this lane's segments (exact blend)
+                float s = 0.f, cc = 0.f, gmu = 0.f, geps = 0.f;
+                float t0x = 0.f, t0y = 0.f, t0z = 0.f, px = 0.f, py = 0.f, pz = 0.f;
+                const uint32_t b0 = j * SPL;
+                auto seg_term = [&](float qq) {
+                    float r = fmaf(sqrt_approx(qq), kc.kscale, kc.roff);
+                    if (r < 0.f) r = 0.f;
+                    if (r > kc.rmax) r = kc.rmax;
+                    const int32_t L = min((int32_t)r, kc.bins - 1);
+                    const int32_t Rb = min(L + 1, kc.bins - 1);
+                    const float d = (r - (float)L) * kc.step;
+                    const float lv = __ldg(ma.lut + L), rv = __ldg(ma.lut + Rb);
+                    const float v = fmaf(d, rv - lv, lv);
+                    kahan_add(s, cc, __log2f(v) * kLog10_2);
+                    const float ml = __ldg(ma.dmu + L), mr = __ldg(ma.dmu + Rb);
+                    const float el = __ldg(ma.deps + L), er = __ldg(ma.deps + Rb);
+                    gmu += fmaf(d, mr - ml, ml) / v;
+                    geps += fmaf(d, er - el, el) / v;
+                };
+#pragma unroll
+                for (int m = 0; m < SPL; ++m) {
+                    float x, y, z;
+                    seg_smem(m, x, y, z);
+                    const float rs = rsqrtf(fmaf(x, x, fmaf(y, y, z * z)));
+                    const float tx = x * rs, ty = y * rs, tz = z * rs;
+                    if (m == 0) { t0x = tx; t0y = ty; t0z = tz; }
+                    else if (b0 + m <= N - 1) {
+                        const float dx = tx - px, dy = ty - py, dz = tz - pz;
+                        seg_term(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+                    }
+                    px = tx; py = ty; pz = tz;
+                }
+                const float nx = __shfl_down_sync(FULL, t0x, 1, G);
+                const float ny = __shfl_down_sync(FULL, t0y, 1, G);
+                const float nz = __shfl_down_sync(FULL, t0z, 1, G);
+                if (b0 + SPL <= N - 1) {
+                    const float dx = nx - px, dy = ny - py, dz = nz - pz;
+                    seg_term(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+                }
+                hi = s;
+                lo = -cc;
+                group_sum_pair<G>(hi, lo);
+                float g3[3] = {0.f, 0.f, 0.f};
+                if (j == 0)
+                    receiver_grad(sx, sy, sz, Lay::addr(gbase, (N - 3) / SPL, (N - 3) % SPL),
+                                  Lay::addr(gbase, (N - 2) / SPL, (N - 2) % SPL),
+                                  Lay::addr(gbase, (N - 1) / SPL, (N - 1) % SPL), ma.lut, kc, c.inv_ds, g3);
+                if (active && !(isnan(hi) || isnan(lo))) {
+                    const float wt = exp2f(((hi - ma.ref_log10) + lo) * kLog2_10);
+                    acc[0] += wt * gmu * kInvLn10;
+                    acc[1] += wt * geps * kInvLn10;
+                    acc[2] += wt * g3[0];
+                    acc[3] += wt * g3[1];
+                    acc[4] += wt * g3[2];
+                    if (j == 0) acc[5] += wt;
+                }
+            } else {
+                path_log10<G, SPL, EXACT>(j, N, s_tab, kc, seg_smem, no_bins, hi, lo, clamped);
+            }
+            if (MODE == kModeExport) {
+                // positions x_0 + prefix sums of the segment vectors, in double; every lane
+                // takes part in the scan, only active chains write
+                double px = 0.0, py = 0.0, pz = 0.0;
+                double lx[SPL], ly[SPL], lz[SPL];
+#pragma unroll
+                for (int m = 0; m < SPL; ++m) {
+                    const uint32_t a = Lay::addr(gbase, j, m);
+                    const bool in = j * SPL + m < N;
+                    px += in ? (double)sx[a] : 0.0;
+                    py += in ? (double)sy[a] : 0.0;
+                    pz += in ? (double)sz[a] : 0.0;
+                    lx[m] = px; ly[m] = py; lz[m] = pz;
+                }
+                double ex = px, ey = py, ez = pz;   // inclusive scan of lane totals
+#pragma unroll
+                for (int o = 1; o < G; o <<= 1) {
+                    const double ux = __shfl_up_sync(FULL, ex, o, G), uy = __shfl_up_sync(FULL, ey, o, G),
+                                 uz = __shfl_up_sync(FULL, ez, o, G);
+                    if ((int)j >= o) { ex += ux; ey += uy; ez += uz; }
+                }
+                ex -= px; ey -= py; ez -= pz;       // exclusive
+                if (active) {
+                    const size_t pidx = (size_t)chain * c.steps + wstep;
+                    float *dst = ma.exp_pos + pidx * 3 * (size_t)(N + 1);
+                    if (j == 0) { dst[0] = ma.x0[0]; dst[1] = ma.x0[1]; dst[2] = ma.x0[2]; }
+#pragma unroll
+                    for (int m = 0; m < SPL; ++m) {
+                        const uint32_t s = j * SPL + m;
+                        if (s < N) {
+                            dst[3 * (s + 1)] = (float)((double)ma.x0[0] + ex + lx[m]);
+                            dst[3 * (s + 1) + 1] = (float)((double)ma.x0[1] + ey + ly[m]);
+                            dst[3 * (s + 1) + 2] = (float)((double)ma.x0[2] + ez + lz[m]);
+                        }
+                    }
+                    if (j == 0)
+                        ma.exp_w[pidx] = (isnan(hi) || isnan(lo)) ? NAN : (double)hi + (double)lo + (N - 1) * ma.log10_abs;
+                }
+            }
+            if (!active) continue;
             if (isnan(hi) || isnan(lo)) {
                 ++failed;
             } else if (valid == 0) {
@@ -309,11 +471,24 @@ __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompCo
         }
     }
     clamped = group_sum_u<G>(clamped);
-    const double chain_log10 = valid ? (double)lse_m + log10((double)lse_s - (double)lse_c) : -INFINITY;
+    if (MODE == kModeAdjoint) {
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            float v = acc[i];
+#pragma unroll
+            for (int o = 1; o < G; o <<= 1) v += __shfl_xor_sync(FULL, v, o);
+            acc[i] = v;
+        }
+        if (j == 0 && real_chain)
+            for (int i = 0; i < 6; ++i) ma.grad[(size_t)chain * 6 + i] = (double)acc[i];
+    }
+    const double chain_log10 = valid ? (double)lse_m + log10((double)lse_s - (double)lse_c) +
+                                       (double)(N - 1) * ma.log10_abs
+                                     : -INFINITY;
     const uint32_t slot = warp * CPW + q;
     if (j == 0) {
         s_res[slot] = real_chain ? chain_log10 : -INFINITY;
-        if (real_chain) {
+        if (real_chain && out) {
             ChainOut o;
             o.log10_sum = chain_log10;
             o.valid = valid;
@@ -373,26 +548,33 @@ __global__ void __launch_bounds__(256) weigh_comp_kernel(const float *__restrict
     }
 }
 
-template <int G, int SPL, bool EXACT>
+template <int G, int SPL, bool EXACT, int MODE>
 cudaError_t launch_t(const ChainSpec &c, const CompConsts &kc, int warps, const float *init_seg, const float2 *tab,
-                     ChainOut *out, double2 *partials, size_t smem, uint32_t blocks, cudaStream_t st)
+                     ChainOut *out, double2 *partials, const ModeArgs &ma, size_t smem, uint32_t blocks, cudaStream_t st)
 {
     constexpr int MAXT = (SPL >= 16) ? 512 : 1024;
     if (warps * 32 > MAXT) return cudaErrorInvalidConfiguration;
-    auto kern = comp_chain_kernel<G, SPL, EXACT, MAXT>;
+    auto kern = comp_chain_kernel<G, SPL, EXACT, MAXT, MODE>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<blocks, warps * 32, smem, st>>>(c, kc, init_seg, tab, out, partials);
+    kern<<<blocks, warps * 32, smem, st>>>(c, kc, init_seg, tab, out, partials, ma);
     return cudaGetLastError();
 }
 
 template <int G, int SPL>
-cudaError_t launch_g(const ChainSpec &c, const CompConsts &kc, const CompTuning &t, const float *init_seg,
-                     const float2 *tab, ChainOut *out, double2 *partials, size_t smem, uint32_t blocks,
-                     cudaStream_t st)
+cudaError_t launch_g(int mode, const ChainSpec &c, const CompConsts &kc, const CompTuning &t, const float *init_seg,
+                     const float2 *tab, ChainOut *out, double2 *partials, const ModeArgs &ma, size_t smem,
+                     uint32_t blocks, cudaStream_t st)
 {
-    if (t.exact_blend) return launch_t<G, SPL, true>(c, kc, t.warps_per_block, init_seg, tab, out, partials, smem, blocks, st);
-    return launch_t<G, SPL, false>(c, kc, t.warps_per_block, init_seg, tab, out, partials, smem, blocks, st);
+    const int w = t.warps_per_block;
+    if (mode == kModeAdjoint)
+        return launch_t<G, SPL, true, kModeAdjoint>(c, kc, w, init_seg, tab, out, partials, ma, smem, blocks, st);
+    if (mode == kModeExport) {
+        if (t.exact_blend) return launch_t<G, SPL, true, kModeExport>(c, kc, w, init_seg, tab, out, partials, ma, smem, blocks, st);
+        return launch_t<G, SPL, false, kModeExport>(c, kc, w, init_seg, tab, out, partials, ma, smem, blocks, st);
+    }
+    if (t.exact_blend) return launch_t<G, SPL, true, kModeForward>(c, kc, w, init_seg, tab, out, partials, ma, smem, blocks, st);
+    return launch_t<G, SPL, false, kModeForward>(c, kc, w, init_seg, tab, out, partials, ma, smem, blocks, st);
 }
 
 CompConsts make_consts(float inv_ds, const LutMetaF &m)
@@ -452,17 +634,19 @@ uint32_t comp_blocks(const ChainSpec &c, const CompTuning &t)
     return (c.n_chains + per_block - 1) / per_block;
 }
 
-cudaError_t launch_comp_chains(const ChainSpec &c, const CompTuning &t, const float *init_seg, const float2 *logtab,
-                               const float2 *lintab, LutMetaF m, ChainOut *out, double2 *block_partials,
-                               cudaStream_t st)
+namespace {
+cudaError_t launch_mode(int mode, const ChainSpec &c, const CompTuning &t, const float *init_seg, const float2 *logtab,
+                        const float2 *lintab, LutMetaF m, ChainOut *out, double2 *block_partials, const ModeArgs &ma,
+                        cudaStream_t st)
 {
     if (!comp_tuning_supported(t, c.n_segments, c.k_eff)) return cudaErrorInvalidValue;
+    if (c.n_chains == 0) return cudaSuccess;
     const CompConsts kc = make_consts(c.inv_ds, m);
     const size_t smem = comp_smem_bytes(t, (uint32_t)m.bins);
     const uint32_t blocks = comp_blocks(c, t);
-    const float2 *tab = t.exact_blend ? lintab : logtab;
+    const float2 *tab = (t.exact_blend || mode == kModeAdjoint) ? lintab : logtab;
 #define TWISTY_CASE(GG, SS) \
-    if (t.group == GG && t.spl == SS) return launch_g<GG, SS>(c, kc, t, init_seg, tab, out, block_partials, smem, blocks, st);
+    if (t.group == GG && t.spl == SS) return launch_g<GG, SS>(mode, c, kc, t, init_seg, tab, out, block_partials, ma, smem, blocks, st);
     TWISTY_CASE(8, 2)
     TWISTY_CASE(8, 4)
     TWISTY_CASE(8, 8)
@@ -476,6 +660,66 @@ cudaError_t launch_comp_chains(const ChainSpec &c, const CompTuning &t, const fl
     TWISTY_CASE(32, 32)
 #undef TWISTY_CASE
     return cudaErrorInvalidValue;
+}
+
+__global__ void __launch_bounds__(1024) grad_reduce_kernel(const double *__restrict__ g, uint32_t n, double *__restrict__ out)
+{
+    __shared__ double red[6][32];
+    double a[6] = {0, 0, 0, 0, 0, 0};
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+        for (int k = 0; k < 6; ++k) a[k] += g[(size_t)i * 6 + k];
+    for (int k = 0; k < 6; ++k)
+        for (int o = 16; o > 0; o >>= 1) a[k] += __shfl_xor_sync(FULL, a[k], o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0)
+        for (int k = 0; k < 6; ++k) red[k][w] = a[k];
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double v = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) v += red[threadIdx.x][i];
+        out[threadIdx.x] = v;
+    }
+}
+}  // namespace
+
+cudaError_t launch_comp_chains(const ChainSpec &c, const CompTuning &t, const float *init_seg, const float2 *logtab,
+                               const float2 *lintab, LutMetaF m, ChainOut *out, double2 *block_partials,
+                               cudaStream_t st)
+{
+    ModeArgs ma{};
+    ma.log10_abs = log10(c.absorption_factor);
+    return launch_mode(kModeForward, c, t, init_seg, logtab, lintab, m, out, block_partials, ma, st);
+}
+
+cudaError_t launch_comp_export(const ChainSpec &c, const CompTuning &t, const float *init_seg, const float2 *logtab,
+                               const float2 *lintab, LutMetaF m, const float x0[3], float *exp_pos, double *exp_w,
+                               ChainOut *out, cudaStream_t st)
+{
+    ModeArgs ma{};
+    ma.log10_abs = log10(c.absorption_factor);
+    ma.exp_pos = exp_pos;
+    ma.exp_w = exp_w;
+    ma.x0[0] = x0[0];
+    ma.x0[1] = x0[1];
+    ma.x0[2] = x0[2];
+    return launch_mode(kModeExport, c, t, init_seg, logtab, lintab, m, out, nullptr, ma, st);
+}
+
+cudaError_t launch_comp_adjoint(const ChainSpec &c, const CompTuning &t, const float *init_seg, const float2 *lintab,
+                                LutMetaF m, const float *lut, const float *dmu, const float *deps, float ref_log10,
+                                double *grad_chains, double *grad_out, cudaStream_t st)
+{
+    ModeArgs ma{};
+    ma.log10_abs = log10(c.absorption_factor);
+    ma.lut = lut;
+    ma.dmu = dmu;
+    ma.deps = deps;
+    ma.ref_log10 = ref_log10;
+    ma.grad = grad_chains;
+    cudaError_t e = launch_mode(kModeAdjoint, c, t, init_seg, lintab, lintab, m, nullptr, nullptr, ma, st);
+    if (e != cudaSuccess) return e;
+    grad_reduce_kernel<<<1, 1024, 0, st>>>(grad_chains, c.n_chains, grad_out);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_weigh_comp(const float *pos, uint64_t n_paths, uint32_t n_segments, float inv_ds,

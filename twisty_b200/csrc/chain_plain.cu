@@ -26,7 +26,9 @@ constexpr int kPlainThreads = 128;
 __global__ void __launch_bounds__(kPlainThreads) plain_chain_kernel(ChainSpec c, const float *__restrict__ init_pos,
                                                                      float *__restrict__ state,
                                                                      const float *__restrict__ lut, LutMetaF mf,
-                                                                     ChainOut *__restrict__ out)
+                                                                     ChainOut *__restrict__ out,
+                                                                     float *__restrict__ exp_pos,
+                                                                     double *__restrict__ exp_w)
 {
     const uint32_t chain = blockIdx.x * blockDim.x + threadIdx.x;
     if (chain >= c.n_chains) return;
@@ -95,6 +97,13 @@ __global__ void __launch_bounds__(kPlainThreads) plain_chain_kernel(ChainSpec c,
         }
         if (ok && !isnan(running)) dev::cw_add(cw, running);
         else ++failed;
+        if (exp_pos) {
+            // export replay: every weighted path of this chain, in step order
+            const size_t pidx = (size_t)chain * c.steps + (s - c.burn_in);
+            float *dst = exp_pos + pidx * 3 * (size_t)(N + 1);
+            for (uint32_t i = 0; i < 3 * (N + 1); ++i) dst[i] = pos[i];
+            exp_w[pidx] = (ok && !isnan(running)) ? running : NAN;
+        }
     }
     ChainOut o;
     o.log10_sum = dev::cw_log10(cw);
@@ -343,10 +352,11 @@ __global__ void __launch_bounds__(128) weigh_plain_kernel(const float *__restric
 }  // namespace
 
 cudaError_t launch_plain_chains(const ChainSpec &c, const float *init_pos, float *state, const float *lut,
-                                LutMetaF m, ChainOut *out, cudaStream_t st)
+                                LutMetaF m, ChainOut *out, cudaStream_t st, float *exp_pos, double *exp_w)
 {
+    if (c.n_chains == 0) return cudaSuccess;
     const uint32_t blocks = (c.n_chains + kPlainThreads - 1) / kPlainThreads;
-    plain_chain_kernel<<<blocks, kPlainThreads, 0, st>>>(c, init_pos, state, lut, m, out);
+    plain_chain_kernel<<<blocks, kPlainThreads, 0, st>>>(c, init_pos, state, lut, m, out, exp_pos, exp_w);
     return cudaGetLastError();
 }
 

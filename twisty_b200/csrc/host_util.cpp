@@ -7,6 +7,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <sstream>
+#include <thread>
 
 namespace twisty {
 
@@ -509,6 +510,81 @@ bool bootstrap_arc(const twisty_bc &bc, uint32_t n, uint32_t seed, std::vector<f
         for (int k = 0; k < 3; ++k) p[k] += dsd * (std::cos(th) * u[k] + std::sin(th) * w2[k]);
         set(2 + i, (float)p[0], (float)p[1], (float)p[2]);
     }
+    return true;
+}
+
+namespace {
+
+constexpr float kTwistyPiF = 3.141592653589793f;  // Twisty/MathConsts.h:8
+
+float gaussian_phase(float p, float m)
+{
+    const float np = std::sqrt((kTwistyPiF * m) * 0.5f) / (1.0f - std::exp(-2.0f / m));
+    const float val = (-m * p * p) * 0.5f;
+    return np * std::exp(val);
+}
+
+double integrand_rt(double p, double kds, double bds, double eps, double mu)
+{
+    const double phase = (double)gaussian_phase((float)p, (float)mu);
+    const double scattering = p * std::exp(bds * phase - 1.0 * (eps * eps * p * p * 0.5));
+    double sin_term = p;
+    if (kds > 0.0) sin_term = std::sin(kds * p) / kds;
+    return scattering * sin_term;
+}
+
+float integrate(float curvature, float mu, float eps, float scatter, float min_bound, float max_bound, float bias,
+                uint32_t n, float ds, std::vector<double> &w)
+{
+    const double kds = (double)(curvature * ds);
+    const double bds = (double)(scatter * ds);
+    const double h = (double)((max_bound - min_bound) / (float)n);
+    const double weight = (double)(1.0f / 3.0f) * h;
+    const double start = (double)min_bound;
+    const double reg = (double)mu, pm = (double)eps;
+    w.assign(n + 1, 0.0);
+    w[0] = integrand_rt(start, kds, bds, reg, pm) * weight;
+    w[n] = integrand_rt((double)max_bound, kds, bds, reg, pm) * weight;
+    for (uint32_t i = 1; i < n / 2; ++i) w[2 * i - 1] = integrand_rt(start + ((double)(2 * i - 1) * h), kds, bds, reg, pm) * weight * 4.0;
+    for (uint32_t i = 1; i < n / 2 - 1; ++i) w[2 * i] = integrand_rt(start + ((double)(2 * i) * h), kds, bds, reg, pm) * weight * 2.0;
+    std::sort(w.begin(), w.end());
+    double sum = 0.0;
+    for (double v : w) sum += v;
+    const double tp = (double)kTwistyPiF;
+    return (float)((sum / (2.0 * tp * tp)) * (double)bias);
+}
+
+}  // namespace
+
+bool lut_faithful_host(float mu, float eps, float scatter, float min_bound, float max_bound, float bias,
+                       uint32_t num_steps_int, uint32_t bins, float ds, float *out, float minmax[2])
+{
+    if (bins < 2 || num_steps_int < 4 || (num_steps_int & 1u) || !(ds > 0.0f)) return false;
+    const float min_k = 0.0f;
+    const float max_k = (float)((2.0 / (double)ds) * (double)1.01f);
+    const float step = (max_k - min_k) / (float)(bins - 1);
+    unsigned nt = std::max(1u, std::thread::hardware_concurrency());
+    nt = std::min<unsigned>(nt, bins);
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; ++t) {
+        th.emplace_back([=]() {
+            std::vector<double> w;
+            for (uint32_t i = (uint32_t)((uint64_t)bins * t / nt); i < (uint32_t)((uint64_t)bins * (t + 1) / nt); ++i) {
+                const float kappa = min_k + ((float)(int64_t)i * step);
+                out[i] = integrate(kappa, mu, eps, scatter, min_bound, max_bound, bias, num_steps_int, ds, w);
+            }
+        });
+    }
+    for (auto &x : th) x.join();
+    float mn = out[0], mx = out[0];
+    for (uint32_t i = 1; i < bins; ++i) {
+        if (out[i] < mn && out[i] >= 0.0f) mn = out[i];
+        if (out[i] > mx && out[i] >= 0.0f) mx = out[i];
+    }
+    for (uint32_t i = 0; i < bins; ++i)
+        if (out[i] <= 0.0f) out[i] = mn;
+    minmax[0] = mn;
+    minmax[1] = mx;
     return true;
 }
 

@@ -41,6 +41,15 @@ float min_arclength(const twisty_bc &bc, uint32_t n);
 // |x_{N-1} - x_1| > (N-2) ds.
 bool bootstrap_arc(const twisty_bc &bc, uint32_t n, uint32_t seed, std::vector<float> &pos, std::string &err);
 
+// The reference's table, rounding for rounding: WeightLookupTableIntegral ctor + Initialize
+// (Twisty/PathWeightUtils.cpp:281-348) with Integrate's sorted sum (:371-433) and the float
+// phase function (:19-33), on host threads. Bins whose integral cancels to a tiny fraction
+// of its terms keep the reference's summation-order rounding only this way, so the
+// faithful table mode (the drop-in's bit-parity setup) is built here; the FP64 tables are
+// built on the device. out[bins]; minmax = {min, max} weight. Returns false on bad params.
+bool lut_faithful_host(float mu, float eps, float scatter, float min_bound, float max_bound, float bias,
+                       uint32_t num_steps_int, uint32_t bins, float ds, float *out, float minmax[2]);
+
 // K4 (Twisty/PathWeightUtils.cpp:643-651) and the z of Norm (:729-732), float math.
 double norm_k4_log10(float z, float ds);
 float norm_z(const twisty_bc &bc, float ds);

@@ -75,7 +75,8 @@ cudaError_t launch_lut_logtable(uint32_t bins, const float *lut32, float step, f
 
 // ------------------------------------------------------------- chains (chain_*.cu)
 cudaError_t launch_plain_chains(const ChainSpec &c, const float *init_pos, float *state,
-                                const float *lut, LutMetaF m, ChainOut *out, cudaStream_t st);
+                                const float *lut, LutMetaF m, ChainOut *out, cudaStream_t st,
+                                float *exp_pos = nullptr, double *exp_w = nullptr);
 // Plain-form state of one chain: positions (N+1)*3, tangents N*3, curvatures N-1,
 // padded to a multiple of 4 floats.
 __host__ __device__ inline size_t plain_state_floats_per_chain(uint32_t n)
@@ -103,6 +104,17 @@ cudaError_t launch_comp_chains(const ChainSpec &c, const CompTuning &t, const fl
                                const float2 *logtab, const float2 *lintab, LutMetaF m,
                                ChainOut *out, double2 *block_partials, cudaStream_t st);
 uint32_t comp_blocks(const ChainSpec &c, const CompTuning &t);
+// Replay of chains that also writes every weighted path: positions x_0 + prefix sums of the
+// segment vectors (exp_pos[chain][step][N+1][3]) and log10 weights (exp_w[chain][step]).
+cudaError_t launch_comp_export(const ChainSpec &c, const CompTuning &t, const float *init_seg, const float2 *logtab,
+                               const float2 *lintab, LutMetaF m, const float x0[3], float *exp_pos, double *exp_w,
+                               ChainOut *out, cudaStream_t st);
+// Adjoint replay: per chain the weight-averaged gradients of log10 w with respect to
+// (mu_s, eps, receiver x, y, z) and the sum of the weights w/10^ref_log10, reduced over
+// chains into grad_out[6].
+cudaError_t launch_comp_adjoint(const ChainSpec &c, const CompTuning &t, const float *init_seg, const float2 *lintab,
+                                LutMetaF m, const float *lut, const float *dmu, const float *deps, float ref_log10,
+                                double *grad_chains, double *grad_out, cudaStream_t st);
 
 // ----------------------------------------------------------- reduction (chain_plain.cu)
 cudaError_t launch_reduce(const ChainOut *chains, uint32_t n, ReduceOut *out, cudaStream_t st);

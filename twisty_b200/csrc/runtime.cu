@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <filesystem>
 #include <fstream>
 #include <functional>
 #include <limits>
@@ -182,6 +183,21 @@ void build_tables(twisty_ctx *ctx, float ds, bool derivatives)
         std::vector<double> h64(host32.begin(), host32.end());
         ck(cudaMemcpyAsync(ctx->lut64.p, h64.data(), sizeof(double) * bins, cudaMemcpyHostToDevice, st), "upload table");
         ck(cudaStreamSynchronize(st), "sync");
+    } else if (p.lut_mode == TWISTY_LUT_FAITHFUL) {
+        if (derivatives) fail(TWISTY_ERR_UNSUPPORTED, "derivative tables need lut_mode FP64");
+        float mm[2];
+        if (!lut_faithful_host(p.mu, p.eps, p.scatter, p.min_bound, p.max_bound, p.bias, p.num_steps_int, bins, ds,
+                               host32.data(), mm))
+            fail(TWISTY_ERR_INVALID_CONFIG, "invalid table parameters");
+        const float max_k = (float)((2.0 / (double)ds) * (double)1.01f);
+        ctx->meta = LutMetaF{0.0f, max_k, (max_k - 0.0f) / (float)(bins - 1), (int32_t)bins};
+        ctx->min_w = mm[0];
+        ctx->max_w = mm[1];
+        ck(ctx->lut64.ensure(sizeof(double) * bins), "alloc table");
+        std::vector<double> h64(host32.begin(), host32.end());
+        ck(cudaMemcpyAsync(ctx->lut32.p, host32.data(), sizeof(float) * bins, cudaMemcpyHostToDevice, st), "upload table");
+        ck(cudaMemcpyAsync(ctx->lut64.p, h64.data(), sizeof(double) * bins, cudaMemcpyHostToDevice, st), "upload table");
+        ck(cudaStreamSynchronize(st), "sync");
     } else {
         // WeightLookupTableIntegral ctor (PathWeightUtils.cpp:281-289), float grid
         const float min_k = 0.0f;
@@ -200,9 +216,8 @@ void build_tables(twisty_ctx *ctx, float ds, bool derivatives)
         s.min_k = min_k;
         s.step = step;
         s.step64 = ((2.0 / (double)ds) * 1.01) / (double)(bins - 1);
-        s.faithful = (p.lut_mode == TWISTY_LUT_FAITHFUL) ? 1 : 0;
+        s.faithful = 0;
         s.derivatives = derivatives ? 1 : 0;
-        if (derivatives && s.faithful) fail(TWISTY_ERR_UNSUPPORTED, "derivative tables need lut_mode FP64");
         ck(ctx->lut64.ensure(sizeof(double) * bins), "alloc table");
         if (derivatives) {
             ck(ctx->dmus.ensure(sizeof(double) * bins), "alloc derivative table");
@@ -411,10 +426,11 @@ void collect(twisty_ctx *ctx, twisty_result *res)
     set_device(ctx);
     ReduceOut r{};
     r.log10_sum = -std::numeric_limits<double>::infinity();
+    // The pass may have been enqueued on any stream; its last event orders the copy.
+    ck(cudaEventSynchronize(ctx->ev[2]), "sync");
     if (ctx->spec.n_chains) {
-        ck(cudaMemcpy(&r, ctx->reduce_out.p, sizeof(r), cudaMemcpyDeviceToHost), "read result");
-    } else {
-        ck(cudaEventSynchronize(ctx->ev[2]), "sync");
+        ck(cudaMemcpyAsync(&r, ctx->reduce_out.p, sizeof(r), cudaMemcpyDeviceToHost, ctx->stream), "read result");
+        ck(cudaStreamSynchronize(ctx->stream), "read result");
     }
     float a = 0, b = 0;
     ck(cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]), "event time");
@@ -456,6 +472,95 @@ twisty_status guard(twisty_ctx *ctx, const std::function<void()> &f)
 }
 
 thread_local std::string g_free_err;
+
+// The angles GeometryRandom_ExportPaths records for five-segment paths
+// (FullExperimentRunnerOptimalPerturb.cpp:318-357), in float.
+void five_segment_angles(const float *p, float out[3])
+{
+    auto sub = [&](int a, int b, float v[3]) {
+        for (int k = 0; k < 3; ++k) v[k] = p[3 * a + k] - p[3 * b + k];
+    };
+    auto norm = [](float v[3]) {
+        const float inv = 1.0f / std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        for (int k = 0; k < 3; ++k) v[k] *= inv;
+    };
+    auto cross = [](const float a[3], const float b[3], float r[3]) {
+        r[0] = a[1] * b[2] - a[2] * b[1];
+        r[1] = a[2] * b[0] - a[0] * b[2];
+        r[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    float s1[3], z[3], x[3], y[3], v[3];
+    sub(2, 1, s1);
+    norm(s1);
+    out[0] = std::acos(s1[2]);
+    out[1] = std::atan2(s1[1], s1[0]);
+    sub(4, 2, z);
+    norm(z);
+    float other[3] = {1.0f, 0.0f, 0.0f};
+    if (std::fabs(z[0]) >= 0.99f) { other[0] = 0.0f; other[1] = 1.0f; }
+    cross(z, other, x);
+    norm(x);
+    cross(z, x, y);
+    sub(3, 2, v);
+    norm(v);
+    out[2] = std::atan2(v[0] * y[0] + v[1] * y[1] + v[2] * y[2], v[0] * x[0] + v[1] * x[1] + v[2] * x[2]);
+}
+
+// BeginPathBatchOutput / GeometryRandom_ExportPaths / EndPathBatchOutput file set
+// (ExperimentRunner.cpp:210-262,303-345,383-396; FullExperimentRunnerOptimalPerturb.cpp:746-856)
+// under dir/GeneratedCurves/. One batch per exported chain, recorded in the .pmd as
+// "chain 0 count".
+void write_path_batch(const char *dir, const twisty_bc &bc, uint32_t N, double log10_norm, const std::vector<float> &pos,
+                      const std::vector<double> &w, const std::vector<uint32_t> &chain_of)
+{
+    namespace fs = std::filesystem;
+    std::error_code ec;
+    const fs::path out = fs::path(dir) / "GeneratedCurves";
+    fs::create_directories(out, ec);
+    if (ec) fail(TWISTY_ERR_IO, "cannot create " + out.string());
+    auto open = [&](const char *name, std::ios::openmode m) {
+        std::ofstream f(out / name, m);
+        if (!f.is_open()) fail(TWISTY_ERR_IO, std::string("cannot open ") + (out / name).string());
+        return f;
+    };
+    {
+        std::ofstream f = open("BoundaryConditions.bcf", std::ios::binary);
+        const float v[13] = {bc.start_pos.x, bc.start_pos.y, bc.start_pos.z, bc.start_dir.x, bc.start_dir.y, bc.start_dir.z,
+                             bc.end_pos.x, bc.end_pos.y, bc.end_pos.z, bc.end_dir.x, bc.end_dir.y, bc.end_dir.z, bc.arclength};
+        f.write(reinterpret_cast<const char *>(v), sizeof(v));
+        f.write(reinterpret_cast<const char *>(&N), sizeof(N));
+    }
+    {
+        std::string name = fs::path(dir).filename().string();
+        if (name.empty()) name = fs::path(dir).parent_path().filename().string();
+        std::ofstream f = open("index.json", std::ios::out);
+        f << "{\n    \"experiment_name\": \"" << name << "\",\n    \"path_batch_links\": []\n}" << std::endl;
+    }
+    std::ofstream pmd = open("Paths_Metadata.pmd", std::ios::out);
+    std::ofstream pbd = open("Paths_Binary.pbd", std::ios::binary);
+    std::ofstream bdt = open("Log10PathWeights_Binary.bdt", std::ios::binary);
+    std::ofstream pwt = open("Log10PathWeights_Text.pwt", std::ios::out);
+    std::ofstream fsb = open("FiveSegment_Binary.bdt", std::ios::binary);
+    const size_t stride = 3 * (size_t)(N + 1);
+    size_t i = 0;
+    while (i < w.size()) {
+        size_t j = i;
+        while (j < w.size() && chain_of[j] == chain_of[i]) ++j;
+        const uint32_t ch = chain_of[i];
+        pmd << ch << " " << 0 << " " << (j - i) << std::endl;
+        pbd.write(reinterpret_cast<const char *>(pos.data() + i * stride), sizeof(float) * stride * (j - i));
+        for (size_t k = i; k < j; ++k) {
+            // the ".bdt" holds linear weights including the normaliser (:751-752)
+            const double lin = std::pow(10.0, w[k] + log10_norm);
+            bdt.write(reinterpret_cast<const char *>(&lin), sizeof(lin));
+            if ((static_cast<uint32_t>((double)(k - i) + ch * (10000.0 / 12.0)) % 10000) == 0) pwt << lin << std::endl;
+            float ang[3] = {0.0f, 0.0f, 0.0f};
+            if (N == 5) five_segment_angles(pos.data() + k * stride, ang);
+            fsb.write(reinterpret_cast<const char *>(ang), sizeof(ang));
+        }
+        i = j;
+    }
+}
 
 }  // namespace
 
@@ -679,7 +784,11 @@ twisty_status twisty_build_lut(twisty_ctx *ctx, float ds, float *lut, twisty_lut
         validate(ctx->p);
         set_device(ctx);
         build_tables(ctx, ds, false);
-        if (lut) ck(cudaMemcpy(lut, ctx->lut32.p, sizeof(float) * ctx->p.num_curvature_steps, cudaMemcpyDeviceToHost), "read table");
+        if (lut) {
+            ck(cudaMemcpyAsync(lut, ctx->lut32.p, sizeof(float) * ctx->p.num_curvature_steps, cudaMemcpyDeviceToHost,
+                               ctx->stream), "read table");
+            ck(cudaStreamSynchronize(ctx->stream), "read table");
+        }
         if (info) {
             info->min_curvature = ctx->meta.min_k;
             info->max_curvature = ctx->meta.max_k;
@@ -747,14 +856,126 @@ twisty_status twisty_export_paths(twisty_ctx *ctx, const twisty_bc *bc, const ch
                                   double *log10w, uint64_t *n_written, twisty_result *res)
 {
     if (!ctx || !bc) return TWISTY_ERR_INVALID_ARGUMENT;
-    (void)dir; (void)max_paths; (void)pos; (void)log10w; (void)n_written; (void)res;
-    return guard(ctx, [&] { fail(TWISTY_ERR_UNSUPPORTED, "path export is not built yet"); });
+    return guard(ctx, [&] {
+        const double t0 = now_ms();
+        prepare(ctx, bc);
+        launch(ctx, ctx->stream);
+        twisty_result r{};
+        collect(ctx, &r);
+        const ChainSpec &c = ctx->spec;
+        const uint32_t N = c.n_segments;
+        std::vector<float> hpos;
+        std::vector<double> hw;
+        std::vector<uint32_t> chain_of;
+        if (max_paths > 0 && c.n_chains > 0) {
+            // replay the first E chains with every weighted path written out
+            const uint64_t E64 = std::min<uint64_t>(c.n_chains, (max_paths + c.steps - 1) / c.steps);
+            const uint32_t E = (uint32_t)E64;
+            ChainSpec ce = c;
+            ce.n_chains = E;
+            ce.last_steps = (E == c.n_chains) ? c.last_steps : c.steps;
+            const size_t npaths = (size_t)E * c.steps;
+            DevBuf dpos, dw, dout;
+            try {
+                ck(dpos.ensure(sizeof(float) * 3 * (size_t)(N + 1) * npaths), "alloc export buffer");
+                ck(dw.ensure(sizeof(double) * npaths), "alloc export buffer");
+                ck(dout.ensure(sizeof(ChainOut) * E), "alloc export buffer");
+                ck(cudaMemsetAsync(dw.p, 0xff, sizeof(double) * npaths, ctx->stream), "memset");  // NaN: not written
+                if (ctx->p.form == TWISTY_FORM_PLAIN_FP32) {
+                    ck(launch_plain_chains(ce, ctx->init_pos.as<float>(), ctx->state.as<float>(), ctx->lut32.as<float>(),
+                                           ctx->meta, dout.as<ChainOut>(), ctx->stream, dpos.as<float>(), dw.as<double>()),
+                       "export replay");
+                } else if (ctx->p.form == TWISTY_FORM_COMPENSATED) {
+                    const float x0[3] = {bc->start_pos.x, bc->start_pos.y, bc->start_pos.z};
+                    ck(launch_comp_export(ce, ctx->tuning, ctx->init_seg.as<float>(), ctx->logtab.as<float2>(),
+                                          ctx->lintab.as<float2>(), ctx->meta, x0, dpos.as<float>(), dw.as<double>(),
+                                          dout.as<ChainOut>(), ctx->stream),
+                       "export replay");
+                } else {
+                    fail(TWISTY_ERR_UNSUPPORTED, "path export runs the plain and compensated forms");
+                }
+                std::vector<float> apos(3 * (size_t)(N + 1) * npaths);
+                std::vector<double> aw(npaths);
+                ck(cudaMemcpyAsync(apos.data(), dpos.p, sizeof(float) * apos.size(), cudaMemcpyDeviceToHost, ctx->stream), "read export");
+                ck(cudaMemcpyAsync(aw.data(), dw.p, sizeof(double) * npaths, cudaMemcpyDeviceToHost, ctx->stream), "read export");
+                ck(cudaStreamSynchronize(ctx->stream), "export");
+                // invalid paths are skipped, as the reference skips them before exporting
+                for (uint32_t ch = 0; ch < E && hw.size() < max_paths; ++ch) {
+                    const uint32_t steps = (ch == c.n_chains - 1) ? c.last_steps : c.steps;
+                    for (uint32_t s = 0; s < steps && hw.size() < max_paths; ++s) {
+                        const size_t i = (size_t)ch * c.steps + s;
+                        if (!std::isfinite(aw[i])) continue;
+                        hw.push_back(aw[i]);
+                        chain_of.push_back(ch);
+                        hpos.insert(hpos.end(), apos.begin() + i * 3 * (N + 1), apos.begin() + (i + 1) * 3 * (N + 1));
+                    }
+                }
+            } catch (...) {
+                dpos.release(); dw.release(); dout.release();
+                throw;
+            }
+            dpos.release(); dw.release(); dout.release();
+        }
+        const uint64_t n = hw.size();
+        if (pos && n) std::memcpy(pos, hpos.data(), sizeof(float) * hpos.size());
+        if (log10w && n) std::memcpy(log10w, hw.data(), sizeof(double) * n);
+        if (n_written) *n_written = n;
+        if (dir) write_path_batch(dir, *bc, N, ctx->log10_norm, hpos, hw, chain_of);
+        r.total_ms = now_ms() - t0;
+        if (res) *res = r;
+    });
 }
 
 twisty_status twisty_adjoint(twisty_ctx *ctx, const twisty_bc *bc, const twisty_result *fwd, double grad[5])
 {
     if (!ctx || !bc || !fwd || !grad) return TWISTY_ERR_INVALID_ARGUMENT;
-    return guard(ctx, [&] { fail(TWISTY_ERR_UNSUPPORTED, "the adjoint is not built yet"); });
+    return guard(ctx, [&] {
+        if (ctx->p.form != TWISTY_FORM_COMPENSATED) fail(TWISTY_ERR_UNSUPPORTED, "the adjoint replays the compensated form");
+        if (ctx->p.lut_mode != TWISTY_LUT_FP64) fail(TWISTY_ERR_UNSUPPORTED, "the adjoint needs lut_mode FP64 (derivative tables)");
+        prepare(ctx, bc);
+        const uint32_t N = ctx->p.num_segments;
+        const float ds = bc->arclength / (float)N;
+        build_tables(ctx, ds, true);
+        const uint32_t bins = ctx->p.num_curvature_steps;
+        std::vector<double> hmu(bins), heps(bins);
+        ck(cudaMemcpyAsync(hmu.data(), ctx->dmus.p, sizeof(double) * bins, cudaMemcpyDeviceToHost, ctx->stream), "read derivative table");
+        ck(cudaMemcpyAsync(heps.data(), ctx->deps.p, sizeof(double) * bins, cudaMemcpyDeviceToHost, ctx->stream), "read derivative table");
+        ck(cudaStreamSynchronize(ctx->stream), "read derivative table");
+        std::vector<float> f(2 * (size_t)bins);
+        for (uint32_t i = 0; i < bins; ++i) {
+            f[i] = (float)hmu[i];
+            f[bins + i] = (float)heps[i];
+        }
+        const ChainSpec &c = ctx->spec;
+        DevBuf dtab, dg, dout;
+        try {
+            ck(dtab.ensure(sizeof(float) * f.size()), "alloc");
+            ck(dg.ensure(sizeof(double) * 6 * std::max<uint32_t>(c.n_chains, 1)), "alloc");
+            ck(dout.ensure(sizeof(double) * 6), "alloc");
+            ck(cudaMemcpyAsync(dtab.p, f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice, ctx->stream), "upload");
+            const double ref = fwd->log10_weight - fwd->log10_normalizer - (double)(N - 1) * std::log10(c.absorption_factor);
+            CompTuning t = ctx->tuning;
+            t.exact_blend = 1;
+            ck(launch_comp_adjoint(c, t, ctx->init_seg.as<float>(), ctx->lintab.as<float2>(), ctx->meta,
+                                   ctx->lut32.as<float>(), dtab.as<float>(), dtab.as<float>() + bins, (float)ref,
+                                   dg.as<double>(), dout.as<double>(), ctx->stream),
+               "adjoint kernel");
+            double g[6];
+            ck(cudaMemcpyAsync(g, dout.p, sizeof(g), cudaMemcpyDeviceToHost, ctx->stream), "read gradient");
+            ck(cudaStreamSynchronize(ctx->stream), "adjoint");
+            if (!(g[5] > 0.0)) fail(TWISTY_ERR_INVALID_ARGUMENT, "forward result does not match this experiment");
+            const double sigma = std::sqrt((double)ctx->p.eps);
+            grad[0] = g[0] / g[5];
+            grad[1] = g[1] / g[5] * 2.0 * sigma;   // eps = sigma^2
+            grad[2] = g[2] / g[5];
+            grad[3] = g[3] / g[5];
+            grad[4] = g[4] / g[5];
+        } catch (...) {
+            dtab.release(); dg.release(); dout.release();
+            throw;
+        }
+        dtab.release(); dg.release(); dout.release();
+    });
 }
 
 twisty_status twisty_set_initial_curve(twisty_ctx *ctx, const float *pos, uint32_t n_points)
