@@ -1,0 +1,60 @@
+"""The cross-rank exchange step (twisty_b200.dist) on CPU with gloo, world size 2."""
+import math
+import os
+import socket
+
+import pytest
+import torch.multiprocessing as mp
+
+from twisty_b200 import dist as D
+
+
+class R:
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+
+PARTS = [
+    dict(log10_weight=-290.25, rel_std_error=0.01, total_paths=1000, failed_paths=1, clamped_curvatures=3, num_chains=10),
+    dict(log10_weight=-290.75, rel_std_error=0.02, total_paths=900, failed_paths=0, clamped_curvatures=1, num_chains=9),
+]
+
+
+def test_combine_math():
+    c = D.combine([D.local_tuple(R(**p)) for p in PARTS])
+    a, b = 10 ** 0.0, 10 ** -0.5   # relative to the larger
+    assert c["log10_weight"] == pytest.approx(-290.25 + math.log10(a + b), abs=1e-12)
+    assert c["rel_std_error"] == pytest.approx(math.hypot(0.01 * a, 0.02 * b) / (a + b), rel=1e-12)
+    assert (c["total_paths"], c["failed_paths"], c["clamped_curvatures"], c["num_chains"]) == (1900, 1, 4, 19)
+    # a rank with no valid path contributes nothing but its counts
+    e = D.combine([D.local_tuple(R(**PARTS[0])),
+                   [-math.inf, math.nan, 0, 5, 0, 4]])
+    assert e["log10_weight"] == pytest.approx(-290.25) and e["failed_paths"] == 6
+
+
+def _worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        q.put((rank, D.all_combine(R(**PARTS[rank]))))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_all_combine_gloo_two_ranks():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = dict(q.get(timeout=120) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    ref = D.combine([D.local_tuple(R(**p)) for p in PARTS])
+    assert out[0] == out[1] == ref

@@ -232,34 +232,24 @@ struct ModeArgs {
     double *grad;        // [chains][6]: d/dmu_s, d/deps, d/dx, d/dy, d/dz (log10 units), sum of weights
 };
 
-template <int G, int SPL, bool EXACT, int MAXT, int MODE>
-__global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompConsts kc,
-                                                             const float *__restrict__ init_seg,
-                                                             const float2 *__restrict__ tab_g,
-                                                             ChainOut *__restrict__ out,
-                                                             double2 *__restrict__ block_partials, ModeArgs ma)
+// Stage a table of `bins` float2 entries into shared memory (float4 vector loads).
+__device__ __forceinline__ void stage_table(float4 *smem4, const float2 *__restrict__ tab_g, int bins)
 {
-    extern __shared__ float4 smem4[];
-    const int bins = kc.bins;
-    float2 *s_tab = reinterpret_cast<float2 *>(smem4);
-    const int tab_f4 = (bins + 1) / 2;  // float2 entries, padded to float4
-    float *s_state = reinterpret_cast<float *>(smem4 + tab_f4);
-    const int warps = blockDim.x >> 5;
-    double *s_res = reinterpret_cast<double *>(s_state + warps * 3 * SPL * 32);
+    for (int i = threadIdx.x; i < bins / 2; i += blockDim.x) smem4[i] = reinterpret_cast<const float4 *>(tab_g)[i];
+    if ((bins & 1) && threadIdx.x == 0) reinterpret_cast<float2 *>(smem4)[bins - 1] = tab_g[bins - 1];
+}
 
-    for (int i = threadIdx.x; i < bins / 2; i += blockDim.x)
-        smem4[i] = reinterpret_cast<const float4 *>(tab_g)[i];
-    if ((bins & 1) && threadIdx.x == 0) s_tab[bins - 1] = tab_g[bins - 1];
-
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t q = lane / G, j = lane % G, gbase = q * G;
-    constexpr int CPW = 32 / G;
-    const uint32_t chain = (blockIdx.x * warps + warp) * CPW + q;
-    const bool real_chain = chain < c.n_chains;
+// One Markov chain run by the G lanes of one group, on its own shared-memory segment
+// planes sx/sy/sz: initial state from init_seg, burn_in + steps proposals, a full
+// recompute of every weighted path, and the chain's running log-sum-exp. Writes out[chain]
+// (when out is set and the chain is real) and returns the chain's log10 sum.
+template <int G, int SPL, bool EXACT, int MODE>
+__device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConsts &kc,
+                                             const float *__restrict__ init_seg, const float2 *s_tab, float *sx,
+                                             float *sy, float *sz, uint32_t gbase, uint32_t j, uint32_t chain,
+                                             bool real_chain, ChainOut *__restrict__ out, const ModeArgs &ma)
+{
     const uint32_t N = c.n_segments;
-    float *sx = s_state + warp * 3 * SPL * 32;
-    float *sy = sx + SPL * 32;
-    float *sz = sy + SPL * 32;
     using Lay = Layout<G, SPL>;
 
 #pragma unroll
@@ -271,7 +261,7 @@ __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompCo
         sy[a] = in ? init_seg[3 * s + 1] : 0.f;
         sz[a] = in ? init_seg[3 * s + 2] : 0.f;
     }
-    __syncthreads();
+    __syncwarp();
 
     const uint32_t steps_c = real_chain ? ((chain == c.n_chains - 1) ? c.last_steps : c.steps) : 0;
     const uint32_t total = c.burn_in + c.steps;
@@ -485,19 +475,43 @@ __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompCo
     const double chain_log10 = valid ? (double)lse_m + log10((double)lse_s - (double)lse_c) +
                                        (double)(N - 1) * ma.log10_abs
                                      : -INFINITY;
-    const uint32_t slot = warp * CPW + q;
-    if (j == 0) {
-        s_res[slot] = real_chain ? chain_log10 : -INFINITY;
-        if (real_chain && out) {
-            ChainOut o;
-            o.log10_sum = chain_log10;
-            o.valid = valid;
-            o.failed = failed;
-            o.clamped = clamped;
-            o.pad = 0;
-            out[chain] = o;
-        }
+    if (j == 0 && real_chain && out) {
+        ChainOut o;
+        o.log10_sum = chain_log10;
+        o.valid = valid;
+        o.failed = failed;
+        o.clamped = clamped;
+        o.pad = 0;
+        out[chain] = o;
     }
+    return real_chain ? chain_log10 : -INFINITY;
+}
+
+template <int G, int SPL, bool EXACT, int MAXT, int MODE>
+__global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompConsts kc,
+                                                             const float *__restrict__ init_seg,
+                                                             const float2 *__restrict__ tab_g,
+                                                             ChainOut *__restrict__ out,
+                                                             double2 *__restrict__ block_partials, ModeArgs ma)
+{
+    extern __shared__ float4 smem4[];
+    const int bins = kc.bins;
+    const float2 *s_tab = reinterpret_cast<const float2 *>(smem4);
+    const int tab_f4 = (bins + 1) / 2;  // float2 entries, padded to float4
+    float *s_state = reinterpret_cast<float *>(smem4 + tab_f4);
+    const int warps = blockDim.x >> 5;
+    double *s_res = reinterpret_cast<double *>(s_state + warps * 3 * SPL * 32);
+    stage_table(smem4, tab_g, bins);
+    __syncthreads();
+
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t q = lane / G, j = lane % G;
+    constexpr int CPW = 32 / G;
+    const uint32_t chain = (blockIdx.x * warps + warp) * CPW + q;
+    float *sx = s_state + warp * 3 * SPL * 32;
+    const double cl = chain_body<G, SPL, EXACT, MODE>(c, kc, init_seg, s_tab, sx, sx + SPL * 32, sx + 2 * SPL * 32,
+                                                      q * G, j, chain, chain < c.n_chains, out, ma);
+    if (j == 0) s_res[warp * CPW + q] = cl;
     __syncthreads();
     // Per-CTA log-sum-exp of the chains, rescaled by the block maximum (FP64).
     if (warp == 0 && block_partials) {

@@ -1,0 +1,51 @@
+"""Sharding one experiment over ranks (one process per GPU) and combining the results.
+
+Every rank runs the same experiment with a disjoint range of chain ids
+(``chain_offset = rank * chains``), so the chains of all ranks are independent draws of the
+same Markov process and the estimate is their sum. The one exchange step combines the
+per-rank results: log10 sums by log-sum-exp, absolute standard errors in quadrature (the
+ranks' chains are independent), counts by addition. It moves 6 doubles per rank.
+"""
+from __future__ import annotations
+
+import math
+from typing import Sequence
+
+FIELDS = ("log10_weight", "rel_std_error", "total_paths", "failed_paths", "clamped_curvatures", "num_chains")
+
+
+def combine(parts: Sequence[Sequence[float]]) -> dict:
+    """Combine per-rank tuples ordered as FIELDS (the normaliser is a common factor)."""
+    logs = [p[0] for p in parts if p[0] > -math.inf]
+    if not logs:
+        m = -math.inf
+        total = 0.0
+    else:
+        m = max(logs)
+        total = sum(10.0 ** (p[0] - m) for p in parts if p[0] > -math.inf)
+    var = 0.0
+    for p in parts:
+        if p[0] > -math.inf and not math.isnan(p[1]):
+            var += (p[1] * 10.0 ** (p[0] - m)) ** 2
+    return {
+        "log10_weight": m + math.log10(total) if total > 0 else -math.inf,
+        "rel_std_error": math.sqrt(var) / total if total > 0 else math.nan,
+        "total_paths": int(sum(p[2] for p in parts)),
+        "failed_paths": int(sum(p[3] for p in parts)),
+        "clamped_curvatures": int(sum(p[4] for p in parts)),
+        "num_chains": int(sum(p[5] for p in parts)),
+    }
+
+
+def local_tuple(result) -> list:
+    return [float(getattr(result, f)) for f in FIELDS]
+
+
+def all_combine(result, group=None, device=None) -> dict:
+    """All-gather the per-rank result tuples over torch.distributed and combine them."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(local_tuple(result), dtype=torch.float64, device=device)
+    parts = [torch.empty_like(t) for _ in range(dist.get_world_size(group))]
+    dist.all_gather(parts, t, group=group)
+    return combine([p.tolist() for p in parts])
