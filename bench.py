@@ -233,7 +233,10 @@ def main():
     ap.add_argument("--no-error", action="store_true", help="skip the FP64 error measurement")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP32 drop-in")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--paths", type=int, default=0, help="paths per pass (default 2^26; smaller for profiling)")
     args = ap.parse_args()
+    if args.paths:
+        W["paths"] = args.paths
     if args.impl == "reference":
         return run_reference_arm(args)
 
