@@ -249,6 +249,54 @@ twisty_status twisty_export_paths(twisty_ctx *ctx, const twisty_bc *bc, const ch
 twisty_status twisty_adjoint(twisty_ctx *ctx, const twisty_bc *bc, const twisty_result *fwd,
                              double grad[5]);
 
+/* ------------------------------------------------------- allocation-free pass */
+/* No counterpart in the reference. For callers that cannot allocate device memory when
+ * they run a pass: an application whose own caching allocator holds nearly all of the
+ * GPU (a library cudaMalloc behind its back can fail or upset its accounting), or a
+ * pipeline that must not stall (cudaMalloc and cudaFree may synchronize the device).
+ * twisty_run_noalloc runs one compensated-form Monte Carlo pass over the caller's device
+ * inputs and writes a twisty_noalloc_result to the caller's device memory; it calls no
+ * cudaMalloc, cudaFree or other allocating routine. Its per-chain scratch is a fixed array
+ * compiled into the library (TWISTY_NOALLOC_MAX_CHAINS chains, 24 bytes each: 384 KiB held
+ * on every GPU that loads the library, until the process exits); more chains are rejected
+ * with TWISTY_ERR_INVALID_ARGUMENT.
+ *
+ * It runs on the calling thread's current device, enqueued on `stream` (NULL: the legacy
+ * default stream). The first call on each device looks up that device's address of the
+ * scratch array; make that first call before any stream capture on the device. Every
+ * call writes each scratch entry it later reads, so nothing carries over between calls,
+ * but all calls share the one array: calls that overlap on the GPU (concurrent streams,
+ * threads) race on it and must be ordered by the caller. */
+#define TWISTY_NOALLOC_MAX_CHAINS 16384u
+
+typedef struct twisty_noalloc_args {
+    const void *table;           /* device float2[bins]: (L_i, L_{i+1} - L_i); last (L_{bins-1}, 0) */
+    uint32_t bins;
+    float min_curvature, max_curvature, curvature_step;
+    const float *init_segments;  /* device float[3 * N]: x_{i+1} - x_i of the initial curve */
+    uint32_t num_segments;       /* 4 <= N <= 1024 */
+    float arclength;
+    float absorption;            /* mu_a */
+    uint64_t seed;
+    uint32_t experiment_id;
+    uint32_t chain_offset;
+    uint32_t num_chains;         /* 1 .. TWISTY_NOALLOC_MAX_CHAINS */
+    uint64_t paths;              /* weighted paths of the pass */
+    uint32_t burn_in;            /* unweighted steps per chain */
+    uint32_t max_sub_chain;      /* 2 .. 64 */
+    float max_angle;             /* [0, pi] */
+    void *result;                /* device twisty_noalloc_result */
+} twisty_noalloc_args;
+
+typedef struct twisty_noalloc_result {
+    double log10_weight;         /* log10 of the summed path weights (normaliser not applied) */
+    double rel_std_error;
+    double max_chain_log10;
+    uint64_t valid_paths, failed_paths, clamped_curvatures;
+} twisty_noalloc_result;
+
+twisty_status twisty_run_noalloc(const twisty_noalloc_args *args, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

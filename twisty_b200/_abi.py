@@ -103,6 +103,24 @@ class Experiment(C.Structure):
                 ("paths", C.c_uint64)]
 
 
+NOALLOC_MAX_CHAINS = 16384
+
+
+class NoAllocArgs(C.Structure):
+    """twisty_noalloc_args: every pointer is device memory owned by the caller."""
+    _fields_ = [("table", C.c_void_p), ("bins", C.c_uint32), ("min_curvature", C.c_float),
+                ("max_curvature", C.c_float), ("curvature_step", C.c_float), ("init_segments", C.c_void_p),
+                ("num_segments", C.c_uint32), ("arclength", C.c_float), ("absorption", C.c_float),
+                ("seed", C.c_uint64), ("experiment_id", C.c_uint32), ("chain_offset", C.c_uint32),
+                ("num_chains", C.c_uint32), ("paths", C.c_uint64), ("burn_in", C.c_uint32),
+                ("max_sub_chain", C.c_uint32), ("max_angle", C.c_float), ("result", C.c_void_p)]
+
+
+class NoAllocResult(C.Structure):
+    _fields_ = [("log10_weight", C.c_double), ("rel_std_error", C.c_double), ("max_chain_log10", C.c_double),
+                ("valid_paths", C.c_uint64), ("failed_paths", C.c_uint64), ("clamped_curvatures", C.c_uint64)]
+
+
 # (name, restype, argtypes): every entry point declared in include/twisty_b200.h
 _P = C.c_void_p
 SIGNATURES = [
@@ -130,6 +148,7 @@ SIGNATURES = [
     ("twisty_export_paths", C.c_int, [_P, C.POINTER(BC), C.c_char_p, C.c_uint64, _P, _P, C.POINTER(C.c_uint64),
                                       C.POINTER(Result)]),
     ("twisty_adjoint", C.c_int, [_P, C.POINTER(BC), C.POINTER(Result), C.POINTER(C.c_double)]),
+    ("twisty_run_noalloc", C.c_int, [C.POINTER(NoAllocArgs), _P]),
 ]
 
 _lib = None

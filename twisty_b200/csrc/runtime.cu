@@ -564,6 +564,11 @@ void write_path_batch(const char *dir, const twisty_bc &bc, uint32_t N, double l
 
 }  // namespace
 
+namespace twisty {
+// Message returned by twisty_last_error(NULL) for entry points without a context.
+void set_free_error(const std::string &msg) { g_free_err = msg; }
+}  // namespace twisty
+
 extern "C" {
 
 int twisty_abi_version(void) { return TWISTY_B200_ABI_VERSION; }
