@@ -8,26 +8,29 @@
 //
 // B200 layout and arithmetic:
 //  * G lanes cooperate on one chain (G = 8, 16 or 32); lane j owns the SPL contiguous
-//    segments j*SPL .. j*SPL+SPL-1. The chain lives in shared memory as its N segment
-//    vectors v_i = x_{i+1} - x_i (three planes x/y/z). A rotation of the points between
-//    left and right about the chord x_right - x_left maps every segment vector
-//    v_left .. v_{right-1} by the same rotation (the chord is the axis, so it is fixed),
-//    which keeps segment-scale magnitudes (|v| ~ ds) instead of absolute positions in the
-//    FP32 state: the rounding of the state is relative to ds, not to |x|.
+//    segments j*SPL .. j*SPL+SPL-1. The chain lives in shared memory as its N unit tangents
+//    t_i and segment lengths l_i (four planes). Rotating the points between left and right
+//    about the chord x_right - x_left turns every tangent t_left .. t_{right-1} by the same
+//    rotation (the chord is the axis and stays fixed) and leaves the lengths alone; each
+//    rotated tangent is renormalised by one Newton step, so |t_i| = 1 to an ulp and the
+//    full recompute needs no normalisation: kappa_i = |t_{i+1} - t_i| N/S.
 //  * Shared-memory address of segment s = j*SPL + m of the chain in lanes q*G..q*G+G-1:
 //    row m, column (q*G + j + m*C) mod 32 with C = max(1, G/SPL). Rows make the full
 //    recompute (all lanes, same m) conflict-free; the column shift spreads the k
 //    consecutive segments of a rotation over distinct banks (at most 2-way conflicts).
-//  * The table is staged once per CTA in shared memory as float2 (log10 L_i, secant slope),
-//    so a segment's log-weight is one 8-byte LDS and one FMA; when the secant is not
-//    accurate to 1e-7 per segment the host selects EXACT mode ((L_i, L_{i+1}-L_i) and a
-//    log2). The per-path log10 sum is Kahan-compensated in FP32 and combined across lanes
-//    with TwoSum; the chain's running sum is a log-sum-exp accumulator rescaled by its
-//    running maximum (FP32 with a compensated mantissa sum). FP64 appears only in the
-//    per-CTA log-sum-exp reduction of the chains and the global reduction.
+//  * The table is staged once per CTA in shared memory as float2. In the fixed-point form
+//    entry i holds round((log10 L_i - c0) 2^s) as int32 bits and the secant slope of
+//    log10 of the blend over the bin: a segment costs one 8-byte LDS, one integer add (exact)
+//    and one FMA (the interpolation correction), and lanes combine their sums exactly with
+//    integer adds. When the fixed point or the secant would lose more than ~1e-7 per
+//    segment, the host selects the exact form: (L_i, L_{i+1} - L_i), a log2 per segment and a
+//    Kahan-compensated FP32 sum combined across lanes by TwoSum.
+//  * The chain's running sum is a log-sum-exp accumulator: reference exponent = the running
+//    maximum, mantissa sum Kahan-compensated in FP32, rescaled when a new maximum arrives.
+//    FP64 appears only per path (assembling the log10 weight), in the per-CTA log-sum-exp
+//    of the chains and in the global reduction.
 //  * Proposals: lane j of a group draws the Philox proposal of step base+j (one draw per
-//    lane per G steps) and shuffles broadcast it, so the RNG costs 1/G of a draw per lane
-//    per step.
+//    lane per G steps) and shuffles broadcast it.
 #include "kernels.h"
 #include "device_common.cuh"
 
@@ -37,7 +40,7 @@ namespace twisty {
 namespace {
 
 constexpr uint32_t FULL = 0xffffffffu;
-constexpr int kMaxSubChain = 64;            // largest k the rotation rounds cover
+constexpr int kMaxSubChain = 64;  // largest k the rotation rounds cover
 constexpr float kLog2_10 = 3.32192809488736234787f;
 constexpr float kLog10_2 = 0.30102999566398119521f;
 constexpr float kInvLn10 = 0.43429448190325182765f;
@@ -49,6 +52,8 @@ struct CompConsts {
     float rsnap;         // 1e-3 / step: overshoot that counts as clamped
     float step;
     int32_t bins;
+    double lw_offset;    // (N-1) c0 of the fixed-point table
+    double inv_scale;    // 2^-s of the fixed-point table
 };
 
 __device__ __forceinline__ float sqrt_approx(float x)
@@ -69,8 +74,8 @@ __device__ __forceinline__ void group_sum3(float &x, float &y, float &z)
     }
 }
 
-template <int G>
-__device__ __forceinline__ uint32_t group_sum_u(uint32_t v)
+template <int G, class T>
+__device__ __forceinline__ T group_sum(T v)
 {
 #pragma unroll
     for (int o = 1; o < G; o <<= 1) v += __shfl_xor_sync(FULL, v, o);
@@ -101,49 +106,64 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float x)
     s = t;
 }
 
-// Log-weight of one segment given |t_{i+1}-t_i|^2; NaN propagates to mark the path invalid.
-template <bool EXACT>
-__device__ __forceinline__ float segment_term(float qq, const float2 *__restrict__ tab, const CompConsts &k,
-                                              uint32_t &clamped, int32_t *bin_out)
+// Per-lane partial of one path's log10 weight. ISUM is uint32_t where the table was built
+// for this lane's segment count, uint64_t where any count must fit.
+template <class ISUM>
+struct PathAcc {
+    ISUM isum;       // fixed point: sum of the uint32 entries
+    float csum;      // fixed point: sum of the interpolation corrections (NaN marks an invalid path)
+    float ks, kc;    // exact: Kahan pair
+};
+
+// One segment: |t_{i+1}-t_i|^2 -> bin -> table -> accumulate. CLAMP handles tables whose
+// curvature range the path can leave; tables spanning [0, 2.02 N/S] (the reference's)
+// cannot be left by unit tangents (|t_{i+1}-t_i| <= 2).
+template <bool EXACT, bool CLAMP, class ISUM>
+__device__ __forceinline__ void segment(float qq, const float2 *__restrict__ tab, const CompConsts &k, PathAcc<ISUM> &a,
+                                        uint32_t &clamped, int32_t *bin_out)
 {
     float r = fmaf(sqrt_approx(qq), k.kscale, k.roff);
-    if (r < 0.0f) r = 0.0f;
-    if (r > k.rmax) {
-        clamped += (r - k.rmax >= k.rsnap) ? 1u : 0u;
-        r = k.rmax;
+    if (CLAMP) {
+        if (r < 0.0f) r = 0.0f;
+        if (r > k.rmax) {
+            clamped += (r - k.rmax >= k.rsnap) ? 1u : 0u;
+            r = k.rmax;
+        }
     }
+    // r >= 0 or NaN here (NaN converts to 0); the bound also keeps a non-finite tangent,
+    // which only a degenerate zero-length chord can produce, inside the table
     const int32_t L = min((int32_t)r, k.bins - 1);
     if (bin_out) *bin_out = isnan(r) ? -1 : L;
     const float d = (r - (float)L) * k.step;
     const float2 e = tab[L];
-    if (EXACT) return __log2f(fmaf(d, e.y, e.x)) * kLog10_2;
-    return fmaf(d, e.y, e.x);
+    if (EXACT) {
+        kahan_add(a.ks, a.kc, __log2f(fmaf(d, e.y, e.x)) * kLog10_2);
+    } else {
+        a.isum += (ISUM)__float_as_uint(e.x);
+        a.csum = fmaf(d, e.y, a.csum);
+    }
 }
 
-// Full recompute of one path's log10 weight from its segment vectors. seg(m, x, y, z)
-// loads segment j*SPL+m of this lane. Returns the group-wide (hi, lo).
-template <int G, int SPL, bool EXACT, class SegFn, class BinFn>
-__device__ __forceinline__ void path_log10(uint32_t j, uint32_t N, const float2 *__restrict__ tab,
-                                           const CompConsts &k, SegFn seg, BinFn bin_sink, float &hi,
-                                           float &lo, uint32_t &clamped)
+// Full recompute of one path's log10 weight. tan(m, x, y, z) gives the unit tangent of
+// segment j*SPL+m of this lane. Returns the group-wide log10 weight (absorption excluded).
+template <int G, int SPL, bool EXACT, bool CLAMP, class ISUM, class TanFn, class BinFn>
+__device__ __forceinline__ double path_log10(uint32_t j, uint32_t N, const float2 *__restrict__ tab,
+                                             const CompConsts &k, TanFn tan, BinFn bin_sink, uint32_t &clamped)
 {
-    float s = 0.0f, c = 0.0f;
+    PathAcc<ISUM> a{0, 0.0f, 0.0f, 0.0f};
     float t0x = 0.f, t0y = 0.f, t0z = 0.f, px = 0.f, py = 0.f, pz = 0.f;
     const uint32_t base = j * SPL;
 #pragma unroll
     for (int m = 0; m < SPL; ++m) {
-        float vx, vy, vz;
-        seg(m, vx, vy, vz);
-        const float rs = rsqrtf(fmaf(vx, vx, fmaf(vy, vy, vz * vz)));
-        const float tx = vx * rs, ty = vy * rs, tz = vz * rs;
+        float tx, ty, tz;
+        tan(m, tx, ty, tz);
         if (m == 0) {
             t0x = tx; t0y = ty; t0z = tz;
         } else if (base + m <= N - 1) {
             const float dx = tx - px, dy = ty - py, dz = tz - pz;
             int32_t b;
-            const float term = segment_term<EXACT>(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), tab, k, clamped, &b);
+            segment<EXACT, CLAMP, ISUM>(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), tab, k, a, clamped, &b);
             bin_sink(base + m - 1, b);
-            kahan_add(s, c, term);
         }
         px = tx; py = ty; pz = tz;
     }
@@ -153,13 +173,17 @@ __device__ __forceinline__ void path_log10(uint32_t j, uint32_t N, const float2 
     if (base + SPL <= N - 1) {
         const float dx = nx - px, dy = ny - py, dz = nz - pz;
         int32_t b;
-        const float term = segment_term<EXACT>(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), tab, k, clamped, &b);
+        segment<EXACT, CLAMP, ISUM>(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), tab, k, a, clamped, &b);
         bin_sink(base + SPL - 1, b);
-        kahan_add(s, c, term);
     }
-    hi = s;
-    lo = -c;
-    group_sum_pair<G>(hi, lo);
+    if (EXACT) {
+        float hi = a.ks, lo = -a.kc;
+        group_sum_pair<G>(hi, lo);
+        return (double)hi + (double)lo;
+    }
+    const unsigned long long is = group_sum<G>((unsigned long long)a.isum);
+    const float cs = group_sum<G>(a.csum);
+    return k.lw_offset + (double)is * k.inv_scale + (double)cs;
 }
 
 template <int G, int SPL>
@@ -173,26 +197,31 @@ struct Layout {
 
 enum { kModeForward = 0, kModeExport = 1, kModeAdjoint = 2 };
 
-// Receiver-position gradient of one path's log10 weight, computed by one lane from the
-// last three segment vectors: moving the receiver moves points N-1 and N together, so only
-// v_{N-2} changes, hence t_{N-2} and the curvatures kappa_{N-3}, kappa_{N-2}. The table's
-// slope is taken per bin, (L_{i+1} - L_i) / step, the derivative of the curve the table
+struct ModeArgs {
+    double log10_abs;    // log10 of the per-segment absorption factor
+    // export
+    float *exp_pos;      // [chains][steps][N+1][3]
+    double *exp_w;       // [chains][steps] log10 weights (absorption included, normaliser not)
+    float x0[3];
+    // adjoint
+    const float *lut;    // float table
+    const float *dmu;    // d table / d mu_s
+    const float *deps;   // d table / d eps
+    float ref_log10;     // log10 of the forward sum of path weights (normaliser and absorption excluded)
+    double *grad;        // [chains][6]: d/dmu_s, d/deps, d/dx, d/dy, d/dz (log10 units), sum of weights
+};
+
+// Receiver-position gradient of one path's log10 weight, computed by one lane from the last
+// three segments: moving the receiver moves points N-1 and N together, so only the segment
+// vector v_{N-2} changes, hence t_{N-2} and the curvatures kappa_{N-3}, kappa_{N-2}. The
+// table's slope is taken per bin, (L_{i+1} - L_i) / step, the derivative of the curve the table
 // samples (the reference's interpolation weight in curvature units makes its own weight
 // almost piecewise constant within a bin, a slope finite differences do not see).
-__device__ __forceinline__ void receiver_grad(const float *sx, const float *sy, const float *sz, uint32_t a3,
-                                              uint32_t a2, uint32_t a1, const float *__restrict__ lut,
-                                              const CompConsts &k, float inv_ds, float g[3])
+__device__ __forceinline__ void receiver_grad(const float t3[3], const float t2[3], const float t1[3], float len2,
+                                              const float *__restrict__ lut, const CompConsts &k, float inv_ds,
+                                              float g[3])
 {
-    const float v3x = sx[a3], v3y = sy[a3], v3z = sz[a3];   // v_{N-3}
-    const float v2x = sx[a2], v2y = sy[a2], v2z = sz[a2];   // v_{N-2}
-    const float v1x = sx[a1], v1y = sy[a1], v1z = sz[a1];   // v_{N-1}
-    const float r3 = rsqrtf(fmaf(v3x, v3x, fmaf(v3y, v3y, v3z * v3z)));
-    const float r2 = rsqrtf(fmaf(v2x, v2x, fmaf(v2y, v2y, v2z * v2z)));
-    const float r1 = rsqrtf(fmaf(v1x, v1x, fmaf(v1y, v1y, v1z * v1z)));
-    const float t3[3] = {v3x * r3, v3y * r3, v3z * r3};
-    const float t2[3] = {v2x * r2, v2y * r2, v2z * r2};
-    const float t1[3] = {v1x * r1, v1y * r1, v1z * r1};
-    // d t2 / d v2 = (I - t2 t2^T) * r2
+    const float r2 = 1.0f / len2;  // d t2 / d v2 = (I - t2 t2^T) / |v2|
     g[0] = g[1] = g[2] = 0.f;
     for (int which = 0; which < 2; ++which) {
         float d[3];
@@ -209,28 +238,12 @@ __device__ __forceinline__ void receiver_grad(const float *sx, const float *sy, 
         const float lv = __ldg(lut + L), rv = __ldg(lut + R);
         const float dd = (r - (float)L) * k.step;
         const float blend = fmaf(dd, rv - lv, lv);
-        // d log10(w)/d kappa, per unit curvature
-        const float dlog = (rv - lv) / (k.step * blend) * kInvLn10;
-        const float dk = dlog * inv_ds * sign / dn;  // d kappa / d t = inv_ds * d/|d| (sign per term)
-        // project through (I - t2 t2^T) r2
+        const float dlog = (rv - lv) / (k.step * blend) * kInvLn10;  // d log10 w / d kappa
+        const float dk = dlog * inv_ds * sign / dn;                  // d kappa / d t = inv_ds d/|d|
         const float dt = d[0] * t2[0] + d[1] * t2[1] + d[2] * t2[2];
         for (int q = 0; q < 3; ++q) g[q] += dk * (d[q] - dt * t2[q]) * r2;
     }
 }
-
-struct ModeArgs {
-    // export
-    float *exp_pos;      // [chains][steps][N+1][3]
-    double *exp_w;       // [chains][steps] log10 weights (absorption included, normaliser not)
-    float x0[3];
-    double log10_abs;
-    // adjoint
-    const float *lut;    // float table
-    const float *dmu;    // d table / d mu_s
-    const float *deps;   // d table / d eps
-    float ref_log10;     // log10 of the forward sum of path weights (normaliser excluded)
-    double *grad;        // [chains][6]: d/dmu_s, d/deps, d/dx, d/dy, d/dz (log10 units), sum of weights
-};
 
 // Stage a table of `bins` float2 entries into shared memory (float4 vector loads).
 __device__ __forceinline__ void stage_table(float4 *smem4, const float2 *__restrict__ tab_g, int bins)
@@ -239,27 +252,46 @@ __device__ __forceinline__ void stage_table(float4 *smem4, const float2 *__restr
     if ((bins & 1) && threadIdx.x == 0) reinterpret_cast<float2 *>(smem4)[bins - 1] = tab_g[bins - 1];
 }
 
-// One Markov chain run by the G lanes of one group, on its own shared-memory segment
-// planes sx/sy/sz: initial state from init_seg, burn_in + steps proposals, a full
+// Shared-memory planes of one warp: tangents x/y/z and lengths, SPL*32 floats each.
+template <int SPL>
+constexpr int kPlaneFloats = SPL * 32;
+template <int SPL>
+constexpr int kWarpStateFloats = 4 * SPL * 32;
+
+// One Markov chain run by the G lanes of one group on its own planes st (tangents x, y, z,
+// lengths): initial state from init_seg (segment vectors), burn_in + steps proposals, a full
 // recompute of every weighted path, and the chain's running log-sum-exp. Writes out[chain]
 // (when out is set and the chain is real) and returns the chain's log10 sum.
-template <int G, int SPL, bool EXACT, int MODE>
+template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MODE>
 __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConsts &kc,
-                                             const float *__restrict__ init_seg, const float2 *s_tab, float *sx,
-                                             float *sy, float *sz, uint32_t gbase, uint32_t j, uint32_t chain,
-                                             bool real_chain, ChainOut *__restrict__ out, const ModeArgs &ma)
+                                             const float *__restrict__ init_seg, const float2 *s_tab, float *st,
+                                             uint32_t gbase, uint32_t j, uint32_t chain, bool real_chain,
+                                             ChainOut *__restrict__ out, const ModeArgs &ma)
 {
     const uint32_t N = c.n_segments;
     using Lay = Layout<G, SPL>;
+    float *sx = st, *sy = st + kPlaneFloats<SPL>, *sz = st + 2 * kPlaneFloats<SPL>, *sl = st + 3 * kPlaneFloats<SPL>;
 
 #pragma unroll
     for (int m = 0; m < SPL; ++m) {
         const uint32_t s = j * SPL + m;
         const uint32_t a = Lay::addr(gbase, j, m);
-        const bool in = s < N;
-        sx[a] = in ? init_seg[3 * s] : 0.f;
-        sy[a] = in ? init_seg[3 * s + 1] : 0.f;
-        sz[a] = in ? init_seg[3 * s + 2] : 0.f;
+        float x = 0.f, y = 0.f, z = 0.f, len = 1.f;
+        if (s < N) {
+            x = init_seg[3 * s];
+            y = init_seg[3 * s + 1];
+            z = init_seg[3 * s + 2];
+            const float ss = fmaf(x, x, fmaf(y, y, z * z));
+            const float r = rsqrtf(ss);
+            len = ss * r;
+            x *= r; y *= r; z *= r;
+            const float h = fmaf(-0.5f, fmaf(x, x, fmaf(y, y, z * z)), 1.5f);   // one Newton step to |t| = 1
+            x *= h; y *= h; z *= h;
+        }
+        sx[a] = x;
+        sy[a] = y;
+        sz[a] = z;
+        sl[a] = len;
     }
     __syncwarp();
 
@@ -270,15 +302,19 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
     uint32_t valid = 0, failed = 0, clamped = 0;
     float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 
-    auto seg_smem = [&](int m, float &x, float &y, float &z) {
+    auto tan_smem = [&](int m, float &x, float &y, float &z) {
         const uint32_t a = Lay::addr(gbase, j, m);
         x = sx[a];
         y = sy[a];
         z = sz[a];
-        if (c.has_eval_shift && j * SPL + m == N - 2) {
-            x += c.eval_shift[0];
-            y += c.eval_shift[1];
-            z += c.eval_shift[2];
+        if (SHIFT && j * SPL + m == N - 2) {
+            // weights evaluated with the receiver moved: v_{N-2} = l t + shift, renormalised
+            const float l = sl[a];
+            x = fmaf(l, x, c.eval_shift[0]);
+            y = fmaf(l, y, c.eval_shift[1]);
+            z = fmaf(l, z, c.eval_shift[2]);
+            const float r = rsqrtf(fmaf(x, x, fmaf(y, y, z * z)));
+            x *= r; y *= r; z *= r;
         }
     };
     auto no_bins = [](uint32_t, int32_t) {};
@@ -294,7 +330,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
             const float sn = __shfl_sync(FULL, psn, jj, G);
             const float cs = __shfl_sync(FULL, pcs, jj, G);
             const uint32_t right = left + k;
-            // chord x_right - x_left = sum of the k segment vectors left .. right-1
+            // chord x_right - x_left = sum of l_s t_s over the k segments left .. right-1
             constexpr int R = (kMaxSubChain + G - 1) / G;
             float vx[R], vy[R], vz[R];
             uint32_t va[R];
@@ -307,9 +343,10 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                     vx[r] = sx[va[r]];
                     vy[r] = sy[va[r]];
                     vz[r] = sz[va[r]];
-                    cx += vx[r];
-                    cy += vy[r];
-                    cz += vz[r];
+                    const float l = sl[va[r]];
+                    cx = fmaf(l, vx[r], cx);
+                    cy = fmaf(l, vy[r], cy);
+                    cz = fmaf(l, vz[r], cz);
                 }
             }
             group_sum3<G>(cx, cy, cz);
@@ -325,9 +362,13 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                 const uint32_t s = left + j + r * G;
                 if (s < right) {
                     const float x = vx[r], y = vy[r], z = vz[r];
-                    sx[va[r]] = fmaf(r00, x, fmaf(r01, y, r02 * z));
-                    sy[va[r]] = fmaf(r10, x, fmaf(r11, y, r12 * z));
-                    sz[va[r]] = fmaf(r20, x, fmaf(r21, y, r22 * z));
+                    float nx = fmaf(r00, x, fmaf(r01, y, r02 * z));
+                    float ny = fmaf(r10, x, fmaf(r11, y, r12 * z));
+                    float nz = fmaf(r20, x, fmaf(r21, y, r22 * z));
+                    const float h = fmaf(-0.5f, fmaf(nx, nx, fmaf(ny, ny, nz * nz)), 1.5f);
+                    sx[va[r]] = nx * h;
+                    sy[va[r]] = ny * h;
+                    sz[va[r]] = nz * h;
                 }
             }
             __syncwarp();
@@ -335,7 +376,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
             if (step < c.burn_in) continue;
             const uint32_t wstep = step - c.burn_in;
             const bool active = wstep < steps_c;
-            float hi, lo;
+            double w;
             if (MODE == kModeAdjoint) {
                 // log10 weight and d/d(mu_s), d/d(eps) of this lane's segments (exact blend)
                 float s = 0.f, cc = 0.f, gmu = 0.f, geps = 0.f;
@@ -358,10 +399,8 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                 };
 #pragma unroll
                 for (int m = 0; m < SPL; ++m) {
-                    float x, y, z;
-                    seg_smem(m, x, y, z);
-                    const float rs = rsqrtf(fmaf(x, x, fmaf(y, y, z * z)));
-                    const float tx = x * rs, ty = y * rs, tz = z * rs;
+                    float tx, ty, tz;
+                    tan_smem(m, tx, ty, tz);
                     if (m == 0) { t0x = tx; t0y = ty; t0z = tz; }
                     else if (b0 + m <= N - 1) {
                         const float dx = tx - px, dy = ty - py, dz = tz - pz;
@@ -376,16 +415,22 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                     const float dx = nx - px, dy = ny - py, dz = nz - pz;
                     seg_term(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
                 }
-                hi = s;
-                lo = -cc;
+                float hi = s, lo = -cc;
                 group_sum_pair<G>(hi, lo);
+                w = (double)hi + (double)lo;
                 float g3[3] = {0.f, 0.f, 0.f};
-                if (j == 0)
-                    receiver_grad(sx, sy, sz, Lay::addr(gbase, (N - 3) / SPL, (N - 3) % SPL),
-                                  Lay::addr(gbase, (N - 2) / SPL, (N - 2) % SPL),
-                                  Lay::addr(gbase, (N - 1) / SPL, (N - 1) % SPL), ma.lut, kc, c.inv_ds, g3);
-                if (active && !(isnan(hi) || isnan(lo))) {
-                    const float wt = exp2f(((hi - ma.ref_log10) + lo) * kLog2_10);
+                if (j == 0) {
+                    float t3[3], t2[3], t1[3];
+                    const uint32_t a3 = Lay::addr(gbase, (N - 3) / SPL, (N - 3) % SPL);
+                    const uint32_t a2 = Lay::addr(gbase, (N - 2) / SPL, (N - 2) % SPL);
+                    const uint32_t a1 = Lay::addr(gbase, (N - 1) / SPL, (N - 1) % SPL);
+                    t3[0] = sx[a3]; t3[1] = sy[a3]; t3[2] = sz[a3];
+                    t2[0] = sx[a2]; t2[1] = sy[a2]; t2[2] = sz[a2];
+                    t1[0] = sx[a1]; t1[1] = sy[a1]; t1[2] = sz[a1];
+                    receiver_grad(t3, t2, t1, sl[a2], ma.lut, kc, c.inv_ds, g3);
+                }
+                if (active && !isnan(w)) {
+                    const float wt = exp2f((float)(w - (double)ma.ref_log10) * kLog2_10);
                     acc[0] += wt * gmu * kInvLn10;
                     acc[1] += wt * geps * kInvLn10;
                     acc[2] += wt * g3[0];
@@ -394,30 +439,31 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                     if (j == 0) acc[5] += wt;
                 }
             } else {
-                path_log10<G, SPL, EXACT>(j, N, s_tab, kc, seg_smem, no_bins, hi, lo, clamped);
+                w = path_log10<G, SPL, EXACT, CLAMP, uint32_t>(j, N, s_tab, kc, tan_smem, no_bins, clamped);
             }
             if (MODE == kModeExport) {
-                // positions x_0 + prefix sums of the segment vectors, in double; every lane
-                // takes part in the scan, only active chains write
+                // positions x_0 + prefix sums of l_s t_s, in double; every lane takes part in
+                // the scan, only active chains write
                 double px = 0.0, py = 0.0, pz = 0.0;
                 double lx[SPL], ly[SPL], lz[SPL];
 #pragma unroll
                 for (int m = 0; m < SPL; ++m) {
                     const uint32_t a = Lay::addr(gbase, j, m);
                     const bool in = j * SPL + m < N;
-                    px += in ? (double)sx[a] : 0.0;
-                    py += in ? (double)sy[a] : 0.0;
-                    pz += in ? (double)sz[a] : 0.0;
+                    const double l = in ? (double)sl[a] : 0.0;
+                    px += l * (double)sx[a];
+                    py += l * (double)sy[a];
+                    pz += l * (double)sz[a];
                     lx[m] = px; ly[m] = py; lz[m] = pz;
                 }
-                double ex = px, ey = py, ez = pz;   // inclusive scan of lane totals
+                double ex = px, ey = py, ez = pz;  // inclusive scan of lane totals
 #pragma unroll
                 for (int o = 1; o < G; o <<= 1) {
                     const double ux = __shfl_up_sync(FULL, ex, o, G), uy = __shfl_up_sync(FULL, ey, o, G),
                                  uz = __shfl_up_sync(FULL, ez, o, G);
                     if ((int)j >= o) { ex += ux; ey += uy; ez += uz; }
                 }
-                ex -= px; ey -= py; ez -= pz;       // exclusive
+                ex -= px; ey -= py; ez -= pz;  // exclusive
                 if (active) {
                     const size_t pidx = (size_t)chain * c.steps + wstep;
                     float *dst = ma.exp_pos + pidx * 3 * (size_t)(N + 1);
@@ -431,14 +477,17 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                             dst[3 * (s + 1) + 2] = (float)((double)ma.x0[2] + ez + lz[m]);
                         }
                     }
-                    if (j == 0)
-                        ma.exp_w[pidx] = (isnan(hi) || isnan(lo)) ? NAN : (double)hi + (double)lo + (N - 1) * ma.log10_abs;
+                    if (j == 0) ma.exp_w[pidx] = isnan(w) ? NAN : w + (N - 1) * ma.log10_abs;
                 }
             }
             if (!active) continue;
-            if (isnan(hi) || isnan(lo)) {
+            if (isnan(w)) {
                 ++failed;
-            } else if (valid == 0) {
+                continue;
+            }
+            const float hi = (float)w;
+            const float lo = (float)(w - (double)hi);
+            if (valid == 0) {
                 lse_m = hi;
                 lse_s = exp2f(lo * kLog2_10);
                 lse_c = 0.f;
@@ -460,15 +509,10 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
             }
         }
     }
-    clamped = group_sum_u<G>(clamped);
+    clamped = group_sum<G>(clamped);
     if (MODE == kModeAdjoint) {
 #pragma unroll
-        for (int i = 0; i < 6; ++i) {
-            float v = acc[i];
-#pragma unroll
-            for (int o = 1; o < G; o <<= 1) v += __shfl_xor_sync(FULL, v, o);
-            acc[i] = v;
-        }
+        for (int i = 0; i < 6; ++i) acc[i] = group_sum<G>(acc[i]);
         if (j == 0 && real_chain)
             for (int i = 0; i < 6; ++i) ma.grad[(size_t)chain * 6 + i] = (double)acc[i];
     }
@@ -487,7 +531,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
     return real_chain ? chain_log10 : -INFINITY;
 }
 
-template <int G, int SPL, bool EXACT, int MAXT, int MODE>
+template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MAXT, int MODE>
 __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompConsts kc,
                                                              const float *__restrict__ init_seg,
                                                              const float2 *__restrict__ tab_g,
@@ -500,7 +544,7 @@ __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompCo
     const int tab_f4 = (bins + 1) / 2;  // float2 entries, padded to float4
     float *s_state = reinterpret_cast<float *>(smem4 + tab_f4);
     const int warps = blockDim.x >> 5;
-    double *s_res = reinterpret_cast<double *>(s_state + warps * 3 * SPL * 32);
+    double *s_res = reinterpret_cast<double *>(s_state + warps * kWarpStateFloats<SPL>);
     stage_table(smem4, tab_g, bins);
     __syncthreads();
 
@@ -508,9 +552,8 @@ __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompCo
     const uint32_t q = lane / G, j = lane % G;
     constexpr int CPW = 32 / G;
     const uint32_t chain = (blockIdx.x * warps + warp) * CPW + q;
-    float *sx = s_state + warp * 3 * SPL * 32;
-    const double cl = chain_body<G, SPL, EXACT, MODE>(c, kc, init_seg, s_tab, sx, sx + SPL * 32, sx + 2 * SPL * 32,
-                                                      q * G, j, chain, chain < c.n_chains, out, ma);
+    const double cl = chain_body<G, SPL, EXACT, CLAMP, SHIFT, MODE>(
+          c, kc, init_seg, s_tab, s_state + warp * kWarpStateFloats<SPL>, q * G, j, chain, chain < c.n_chains, out, ma);
     if (j == 0) s_res[warp * CPW + q] = cl;
     __syncthreads();
     // Per-CTA log-sum-exp of the chains, rescaled by the block maximum (FP64).
@@ -527,7 +570,60 @@ __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompCo
     }
 }
 
-// Compensated weigher of given paths: one group of 32 lanes per path.
+// ---------------------------------------------------------------------------------------
+// Batched persistent form: many experiments (uneven N, S, mu_s, eps) per launch. Work items
+// are (experiment, first chain of a CTA's worth of chains), sorted by cost; persistent CTAs
+// pull items from a device counter (atomicAdd), stage that experiment's table in shared
+// memory (or read it through L1), and run their chains with chain_body.
+// ---------------------------------------------------------------------------------------
+struct BatchExp {
+    ChainSpec spec;
+    CompConsts kc;
+    const float2 *tab;
+    const float *init_seg;
+    double log10_abs;
+    uint32_t out_offset;
+    uint32_t pad;
+};
+
+template <int G, int SPL, bool EXACT, bool LUT_SMEM, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1) batch_kernel(const BatchExp *__restrict__ exps,
+                                                        const uint2 *__restrict__ items, uint32_t n_items,
+                                                        uint32_t *__restrict__ counter, ChainOut *__restrict__ out,
+                                                        int bins)
+{
+    extern __shared__ float4 smem4[];
+    __shared__ uint32_t s_item;
+    const int tab_f4 = LUT_SMEM ? (bins + 1) / 2 : 0;
+    float *s_state = reinterpret_cast<float *>(smem4 + tab_f4);
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t q = lane / G, j = lane % G;
+    constexpr int CPW = 32 / G;
+    float *st = s_state + warp * kWarpStateFloats<SPL>;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1u);
+        __syncthreads();
+        const uint32_t item = s_item;
+        if (item >= n_items) break;
+        const uint2 it = items[item];
+        const BatchExp &e = exps[it.x];
+        const float2 *tab = e.tab;
+        if (LUT_SMEM) {
+            stage_table(smem4, e.tab, bins);
+            tab = reinterpret_cast<const float2 *>(smem4);
+        }
+        __syncthreads();
+        ModeArgs ma{};
+        ma.log10_abs = e.log10_abs;
+        const uint32_t chain = it.y + warp * CPW + q;
+        chain_body<G, SPL, EXACT, true, false, kModeForward>(e.spec, e.kc, e.init_seg, tab, st, q * G, j, chain,
+                                                              chain < e.spec.n_chains, out + e.out_offset, ma);
+        __syncthreads();
+    }
+}
+
+// Compensated weigher of given paths: one group of 32 lanes per path; tangents from the
+// positions, normalised here.
 template <int SPL, bool EXACT>
 __global__ void __launch_bounds__(256) weigh_comp_kernel(const float *__restrict__ pos, uint64_t n_paths, uint32_t N,
                                                           CompConsts kc, const float2 *__restrict__ tab,
@@ -538,12 +634,14 @@ __global__ void __launch_bounds__(256) weigh_comp_kernel(const float *__restrict
     const uint32_t j = threadIdx.x & 31;
     if (p >= n_paths) return;  // whole warps exit together
     const float *pp = pos + p * 3 * (uint64_t)(N + 1);
-    auto seg = [&](int m, float &x, float &y, float &z) {
+    auto tan = [&](int m, float &x, float &y, float &z) {
         const uint32_t s = j * SPL + m;
         if (s < N) {
             x = pp[3 * s + 3] - pp[3 * s];
             y = pp[3 * s + 4] - pp[3 * s + 1];
             z = pp[3 * s + 5] - pp[3 * s + 2];
+            const float r = rsqrtf(fmaf(x, x, fmaf(y, y, z * z)));
+            x *= r; y *= r; z *= r;
         } else {
             x = y = z = 0.f;
         }
@@ -553,45 +651,46 @@ __global__ void __launch_bounds__(256) weigh_comp_kernel(const float *__restrict
         if (brow) brow[i] = b;
     };
     uint32_t clamped = 0;
-    float hi, lo;
-    path_log10<32, SPL, EXACT>(j, N, tab, kc, seg, sink, hi, lo, clamped);
+    const double w = path_log10<32, SPL, EXACT, true, unsigned long long>(j, N, tab, kc, tan, sink, clamped);
     if (j == 0) {
-        const bool ok = !(isnan(hi) || isnan(lo));
-        log10w[p] = ok ? (double)hi + (double)lo + (double)(N - 1) * log10_absorption : 0.0;
+        const bool ok = !isnan(w);
+        log10w[p] = ok ? w + (double)(N - 1) * log10_absorption : 0.0;
         if (valid) valid[p] = ok ? 1 : 0;
     }
 }
 
-template <int G, int SPL, bool EXACT, int MODE>
+// ------------------------------------------------------------------------------ launchers
+template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MODE>
 cudaError_t launch_t(const ChainSpec &c, const CompConsts &kc, int warps, const float *init_seg, const float2 *tab,
                      ChainOut *out, double2 *partials, const ModeArgs &ma, size_t smem, uint32_t blocks, cudaStream_t st)
 {
     constexpr int MAXT = (SPL >= 16) ? 512 : 1024;
     if (warps * 32 > MAXT) return cudaErrorInvalidConfiguration;
-    auto kern = comp_chain_kernel<G, SPL, EXACT, MAXT, MODE>;
+    auto kern = comp_chain_kernel<G, SPL, EXACT, CLAMP, SHIFT, MAXT, MODE>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     kern<<<blocks, warps * 32, smem, st>>>(c, kc, init_seg, tab, out, partials, ma);
     return cudaGetLastError();
 }
 
+// Instantiated variants: forward (fixed/exact x clamp/no clamp, plus an exact+clamp+shift
+// variant for receiver-shifted evaluation), export (fixed/exact with clamp), adjoint (exact).
 template <int G, int SPL>
-cudaError_t launch_g(int mode, const ChainSpec &c, const CompConsts &kc, const CompTuning &t, const float *init_seg,
-                     const float2 *tab, ChainOut *out, double2 *partials, const ModeArgs &ma, size_t smem,
-                     uint32_t blocks, cudaStream_t st)
+cudaError_t launch_g(int mode, bool exact, bool clamp, bool shift, const ChainSpec &c, const CompConsts &kc,
+                     const CompTuning &t, const float *init_seg, const float2 *tab, ChainOut *out, double2 *partials,
+                     const ModeArgs &ma, size_t smem, uint32_t blocks, cudaStream_t st)
 {
     const int w = t.warps_per_block;
-    if (mode == kModeAdjoint)
-        return launch_t<G, SPL, true, kModeAdjoint>(c, kc, w, init_seg, tab, out, partials, ma, smem, blocks, st);
-    if (mode == kModeExport) {
-        if (t.exact_blend) return launch_t<G, SPL, true, kModeExport>(c, kc, w, init_seg, tab, out, partials, ma, smem, blocks, st);
-        return launch_t<G, SPL, false, kModeExport>(c, kc, w, init_seg, tab, out, partials, ma, smem, blocks, st);
-    }
-    if (t.exact_blend) return launch_t<G, SPL, true, kModeForward>(c, kc, w, init_seg, tab, out, partials, ma, smem, blocks, st);
-    return launch_t<G, SPL, false, kModeForward>(c, kc, w, init_seg, tab, out, partials, ma, smem, blocks, st);
+#define TWISTY_L(E, CL, SH, MO) launch_t<G, SPL, E, CL, SH, MO>(c, kc, w, init_seg, tab, out, partials, ma, smem, blocks, st)
+    if (mode == kModeAdjoint) return TWISTY_L(true, true, false, kModeAdjoint);
+    if (mode == kModeExport) return exact ? TWISTY_L(true, true, false, kModeExport) : TWISTY_L(false, true, false, kModeExport);
+    if (shift) return TWISTY_L(true, true, true, kModeForward);
+    if (exact) return clamp ? TWISTY_L(true, true, false, kModeForward) : TWISTY_L(true, false, false, kModeForward);
+    return clamp ? TWISTY_L(false, true, false, kModeForward) : TWISTY_L(false, false, false, kModeForward);
+#undef TWISTY_L
 }
 
-CompConsts make_consts(float inv_ds, const LutMetaF &m)
+CompConsts make_consts(float inv_ds, const LutMetaF &m, uint32_t n_segments, const LogFixed &lf)
 {
     CompConsts k;
     k.kscale = inv_ds / m.step;
@@ -600,7 +699,90 @@ CompConsts make_consts(float inv_ds, const LutMetaF &m)
     k.rsnap = 1e-3f / m.step;
     k.step = m.step;
     k.bins = m.bins;
+    k.lw_offset = (double)(n_segments - 1) * lf.c0;
+    k.inv_scale = lf.inv_scale;
     return k;
+}
+
+// A table whose range covers every curvature unit tangents can produce, |t_{i+1}-t_i| <= 2
+// (with margin for rounding), needs no clamping.
+bool table_needs_clamp(const CompConsts &k) { return !(k.roff == 0.0f && k.rmax >= 2.0001f * k.kscale); }
+
+cudaError_t launch_mode(int mode, const ChainSpec &c, const CompTuning &t, const float *init_seg, const float2 *fixtab,
+                        const float2 *lintab, LutMetaF m, ChainOut *out, double2 *block_partials, const ModeArgs &ma,
+                        const LogFixed &lf, cudaStream_t st)
+{
+    if (!comp_tuning_supported(t, c.n_segments, c.k_eff)) return cudaErrorInvalidValue;
+    if (c.has_eval_shift && mode != kModeForward) return cudaErrorInvalidValue;
+    if (c.n_chains == 0) return cudaSuccess;
+    const bool exact = t.exact_blend || mode == kModeAdjoint || lf.inv_scale == 0.0;
+    const CompConsts kc = make_consts(c.inv_ds, m, c.n_segments, lf);
+    const size_t smem = comp_smem_bytes(t, (uint32_t)m.bins);
+    const uint32_t blocks = comp_blocks(c, t);
+    const float2 *tab = exact ? lintab : fixtab;
+    const bool clamp = table_needs_clamp(kc);
+    const bool shift = c.has_eval_shift != 0;
+#define TWISTY_CASE(GG, SS)                                                                                             \
+    if (t.group == GG && t.spl == SS)                                                                                   \
+        return launch_g<GG, SS>(mode, exact || shift, clamp, shift, c, kc, t, init_seg, (exact || shift) ? lintab : tab, \
+                                out, block_partials, ma, smem, blocks, st);
+    TWISTY_CASE(8, 2)
+    TWISTY_CASE(8, 4)
+    TWISTY_CASE(8, 8)
+    TWISTY_CASE(8, 16)
+    TWISTY_CASE(16, 4)
+    TWISTY_CASE(16, 8)
+    TWISTY_CASE(16, 16)
+    TWISTY_CASE(32, 4)
+    TWISTY_CASE(32, 8)
+    TWISTY_CASE(32, 16)
+    TWISTY_CASE(32, 32)
+#undef TWISTY_CASE
+    return cudaErrorInvalidValue;
+}
+
+__global__ void __launch_bounds__(1024) grad_reduce_kernel(const double *__restrict__ g, uint32_t n, double *__restrict__ out)
+{
+    __shared__ double red[6][32];
+    double a[6] = {0, 0, 0, 0, 0, 0};
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+        for (int k = 0; k < 6; ++k) a[k] += g[(size_t)i * 6 + k];
+    for (int k = 0; k < 6; ++k)
+        for (int o = 16; o > 0; o >>= 1) a[k] += __shfl_xor_sync(FULL, a[k], o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0)
+        for (int k = 0; k < 6; ++k) red[k][w] = a[k];
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double v = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) v += red[threadIdx.x][i];
+        out[threadIdx.x] = v;
+    }
+}
+
+template <int G, int SPL, bool EXACT, bool LS>
+cudaError_t batch_t(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items, uint32_t *counter,
+                    ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st)
+{
+    constexpr int MAXT = (SPL >= 16) ? 512 : 1024;
+    if (s.warps * 32 > MAXT) return cudaErrorInvalidConfiguration;
+    auto kern = batch_kernel<G, SPL, EXACT, LS, MAXT>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, s.warps * 32, smem, st>>>(exps, items, n_items, counter, out, bins);
+    return cudaGetLastError();
+}
+
+template <int G, int SPL>
+cudaError_t batch_g(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items, uint32_t *counter,
+                    ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st)
+{
+    if (s.exact) {
+        if (s.lut_smem) return batch_t<G, SPL, true, true>(s, exps, items, n_items, counter, out, bins, grid, smem, st);
+        return batch_t<G, SPL, true, false>(s, exps, items, n_items, counter, out, bins, grid, smem, st);
+    }
+    if (s.lut_smem) return batch_t<G, SPL, false, true>(s, exps, items, n_items, counter, out, bins, grid, smem, st);
+    return batch_t<G, SPL, false, false>(s, exps, items, n_items, counter, out, bins, grid, smem, st);
 }
 
 }  // namespace
@@ -637,7 +819,7 @@ uint32_t comp_default_chains(uint32_t n, int sm_count)
 size_t comp_smem_bytes(const CompTuning &t, uint32_t bins)
 {
     const size_t tab = (size_t)((bins + 1) / 2) * sizeof(float4);
-    const size_t state = (size_t)t.warps_per_block * 3 * t.spl * 32 * sizeof(float);
+    const size_t state = (size_t)t.warps_per_block * 4 * t.spl * 32 * sizeof(float);
     const size_t res = (size_t)t.warps_per_block * (32 / t.group) * sizeof(double);
     return tab + state + res;
 }
@@ -648,66 +830,18 @@ uint32_t comp_blocks(const ChainSpec &c, const CompTuning &t)
     return (c.n_chains + per_block - 1) / per_block;
 }
 
-namespace {
-cudaError_t launch_mode(int mode, const ChainSpec &c, const CompTuning &t, const float *init_seg, const float2 *logtab,
-                        const float2 *lintab, LutMetaF m, ChainOut *out, double2 *block_partials, const ModeArgs &ma,
-                        cudaStream_t st)
-{
-    if (!comp_tuning_supported(t, c.n_segments, c.k_eff)) return cudaErrorInvalidValue;
-    if (c.n_chains == 0) return cudaSuccess;
-    const CompConsts kc = make_consts(c.inv_ds, m);
-    const size_t smem = comp_smem_bytes(t, (uint32_t)m.bins);
-    const uint32_t blocks = comp_blocks(c, t);
-    const float2 *tab = (t.exact_blend || mode == kModeAdjoint) ? lintab : logtab;
-#define TWISTY_CASE(GG, SS) \
-    if (t.group == GG && t.spl == SS) return launch_g<GG, SS>(mode, c, kc, t, init_seg, tab, out, block_partials, ma, smem, blocks, st);
-    TWISTY_CASE(8, 2)
-    TWISTY_CASE(8, 4)
-    TWISTY_CASE(8, 8)
-    TWISTY_CASE(8, 16)
-    TWISTY_CASE(16, 4)
-    TWISTY_CASE(16, 8)
-    TWISTY_CASE(16, 16)
-    TWISTY_CASE(32, 4)
-    TWISTY_CASE(32, 8)
-    TWISTY_CASE(32, 16)
-    TWISTY_CASE(32, 32)
-#undef TWISTY_CASE
-    return cudaErrorInvalidValue;
-}
-
-__global__ void __launch_bounds__(1024) grad_reduce_kernel(const double *__restrict__ g, uint32_t n, double *__restrict__ out)
-{
-    __shared__ double red[6][32];
-    double a[6] = {0, 0, 0, 0, 0, 0};
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
-        for (int k = 0; k < 6; ++k) a[k] += g[(size_t)i * 6 + k];
-    for (int k = 0; k < 6; ++k)
-        for (int o = 16; o > 0; o >>= 1) a[k] += __shfl_xor_sync(FULL, a[k], o);
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0)
-        for (int k = 0; k < 6; ++k) red[k][w] = a[k];
-    __syncthreads();
-    if (threadIdx.x < 6) {
-        double v = 0.0;
-        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) v += red[threadIdx.x][i];
-        out[threadIdx.x] = v;
-    }
-}
-}  // namespace
-
-cudaError_t launch_comp_chains(const ChainSpec &c, const CompTuning &t, const float *init_seg, const float2 *logtab,
+cudaError_t launch_comp_chains(const ChainSpec &c, const CompTuning &t, const float *init_seg, const float2 *fixtab,
                                const float2 *lintab, LutMetaF m, ChainOut *out, double2 *block_partials,
-                               cudaStream_t st)
+                               cudaStream_t st, LogFixed lf)
 {
     ModeArgs ma{};
     ma.log10_abs = log10(c.absorption_factor);
-    return launch_mode(kModeForward, c, t, init_seg, logtab, lintab, m, out, block_partials, ma, st);
+    return launch_mode(kModeForward, c, t, init_seg, fixtab, lintab, m, out, block_partials, ma, lf, st);
 }
 
-cudaError_t launch_comp_export(const ChainSpec &c, const CompTuning &t, const float *init_seg, const float2 *logtab,
+cudaError_t launch_comp_export(const ChainSpec &c, const CompTuning &t, const float *init_seg, const float2 *fixtab,
                                const float2 *lintab, LutMetaF m, const float x0[3], float *exp_pos, double *exp_w,
-                               ChainOut *out, cudaStream_t st)
+                               ChainOut *out, cudaStream_t st, LogFixed lf)
 {
     ModeArgs ma{};
     ma.log10_abs = log10(c.absorption_factor);
@@ -716,7 +850,7 @@ cudaError_t launch_comp_export(const ChainSpec &c, const CompTuning &t, const fl
     ma.x0[0] = x0[0];
     ma.x0[1] = x0[1];
     ma.x0[2] = x0[2];
-    return launch_mode(kModeExport, c, t, init_seg, logtab, lintab, m, out, nullptr, ma, st);
+    return launch_mode(kModeExport, c, t, init_seg, fixtab, lintab, m, out, nullptr, ma, lf, st);
 }
 
 cudaError_t launch_comp_adjoint(const ChainSpec &c, const CompTuning &t, const float *init_seg, const float2 *lintab,
@@ -730,23 +864,26 @@ cudaError_t launch_comp_adjoint(const ChainSpec &c, const CompTuning &t, const f
     ma.deps = deps;
     ma.ref_log10 = ref_log10;
     ma.grad = grad_chains;
-    cudaError_t e = launch_mode(kModeAdjoint, c, t, init_seg, lintab, lintab, m, nullptr, nullptr, ma, st);
+    cudaError_t e = launch_mode(kModeAdjoint, c, t, init_seg, lintab, lintab, m, nullptr, nullptr, ma,
+                                LogFixed{0.0, 0.0}, st);
     if (e != cudaSuccess) return e;
     grad_reduce_kernel<<<1, 1024, 0, st>>>(grad_chains, c.n_chains, grad_out);
     return cudaGetLastError();
 }
 
 cudaError_t launch_weigh_comp(const float *pos, uint64_t n_paths, uint32_t n_segments, float inv_ds,
-                              const float2 *logtab, const float2 *lintab, int exact_blend, LutMetaF m,
-                              double log10_absorption, double *log10w, uint8_t *valid, int32_t *bins, cudaStream_t st)
+                              const float2 *fixtab, const float2 *lintab, int exact_blend, LutMetaF m,
+                              double log10_absorption, double *log10w, uint8_t *valid, int32_t *bins, cudaStream_t st,
+                              LogFixed lf)
 {
     if (n_paths == 0) return cudaSuccess;
-    const CompConsts kc = make_consts(inv_ds, m);
+    const CompConsts kc = make_consts(inv_ds, m, n_segments, lf);
     const uint64_t blocks = (n_paths * 32 + 255) / 256;
-    const float2 *tab = exact_blend ? lintab : logtab;
+    const bool exact = exact_blend || lf.inv_scale == 0.0;
+    const float2 *tab = exact ? lintab : fixtab;
 #define TWISTY_W(SS)                                                                                           \
     if (n_segments <= 32u * SS) {                                                                              \
-        if (exact_blend)                                                                                       \
+        if (exact)                                                                                             \
             weigh_comp_kernel<SS, true><<<(unsigned)blocks, 256, 0, st>>>(pos, n_paths, n_segments, kc, tab,  \
                                                                           log10_absorption, log10w, valid, bins); \
         else                                                                                                   \
@@ -761,6 +898,59 @@ cudaError_t launch_weigh_comp(const float *pos, uint64_t n_paths, uint32_t n_seg
     TWISTY_W(16)
     TWISTY_W(32)
 #undef TWISTY_W
+    return cudaErrorInvalidValue;
+}
+
+// ------------------------------------------------------------------------- batched form
+size_t batch_exp_bytes() { return sizeof(BatchExp); }
+
+void batch_pack_experiments(const BatchExpHost *in, uint32_t n, void *dst)
+{
+    BatchExp *d = static_cast<BatchExp *>(dst);
+    for (uint32_t i = 0; i < n; ++i) {
+        BatchExp e{};
+        e.spec = in[i].spec;
+        e.kc = make_consts(in[i].spec.inv_ds, in[i].meta, in[i].spec.n_segments, in[i].lf);
+        e.tab = in[i].tab;
+        e.init_seg = in[i].init_seg;
+        e.log10_abs = log10(in[i].spec.absorption_factor);
+        e.out_offset = in[i].out_offset;
+        d[i] = e;
+    }
+}
+
+bool batch_shape_supported(const BatchShape &s, uint32_t n_max, uint32_t k_eff)
+{
+    CompTuning t{s.group, s.spl, s.warps, s.exact};
+    return comp_tuning_supported(t, n_max, k_eff);
+}
+
+size_t batch_smem_bytes(const BatchShape &s, uint32_t bins)
+{
+    return (s.lut_smem ? (size_t)((bins + 1) / 2) * sizeof(float4) : 0) + (size_t)s.warps * 4 * s.spl * 32 * sizeof(float);
+}
+
+int batch_chains_per_block(const BatchShape &s) { return s.warps * (32 / s.group); }
+
+cudaError_t launch_batch(const BatchShape &s, const void *d_exps, const uint2 *d_items, uint32_t n_items,
+                         uint32_t *d_counter, ChainOut *out, int bins, int grid, cudaStream_t st)
+{
+    const BatchExp *exps = static_cast<const BatchExp *>(d_exps);
+    const size_t smem = batch_smem_bytes(s, (uint32_t)bins);
+#define TWISTY_B(GG, SS) \
+    if (s.group == GG && s.spl == SS) return batch_g<GG, SS>(s, exps, d_items, n_items, d_counter, out, bins, grid, smem, st);
+    TWISTY_B(8, 2)
+    TWISTY_B(8, 4)
+    TWISTY_B(8, 8)
+    TWISTY_B(8, 16)
+    TWISTY_B(16, 4)
+    TWISTY_B(16, 8)
+    TWISTY_B(16, 16)
+    TWISTY_B(32, 4)
+    TWISTY_B(32, 8)
+    TWISTY_B(32, 16)
+    TWISTY_B(32, 32)
+#undef TWISTY_B
     return cudaErrorInvalidValue;
 }
 

@@ -610,4 +610,56 @@ double norm_k4_log10(float z, float ds)
     return std::log10((double)result);
 }
 
+bool compensated_tables(const float *lut, uint32_t bins, float step, uint32_t spl, std::vector<float> &lin,
+                        std::vector<float> &fix, double &c0, double &inv_scale, double &secant_err)
+{
+    lin.assign(2 * (size_t)bins, 0.0f);
+    fix.assign(2 * (size_t)bins, 0.0f);
+    c0 = 0.0;
+    inv_scale = 0.0;
+    secant_err = 0.0;
+    bool positive = true;
+    std::vector<double> lg(bins);
+    double lo = INFINITY, hi = -INFINITY;
+    const double st = (double)step;
+    for (uint32_t i = 0; i < bins; ++i) {
+        const float a = lut[i], b = lut[i + 1 < bins ? i + 1 : i];
+        lin[2 * i] = a;
+        lin[2 * i + 1] = b - a;
+        if (!(a > 0.0f) || !std::isfinite(a)) {
+            positive = false;
+            continue;
+        }
+        lg[i] = std::log10((double)a);
+        lo = std::min(lo, lg[i]);
+        hi = std::max(hi, lg[i]);
+        if (i + 1 < bins) {
+            const double r = (double)b / (double)a - 1.0;
+            secant_err = std::max(secant_err, (st * r) * (st * r) / (8.0 * 2.302585092994046));
+        }
+    }
+    if (!positive) {
+        secant_err = INFINITY;
+        return false;
+    }
+    // largest s with spl * round(range * 2^s) < 2^32, at most 30
+    const double cap = std::floor(4294967295.0 / (double)(spl ? spl : 1)) - 1.0;
+    const double range = hi - lo;
+    int s = 30;
+    while (s > 0 && range * std::ldexp(1.0, s) > cap) --s;
+    if (secant_err > 1e-7 || s < 22) return false;
+    c0 = lo;
+    inv_scale = std::ldexp(1.0, -s);
+    for (uint32_t i = 0; i < bins; ++i) {
+        double e = std::nearbyint((lg[i] - lo) * std::ldexp(1.0, s));
+        e = std::min(std::max(e, 0.0), cap);
+        const uint32_t u = (uint32_t)e;
+        std::memcpy(&fix[2 * i], &u, 4);
+        double slope = 0.0;
+        if (i + 1 < bins) slope = std::log10(1.0 + st * ((double)lut[i + 1] / (double)lut[i] - 1.0)) / st;
+        fix[2 * i + 1] = (float)slope;
+    }
+    return true;
+}
+
 }  // namespace twisty

@@ -69,9 +69,6 @@ cudaError_t launch_lut_build(const LutBuildSpec &s, double *out64, double *d_mus
 // Non-positive entries replaced by the smallest non-negative one (PathWeightUtils.cpp:
 // 327-344); min/max returned through minmax[2]; float copy written to out32.
 cudaError_t launch_lut_finalize(uint32_t bins, double *lut64, float *out32, double *minmax, cudaStream_t st);
-// Compensated-form table: per bin (log10 L_i, secant slope in log10 per curvature unit).
-cudaError_t launch_lut_logtable(uint32_t bins, const float *lut32, float step, float2 *out,
-                                double *max_err, cudaStream_t st);
 
 // ------------------------------------------------------------- chains (chain_*.cu)
 cudaError_t launch_plain_chains(const ChainSpec &c, const float *init_pos, float *state,
@@ -90,6 +87,17 @@ cudaError_t launch_fp64_chains(const ChainSpec &c, const float *init_pos, double
                                int32_t bins, ChainOut *out, cudaStream_t st);
 
 // Compensated form. init_seg holds the N initial segment vectors (float3, x_{i+1}-x_i).
+//
+// Fixed-point form of the compensated log table: entry i of the float2 table holds
+// round((log10 L_i - c0) * 2^s) as uint32 bits in .x (c0 = the smallest log10 L_i, so every
+// entry is non-negative) and the float secant slope in .y; a path's log10 weight is
+// (N-1) c0 + (sum of the uint32 entries) * 2^-s + (sum of the slope corrections). A lane
+// sums at most `spl` entries in 32 bits, so the table is built with spl * max entry < 2^32.
+// inv_scale = 0 selects the exact (L_i, L_{i+1}-L_i) table instead.
+struct LogFixed {
+    double c0;
+    double inv_scale;
+};
 struct CompTuning {
     int group;               // lanes per chain (4, 8, 16, 32)
     int spl;                 // segments per lane
@@ -101,20 +109,45 @@ bool comp_tuning_supported(const CompTuning &t, uint32_t n_segments, uint32_t k_
 uint32_t comp_default_chains(uint32_t n_segments, int sm_count);
 size_t comp_smem_bytes(const CompTuning &t, uint32_t bins);
 cudaError_t launch_comp_chains(const ChainSpec &c, const CompTuning &t, const float *init_seg,
-                               const float2 *logtab, const float2 *lintab, LutMetaF m,
-                               ChainOut *out, double2 *block_partials, cudaStream_t st);
+                               const float2 *fixtab, const float2 *lintab, LutMetaF m,
+                               ChainOut *out, double2 *block_partials, cudaStream_t st,
+                               LogFixed lf = LogFixed{0.0, 0.0});
 uint32_t comp_blocks(const ChainSpec &c, const CompTuning &t);
 // Replay of chains that also writes every weighted path: positions x_0 + prefix sums of the
 // segment vectors (exp_pos[chain][step][N+1][3]) and log10 weights (exp_w[chain][step]).
-cudaError_t launch_comp_export(const ChainSpec &c, const CompTuning &t, const float *init_seg, const float2 *logtab,
+cudaError_t launch_comp_export(const ChainSpec &c, const CompTuning &t, const float *init_seg, const float2 *fixtab,
                                const float2 *lintab, LutMetaF m, const float x0[3], float *exp_pos, double *exp_w,
-                               ChainOut *out, cudaStream_t st);
+                               ChainOut *out, cudaStream_t st, LogFixed lf = LogFixed{0.0, 0.0});
 // Adjoint replay: per chain the weight-averaged gradients of log10 w with respect to
 // (mu_s, eps, receiver x, y, z) and the sum of the weights w/10^ref_log10, reduced over
 // chains into grad_out[6].
 cudaError_t launch_comp_adjoint(const ChainSpec &c, const CompTuning &t, const float *init_seg, const float2 *lintab,
                                 LutMetaF m, const float *lut, const float *dmu, const float *deps, float ref_log10,
                                 double *grad_chains, double *grad_out, cudaStream_t st);
+
+// Batched persistent form: one launch runs the chains of many experiments that share a
+// kernel shape. Work items (experiment, first chain) are taken from *d_counter (zeroed by
+// the caller) by persistent CTAs; each experiment's chains write out[out_offset + chain].
+struct BatchShape {
+    int group, spl, warps;
+    int exact;               // tables are (L_i, L_{i+1}-L_i) with a log2 per segment
+    int lut_smem;            // stage each item's table in shared memory (else read through L1)
+};
+struct BatchExpHost {
+    ChainSpec spec;
+    LutMetaF meta;
+    LogFixed lf;
+    const float2 *tab;       // device table of meta.bins entries in the shape's form
+    const float *init_seg;   // device initial segment vectors
+    uint32_t out_offset;
+};
+size_t batch_exp_bytes();
+void batch_pack_experiments(const BatchExpHost *in, uint32_t n, void *dst);
+bool batch_shape_supported(const BatchShape &s, uint32_t n_max, uint32_t k_eff);
+size_t batch_smem_bytes(const BatchShape &s, uint32_t bins);
+int batch_chains_per_block(const BatchShape &s);
+cudaError_t launch_batch(const BatchShape &s, const void *d_exps, const uint2 *d_items, uint32_t n_items,
+                         uint32_t *d_counter, ChainOut *out, int bins, int grid, cudaStream_t st);
 
 // ----------------------------------------------------------- reduction (chain_plain.cu)
 cudaError_t launch_reduce(const ChainOut *chains, uint32_t n, ReduceOut *out, cudaStream_t st);
@@ -124,9 +157,9 @@ cudaError_t launch_weigh_plain(const float *pos, uint64_t n_paths, uint32_t n_se
                                const float *lut, LutMetaF m, double absorption_factor,
                                double *log10w, uint8_t *valid, int32_t *bins, cudaStream_t st);
 cudaError_t launch_weigh_comp(const float *pos, uint64_t n_paths, uint32_t n_segments, float inv_ds,
-                              const float2 *logtab, const float2 *lintab, int exact_blend, LutMetaF m,
+                              const float2 *fixtab, const float2 *lintab, int exact_blend, LutMetaF m,
                               double log10_absorption, double *log10w, uint8_t *valid, int32_t *bins,
-                              cudaStream_t st);
+                              cudaStream_t st, LogFixed lf = LogFixed{0.0, 0.0});
 
 // ------------------------------------------------------------ normaliser (norm.cu)
 uint32_t norm_partial_blocks();

@@ -223,33 +223,6 @@ __global__ void __launch_bounds__(1024) lut_finalize_kernel(uint32_t bins, doubl
     }
 }
 
-__device__ __forceinline__ void atomic_max_nonneg(double *addr, double v)
-{
-    // Non-negative doubles order like their bit patterns.
-    atomicMax(reinterpret_cast<unsigned long long *>(addr), (unsigned long long)__double_as_longlong(v));
-}
-
-// Per bin: (log10 L_i, secant slope of log10(blend) over the bin in curvature units).
-// With the reference's interpolation weight in curvature units (PathWeighters.cpp:79-82),
-// the blend over bin i is L_i (1 + d (L_{i+1}/L_i - 1)) for d in [0, step); the secant
-// through d = 0 and d = step has error at most (step (L_{i+1}/L_i - 1))^2 / (8 ln 10),
-// reported through max_err so the caller can fall back to the exact blend.
-__global__ void lut_logtable_kernel(uint32_t bins, const float *lut32, float step, float2 *out, double *max_err)
-{
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= bins) return;
-    const double li = (double)lut32[i];
-    double slope = 0.0, err = 0.0;
-    if (i + 1 < bins) {
-        const double a = (double)lut32[i + 1] / li - 1.0;
-        const double st = (double)step;
-        slope = log10(1.0 + st * a) / st;
-        err = (st * a) * (st * a) / (8.0 * 2.302585092994046);
-    }
-    out[i] = make_float2((float)log10(li), (float)slope);
-    if (max_err) atomic_max_nonneg(max_err, err);
-}
-
 }  // namespace
 
 cudaError_t launch_lut_build(const LutBuildSpec &s, double *out64, double *d_mus, double *d_eps, cudaStream_t st)
@@ -262,13 +235,6 @@ cudaError_t launch_lut_build(const LutBuildSpec &s, double *out64, double *d_mus
 cudaError_t launch_lut_finalize(uint32_t bins, double *lut64, float *out32, double *minmax, cudaStream_t st)
 {
     lut_finalize_kernel<<<1, 1024, 0, st>>>(bins, lut64, out32, minmax);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_lut_logtable(uint32_t bins, const float *lut32, float step, float2 *out, double *max_err,
-                                cudaStream_t st)
-{
-    lut_logtable_kernel<<<(bins + 255) / 256, 256, 0, st>>>(bins, lut32, step, out, max_err);
     return cudaGetLastError();
 }
 

@@ -88,10 +88,11 @@ struct twisty_ctx {
     // tables for the current key
     bool lut_ready = false;
     uint64_t lut_key[4] = {0, 0, 0, 0};
-    DevBuf lut64, lut32, logtab, lintab, dmus, deps, lutaux;
+    DevBuf lut64, lut32, fixtab, lintab, dmus, deps, lutaux;
     LutMetaF meta{};
-    double min_w = 0, max_w = 0, logtab_err = 0;
+    double min_w = 0, max_w = 0, secant_err = 0;
     int exact_blend = 0;
+    LogFixed lf{0.0, 0.0};   // fixed-point form of fixtab; inv_scale 0 when exact_blend
     std::vector<float> ext_lut;
     twisty_lut_info ext_info{};
 
@@ -168,7 +169,7 @@ void build_tables(twisty_ctx *ctx, float ds, bool derivatives)
     ctx->lut_ready = false;
     cudaStream_t st = ctx->stream;
     ck(ctx->lut32.ensure(sizeof(float) * bins), "alloc table");
-    ck(ctx->logtab.ensure(sizeof(float2) * bins), "alloc log table");
+    ck(ctx->fixtab.ensure(sizeof(float2) * bins), "alloc fixed-point table");
     ck(ctx->lintab.ensure(sizeof(float2) * bins), "alloc linear table");
     ck(ctx->lutaux.ensure(sizeof(double) * 4), "alloc table scratch");
     std::vector<float> host32(bins);
@@ -236,22 +237,20 @@ void build_tables(twisty_ctx *ctx, float ds, bool derivatives)
     }
     for (uint32_t i = 0; i < bins; ++i)
         if (!std::isfinite(host32[i])) fail(TWISTY_ERR_LUT_INVALID, "weight table has non-finite entries");
-    // compensated-form tables
-    ck(cudaMemsetAsync(ctx->lutaux.p, 0, sizeof(double), st), "memset");
-    ck(launch_lut_logtable(bins, ctx->lut32.as<float>(), ctx->meta.step, ctx->logtab.as<float2>(), ctx->lutaux.as<double>(), st),
-       "log table");
-    std::vector<float2> lin(bins);
-    for (uint32_t i = 0; i < bins; ++i) {
-        const float a = host32[i], b = host32[i + 1 < bins ? i + 1 : i];
-        lin[i] = make_float2(a, b - a);
-    }
-    ck(cudaMemcpyAsync(ctx->lintab.p, lin.data(), sizeof(float2) * bins, cudaMemcpyHostToDevice, st), "upload linear table");
-    double err = 0;
-    ck(cudaMemcpyAsync(&err, ctx->lutaux.p, sizeof(double), cudaMemcpyDeviceToHost, st), "read table error");
+    // compensated-form tables, built for lanes of up to 32 segments (every kernel shape).
+    // The fixed-point secant form is used only when its worst-case error is below 1e-7 per
+    // segment; otherwise the exact blend.
+    std::vector<float> lin, fix;
+    double c0 = 0.0, inv_scale = 0.0, err = 0.0;
+    const bool fixed_ok = compensated_tables(host32.data(), bins, ctx->meta.step, 32, lin, fix, c0, inv_scale, err);
+    ck(cudaMemcpyAsync(ctx->lintab.p, lin.data(), sizeof(float) * lin.size(), cudaMemcpyHostToDevice, st), "upload linear table");
+    if (fixed_ok)
+        ck(cudaMemcpyAsync(ctx->fixtab.p, fix.data(), sizeof(float) * fix.size(), cudaMemcpyHostToDevice, st),
+           "upload fixed-point table");
     ck(cudaStreamSynchronize(st), "tables");
-    ctx->logtab_err = err;
-    // The secant form is used only when its worst-case error is below 1e-7 per segment.
-    ctx->exact_blend = (err > 1e-7) ? 1 : 0;
+    ctx->secant_err = err;
+    ctx->exact_blend = fixed_ok ? 0 : 1;
+    ctx->lf = fixed_ok ? LogFixed{c0, inv_scale} : LogFixed{0.0, 0.0};
     std::memcpy(ctx->lut_key, key, sizeof(key));
     ctx->lut_ready = true;
 }
@@ -408,8 +407,8 @@ void launch(twisty_ctx *ctx, cudaStream_t st)
                                   step, (int32_t)p.num_curvature_steps, ctx->chain_out.as<ChainOut>(), st),
                "fp64 chain kernel");
         } else {
-            ck(launch_comp_chains(c, ctx->tuning, ctx->init_seg.as<float>(), ctx->logtab.as<float2>(), ctx->lintab.as<float2>(),
-                                  ctx->meta, ctx->chain_out.as<ChainOut>(), ctx->partials.as<double2>(), st),
+            ck(launch_comp_chains(c, ctx->tuning, ctx->init_seg.as<float>(), ctx->fixtab.as<float2>(), ctx->lintab.as<float2>(),
+                                  ctx->meta, ctx->chain_out.as<ChainOut>(), ctx->partials.as<double2>(), st, ctx->lf),
                "compensated chain kernel");
         }
     }
@@ -678,7 +677,7 @@ void twisty_destroy(twisty_ctx *ctx)
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    DevBuf *bufs[] = {&ctx->lut64, &ctx->lut32, &ctx->logtab, &ctx->lintab, &ctx->dmus, &ctx->deps, &ctx->lutaux,
+    DevBuf *bufs[] = {&ctx->lut64, &ctx->lut32, &ctx->fixtab, &ctx->lintab, &ctx->dmus, &ctx->deps, &ctx->lutaux,
                       &ctx->init_pos, &ctx->init_seg, &ctx->state, &ctx->chain_out, &ctx->partials, &ctx->reduce_out,
                       &ctx->norm_scratch};
     for (DevBuf *b : bufs) b->release();
@@ -758,9 +757,9 @@ twisty_status twisty_weight_paths(twisty_ctx *ctx, const twisty_bc *bc, const fl
             const float inv_ds = (float)N / bc->arclength;
             const double af = (double)std::exp(-ctx->p.absorption * ds);
             if (form == TWISTY_FORM_COMPENSATED) {
-                ck(launch_weigh_comp(dpos.as<float>(), n_paths, N, inv_ds, ctx->logtab.as<float2>(), ctx->lintab.as<float2>(),
+                ck(launch_weigh_comp(dpos.as<float>(), n_paths, N, inv_ds, ctx->fixtab.as<float2>(), ctx->lintab.as<float2>(),
                                      ctx->exact_blend, ctx->meta, std::log10(af), dw.as<double>(), dv.as<uint8_t>(),
-                                     bins ? db.as<int32_t>() : nullptr, st),
+                                     bins ? db.as<int32_t>() : nullptr, st, ctx->lf),
                    "weigh kernel");
             } else if (form == TWISTY_FORM_PLAIN_FP32) {
                 ck(launch_weigh_plain(dpos.as<float>(), n_paths, N, inv_ds, ctx->lut32.as<float>(), ctx->meta, af,
@@ -891,10 +890,11 @@ twisty_status twisty_export_paths(twisty_ctx *ctx, const twisty_bc *bc, const ch
                                            ctx->meta, dout.as<ChainOut>(), ctx->stream, dpos.as<float>(), dw.as<double>()),
                        "export replay");
                 } else if (ctx->p.form == TWISTY_FORM_COMPENSATED) {
+                    if (ce.has_eval_shift) fail(TWISTY_ERR_UNSUPPORTED, "eval_end_shift applies to forward passes of the compensated form only");
                     const float x0[3] = {bc->start_pos.x, bc->start_pos.y, bc->start_pos.z};
-                    ck(launch_comp_export(ce, ctx->tuning, ctx->init_seg.as<float>(), ctx->logtab.as<float2>(),
+                    ck(launch_comp_export(ce, ctx->tuning, ctx->init_seg.as<float>(), ctx->fixtab.as<float2>(),
                                           ctx->lintab.as<float2>(), ctx->meta, x0, dpos.as<float>(), dw.as<double>(),
-                                          dout.as<ChainOut>(), ctx->stream),
+                                          dout.as<ChainOut>(), ctx->stream, ctx->lf),
                        "export replay");
                 } else {
                     fail(TWISTY_ERR_UNSUPPORTED, "path export runs the plain and compensated forms");
@@ -937,6 +937,8 @@ twisty_status twisty_adjoint(twisty_ctx *ctx, const twisty_bc *bc, const twisty_
     return guard(ctx, [&] {
         if (ctx->p.form != TWISTY_FORM_COMPENSATED) fail(TWISTY_ERR_UNSUPPORTED, "the adjoint replays the compensated form");
         if (ctx->p.lut_mode != TWISTY_LUT_FP64) fail(TWISTY_ERR_UNSUPPORTED, "the adjoint needs lut_mode FP64 (derivative tables)");
+        const twisty_vec3 &sh = ctx->p.eval_end_shift;
+        if (sh.x != 0.f || sh.y != 0.f || sh.z != 0.f) fail(TWISTY_ERR_UNSUPPORTED, "eval_end_shift applies to forward passes only");
         prepare(ctx, bc);
         const uint32_t N = ctx->p.num_segments;
         const float ds = bc->arclength / (float)N;
