@@ -113,6 +113,11 @@ typedef struct twisty_params {
     int32_t bootstrap_kind;      /* 0 auto, 1 reference recursion (N-2 in {4,6,8,12,16,24,...}), 2 arc */
     twisty_vec3 eval_end_shift;  /* weights evaluated with the receiver moved by this vector,
                                     the chain itself unchanged (finite-difference checks) */
+    /* compensated-form kernel shape; 0 = chosen from N. comp_group lanes per chain (8, 16,
+       32) x comp_spl segments per lane (>= N in total), comp_warps warps per CTA. */
+    uint32_t comp_group;
+    uint32_t comp_spl;
+    uint32_t comp_warps;
 } twisty_params;
 
 /* ExperimentRunner::ExperimentResults (Twisty/ExperimentRunner.h:73-82). */

@@ -71,6 +71,9 @@ class Params(C.Structure):
         ("experiment_id", C.c_uint32),
         ("bootstrap_kind", C.c_int32),
         ("eval_end_shift", Vec3),
+        ("comp_group", C.c_uint32),
+        ("comp_spl", C.c_uint32),
+        ("comp_warps", C.c_uint32),
     ]
 
 

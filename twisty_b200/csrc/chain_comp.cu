@@ -15,20 +15,25 @@
 //    rotated tangent is renormalised by one Newton step, so |t_i| = 1 to an ulp and the
 //    full recompute needs no normalisation: kappa_i = |t_{i+1} - t_i| N/S.
 //  * Shared-memory address of segment s = j*SPL + m of the chain in lanes q*G..q*G+G-1:
-//    row m, column (q*G + j + m*C) mod 32 with C = max(1, G/SPL). Rows make the full
-//    recompute (all lanes, same m) conflict-free; the column shift spreads the k
-//    consecutive segments of a rotation over distinct banks (at most 2-way conflicts).
+//    m*P + q*G + j with row pitch P = 32 + C, C = max(1, G/SPL) floats. A lane's own
+//    segments are one base register plus immediate offsets; the full recompute (all lanes,
+//    same m) reads 32 consecutive words (conflict-free); the pitch shifts row m by m*C
+//    banks, which spreads the k consecutive segments of a rotation over distinct banks (at
+//    most 2-way conflicts).
 //  * The table is staged once per CTA in shared memory as float2. In the fixed-point form
-//    entry i holds round((log10 L_i - c0) 2^s) as int32 bits and the secant slope of
-//    log10 of the blend over the bin: a segment costs one 8-byte LDS, one integer add (exact)
-//    and one FMA (the interpolation correction), and lanes combine their sums exactly with
-//    integer adds. When the fixed point or the secant would lose more than ~1e-7 per
-//    segment, the host selects the exact form: (L_i, L_{i+1} - L_i), a log2 per segment and a
-//    Kahan-compensated FP32 sum combined across lanes by TwoSum.
-//  * The chain's running sum is a log-sum-exp accumulator: reference exponent = the running
-//    maximum, mantissa sum Kahan-compensated in FP32, rescaled when a new maximum arrives.
-//    FP64 appears only per path (assembling the log10 weight), in the per-CTA log-sum-exp
-//    of the chains and in the global reduction.
+//    entry i holds round((log10 L_i - c0) 2^s) as uint32 bits and the change of log10 of
+//    the blend across the bin (secant): a segment costs one 8-byte LDS, one integer add
+//    (exact) and one FMA (the interpolation correction). Each lane rounds its correction
+//    sum to the same fixed point, the group adds the lanes' totals with integer shuffles
+//    (exact), and the chain's running log-sum-exp keeps its reference exponent as an
+//    integer path total, so a path's weight relative to the running maximum is exp2 of an
+//    exact integer difference. The host scales the table so that N+1 entries stay below
+//    2^31; when that leaves fewer than 22 fraction bits, or the secant would lose more
+//    than ~1e-7 per segment, the host selects the exact form instead: (L_i, L_{i+1} - L_i),
+//    a log2 per segment, a Kahan-compensated FP32 sum combined across lanes by TwoSum and
+//    a log-sum-exp over (hi, lo) float pairs.
+//  * FP64 appears only per chain (assembling its log10 sum), in the per-CTA log-sum-exp of
+//    the chains and in the global reduction (and per path in the exact form).
 //  * Proposals: lane j of a group draws the Philox proposal of step base+j (one draw per
 //    lane per G steps) and shuffles broadcast it.
 #include "kernels.h"
@@ -52,6 +57,8 @@ struct CompConsts {
     float rsnap;         // 1e-3 / step: overshoot that counts as clamped
     float step;
     int32_t bins;
+    float fscale;        // 2^s of the fixed-point table
+    float l2s;           // 2^-s log2(10): fixed-point units -> log2
     double lw_offset;    // (N-1) c0 of the fixed-point table
     double inv_scale;    // 2^-s of the fixed-point table
 };
@@ -60,6 +67,13 @@ __device__ __forceinline__ float sqrt_approx(float x)
 {
     float r;
     asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ float ex2_approx(float x)
+{
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
 }
 
@@ -106,21 +120,13 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float x)
     s = t;
 }
 
-// Per-lane partial of one path's log10 weight. ISUM is uint32_t where the table was built
-// for this lane's segment count, uint64_t where any count must fit.
-template <class ISUM>
-struct PathAcc {
-    ISUM isum;       // fixed point: sum of the uint32 entries
-    float csum;      // fixed point: sum of the interpolation corrections (NaN marks an invalid path)
-    float ks, kc;    // exact: Kahan pair
-};
-
-// One segment: |t_{i+1}-t_i|^2 -> bin -> table -> accumulate. CLAMP handles tables whose
-// curvature range the path can leave; tables spanning [0, 2.02 N/S] (the reference's)
-// cannot be left by unit tangents (|t_{i+1}-t_i| <= 2).
-template <bool EXACT, bool CLAMP, class ISUM>
-__device__ __forceinline__ void segment(float qq, const float2 *__restrict__ tab, const CompConsts &k, PathAcc<ISUM> &a,
-                                        uint32_t &clamped, int32_t *bin_out)
+// Fractional bin index of |t_{i+1}-t_i|^2 and its bin. CLAMP handles tables whose curvature
+// range a path can leave; tables spanning [0, 2.02 N/S] (the reference's) cannot be left by
+// unit tangents (|t_{i+1}-t_i| <= 2). r >= 0 or NaN after this (NaN converts to bin 0 and
+// propagates through the interpolation fraction); the bound on the bin also keeps a
+// non-finite tangent, which only a degenerate zero-length chord can produce, in the table.
+template <bool CLAMP>
+__device__ __forceinline__ float bin_of(float qq, const CompConsts &k, uint32_t &clamped, int32_t &L)
 {
     float r = fmaf(sqrt_approx(qq), k.kscale, k.roff);
     if (CLAMP) {
@@ -130,27 +136,16 @@ __device__ __forceinline__ void segment(float qq, const float2 *__restrict__ tab
             r = k.rmax;
         }
     }
-    // r >= 0 or NaN here (NaN converts to 0); the bound also keeps a non-finite tangent,
-    // which only a degenerate zero-length chord can produce, inside the table
-    const int32_t L = min((int32_t)r, k.bins - 1);
-    if (bin_out) *bin_out = isnan(r) ? -1 : L;
-    const float d = (r - (float)L) * k.step;
-    const float2 e = tab[L];
-    if (EXACT) {
-        kahan_add(a.ks, a.kc, __log2f(fmaf(d, e.y, e.x)) * kLog10_2);
-    } else {
-        a.isum += (ISUM)__float_as_uint(e.x);
-        a.csum = fmaf(d, e.y, a.csum);
-    }
+    L = min((int32_t)r, k.bins - 1);
+    return r;
 }
 
-// Full recompute of one path's log10 weight. tan(m, x, y, z) gives the unit tangent of
-// segment j*SPL+m of this lane. Returns the group-wide log10 weight (absorption excluded).
-template <int G, int SPL, bool EXACT, bool CLAMP, class ISUM, class TanFn, class BinFn>
-__device__ __forceinline__ double path_log10(uint32_t j, uint32_t N, const float2 *__restrict__ tab,
-                                             const CompConsts &k, TanFn tan, BinFn bin_sink, uint32_t &clamped)
+// Walk the curvatures this lane owns: seg(i, qq) for curvature i = base+m-1 (between
+// segments base+m-1 and base+m), the last one with the next lane's first tangent.
+// tan(m, x, y, z) gives the unit tangent of segment j*SPL+m.
+template <int G, int SPL, class TanFn, class SegFn>
+__device__ __forceinline__ void for_curvatures(uint32_t j, uint32_t N, TanFn tan, SegFn seg)
 {
-    PathAcc<ISUM> a{0, 0.0f, 0.0f, 0.0f};
     float t0x = 0.f, t0y = 0.f, t0z = 0.f, px = 0.f, py = 0.f, pz = 0.f;
     const uint32_t base = j * SPL;
 #pragma unroll
@@ -161,9 +156,7 @@ __device__ __forceinline__ double path_log10(uint32_t j, uint32_t N, const float
             t0x = tx; t0y = ty; t0z = tz;
         } else if (base + m <= N - 1) {
             const float dx = tx - px, dy = ty - py, dz = tz - pz;
-            int32_t b;
-            segment<EXACT, CLAMP, ISUM>(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), tab, k, a, clamped, &b);
-            bin_sink(base + m - 1, b);
+            seg(base + m - 1, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
         }
         px = tx; py = ty; pz = tz;
     }
@@ -172,28 +165,78 @@ __device__ __forceinline__ double path_log10(uint32_t j, uint32_t N, const float
     const float nz = __shfl_down_sync(FULL, t0z, 1, G);
     if (base + SPL <= N - 1) {
         const float dx = nx - px, dy = ny - py, dz = nz - pz;
-        int32_t b;
-        segment<EXACT, CLAMP, ISUM>(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), tab, k, a, clamped, &b);
-        bin_sink(base + SPL - 1, b);
+        seg(base + SPL - 1, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
     }
+}
+
+// Generic full recompute of one path's log10 weight (absorption excluded), for the exact
+// table or, with 64-bit lane sums, for the fixed-point table at any lane width. bin_sink(i,
+// bin) receives every curvature's bin (-1 for NaN).
+template <int G, int SPL, bool EXACT, bool CLAMP, class TanFn, class BinFn>
+__device__ __forceinline__ double path_log10(uint32_t j, uint32_t N, const float2 *__restrict__ tab,
+                                             const CompConsts &k, TanFn tan, BinFn bin_sink, uint32_t &clamped)
+{
+    unsigned long long isum = 0;
+    float csum = 0.f, ks = 0.f, kc = 0.f;
+    for_curvatures<G, SPL>(j, N, tan, [&](uint32_t i, float qq) {
+        int32_t L;
+        const float r = bin_of<CLAMP>(qq, k, clamped, L);
+        bin_sink(i, isnan(r) ? -1 : L);
+        const float frac = r - (float)L;
+        const float2 e = tab[L];
+        if (EXACT) {
+            kahan_add(ks, kc, __log2f(fmaf(frac * k.step, e.y, e.x)) * kLog10_2);
+        } else {
+            isum += __float_as_uint(e.x);
+            csum = fmaf(frac, e.y, csum);
+        }
+    });
     if (EXACT) {
-        float hi = a.ks, lo = -a.kc;
+        float hi = ks, lo = -kc;
         group_sum_pair<G>(hi, lo);
         return (double)hi + (double)lo;
     }
-    const unsigned long long is = group_sum<G>((unsigned long long)a.isum);
-    const float cs = group_sum<G>(a.csum);
+    const unsigned long long is = group_sum<G>(isum);
+    const float cs = group_sum<G>(csum);
     return k.lw_offset + (double)is * k.inv_scale + (double)cs;
+}
+
+// Fixed-point full recompute for chains: the group's total of table entries plus rounded
+// interpolation corrections, in units of 2^-s (exact: the table was scaled for N). *bad is
+// set when any curvature of the path is NaN.
+template <int G, int SPL, bool CLAMP, class TanFn>
+__device__ __forceinline__ uint32_t path_fixed(uint32_t j, uint32_t gbase, uint32_t N, const float2 *__restrict__ tab,
+                                               const CompConsts &k, TanFn tan, bool &bad, uint32_t &clamped)
+{
+    uint32_t isum = 0;
+    float csum = 0.f;
+    for_curvatures<G, SPL>(j, N, tan, [&](uint32_t, float qq) {
+        int32_t L;
+        const float r = bin_of<CLAMP>(qq, k, clamped, L);
+        const float2 e = tab[L];
+        isum += __float_as_uint(e.x);
+        csum = fmaf(r - (float)L, e.y, csum);
+    });
+    const uint32_t nan_lanes = __ballot_sync(FULL, isnan(csum));
+    constexpr uint32_t gmask = (G == 32) ? FULL : ((1u << G) - 1u);
+    bad = ((nan_lanes >> gbase) & gmask) != 0u;
+    isum += (uint32_t)__float2int_rn(csum * k.fscale);
+    return group_sum<G>(isum);
 }
 
 template <int G, int SPL>
 struct Layout {
     static constexpr int C = (G / SPL) > 1 ? (G / SPL) : 1;
-    __device__ __forceinline__ static uint32_t addr(uint32_t lane_in_warp_base, uint32_t owner, uint32_t m)
+    static constexpr int P = 32 + C;                 // row pitch (floats)
+    static constexpr int PLANE = SPL * P;            // one plane of a warp (floats)
+    static constexpr int WARP = 4 * PLANE;           // tangents x, y, z and lengths
+    __device__ __forceinline__ static uint32_t addr(uint32_t gbase, uint32_t owner, uint32_t m)
     {
-        return m * 32u + ((lane_in_warp_base + owner + m * C) & 31u);
+        return m * (uint32_t)P + gbase + owner;
     }
 };
+
+constexpr int warp_state_floats(int G, int SPL) { return 4 * SPL * (32 + ((G / SPL) > 1 ? (G / SPL) : 1)); }
 
 enum { kModeForward = 0, kModeExport = 1, kModeAdjoint = 2 };
 
@@ -252,12 +295,6 @@ __device__ __forceinline__ void stage_table(float4 *smem4, const float2 *__restr
     if ((bins & 1) && threadIdx.x == 0) reinterpret_cast<float2 *>(smem4)[bins - 1] = tab_g[bins - 1];
 }
 
-// Shared-memory planes of one warp: tangents x/y/z and lengths, SPL*32 floats each.
-template <int SPL>
-constexpr int kPlaneFloats = SPL * 32;
-template <int SPL>
-constexpr int kWarpStateFloats = 4 * SPL * 32;
-
 // One Markov chain run by the G lanes of one group on its own planes st (tangents x, y, z,
 // lengths): initial state from init_seg (segment vectors), burn_in + steps proposals, a full
 // recompute of every weighted path, and the chain's running log-sum-exp. Writes out[chain]
@@ -268,9 +305,10 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                                              uint32_t gbase, uint32_t j, uint32_t chain, bool real_chain,
                                              ChainOut *__restrict__ out, const ModeArgs &ma)
 {
+    constexpr bool FIX = !EXACT && MODE != kModeAdjoint;
     const uint32_t N = c.n_segments;
     using Lay = Layout<G, SPL>;
-    float *sx = st, *sy = st + kPlaneFloats<SPL>, *sz = st + 2 * kPlaneFloats<SPL>, *sl = st + 3 * kPlaneFloats<SPL>;
+    float *sx = st, *sy = st + Lay::PLANE, *sz = st + 2 * Lay::PLANE, *sl = st + 3 * Lay::PLANE;
 
 #pragma unroll
     for (int m = 0; m < SPL; ++m) {
@@ -298,12 +336,16 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
     const uint32_t steps_c = real_chain ? ((chain == c.n_chains - 1) ? c.last_steps : c.steps) : 0;
     const uint32_t total = c.burn_in + c.steps;
     const uint32_t gchain = c.chain0 + (real_chain ? chain : 0);
-    float lse_m = 0.f, lse_s = 0.f, lse_c = 0.f;
+    // rotation rounds actually needed: sub-chains have at most k_eff segments
+    const uint32_t rounds = (c.k_eff + G - 1) / G;
+    float lse_m = 0.f, lse_s = 0.f, lse_c = 0.f;  // exact form: running max (float) and Kahan sum
+    uint32_t lse_t = 0;                             // fixed form: running max as a path total
     uint32_t valid = 0, failed = 0, clamped = 0;
     float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 
+    const uint32_t own = gbase + j;
     auto tan_smem = [&](int m, float &x, float &y, float &z) {
-        const uint32_t a = Lay::addr(gbase, j, m);
+        const uint32_t a = own + (uint32_t)(m * Lay::P);
         x = sx[a];
         y = sy[a];
         z = sz[a];
@@ -337,6 +379,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
             float cx = 0.f, cy = 0.f, cz = 0.f;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
+                if (r > 0 && (uint32_t)r >= rounds) break;
                 const uint32_t s = left + j + r * G;
                 va[r] = Lay::addr(gbase, s / SPL, s % SPL);
                 if (s < right) {
@@ -359,6 +402,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
             __syncwarp();
 #pragma unroll
             for (int r = 0; r < R; ++r) {
+                if (r > 0 && (uint32_t)r >= rounds) break;
                 const uint32_t s = left + j + r * G;
                 if (s < right) {
                     const float x = vx[r], y = vy[r], z = vz[r];
@@ -376,13 +420,88 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
             if (step < c.burn_in) continue;
             const uint32_t wstep = step - c.burn_in;
             const bool active = wstep < steps_c;
+
+            if (FIX) {
+                bool bad;
+                const uint32_t tot = path_fixed<G, SPL, CLAMP>(j, gbase, N, s_tab, kc, tan_smem, bad, clamped);
+                if (MODE == kModeExport) {
+                    const double w = bad ? NAN : kc.lw_offset + (double)tot * kc.inv_scale;
+                    // positions below
+                    if (active) {
+                        const size_t pidx = (size_t)chain * c.steps + wstep;
+                        if (j == 0) ma.exp_w[pidx] = isnan(w) ? NAN : w + (N - 1) * ma.log10_abs;
+                    }
+                }
+                if (MODE == kModeExport) {
+                    // positions x_0 + prefix sums of l_s t_s, in double; every lane takes part in
+                    // the scan, only active chains write
+                    double px = 0.0, py = 0.0, pz = 0.0;
+                    double lx[SPL], ly[SPL], lz[SPL];
+#pragma unroll
+                    for (int m = 0; m < SPL; ++m) {
+                        const uint32_t a = Lay::addr(gbase, j, m);
+                        const bool in = j * SPL + m < N;
+                        const double l = in ? (double)sl[a] : 0.0;
+                        px += l * (double)sx[a];
+                        py += l * (double)sy[a];
+                        pz += l * (double)sz[a];
+                        lx[m] = px; ly[m] = py; lz[m] = pz;
+                    }
+                    double ex = px, ey = py, ez = pz;  // inclusive scan of lane totals
+#pragma unroll
+                    for (int o = 1; o < G; o <<= 1) {
+                        const double ux = __shfl_up_sync(FULL, ex, o, G), uy = __shfl_up_sync(FULL, ey, o, G),
+                                     uz = __shfl_up_sync(FULL, ez, o, G);
+                        if ((int)j >= o) { ex += ux; ey += uy; ez += uz; }
+                    }
+                    ex -= px; ey -= py; ez -= pz;  // exclusive
+                    if (active) {
+                        const size_t pidx = (size_t)chain * c.steps + wstep;
+                        float *dst = ma.exp_pos + pidx * 3 * (size_t)(N + 1);
+                        if (j == 0) { dst[0] = ma.x0[0]; dst[1] = ma.x0[1]; dst[2] = ma.x0[2]; }
+#pragma unroll
+                        for (int m = 0; m < SPL; ++m) {
+                            const uint32_t s = j * SPL + m;
+                            if (s < N) {
+                                dst[3 * (s + 1)] = (float)((double)ma.x0[0] + ex + lx[m]);
+                                dst[3 * (s + 1) + 1] = (float)((double)ma.x0[1] + ey + ly[m]);
+                                dst[3 * (s + 1) + 2] = (float)((double)ma.x0[2] + ez + lz[m]);
+                            }
+                        }
+                    }
+                }
+                if (!active) continue;
+                if (bad) {
+                    ++failed;
+                    continue;
+                }
+                if (valid == 0) {
+                    lse_t = tot;
+                    lse_s = 1.f;
+                    lse_c = 0.f;
+                } else {
+                    // exact integer difference: totals stay below 2^31
+                    const float x = (float)(int32_t)(tot - lse_t) * kc.l2s;
+                    float term = 1.f;
+                    if (x > 0.f) {
+                        const float f = ex2_approx(-x);
+                        lse_s *= f;
+                        lse_c *= f;
+                        lse_t = tot;
+                    } else {
+                        term = ex2_approx(x);
+                    }
+                    kahan_add(lse_s, lse_c, term);
+                }
+                ++valid;
+                continue;
+            }
+
             double w;
             if (MODE == kModeAdjoint) {
                 // log10 weight and d/d(mu_s), d/d(eps) of this lane's segments (exact blend)
                 float s = 0.f, cc = 0.f, gmu = 0.f, geps = 0.f;
-                float t0x = 0.f, t0y = 0.f, t0z = 0.f, px = 0.f, py = 0.f, pz = 0.f;
-                const uint32_t b0 = j * SPL;
-                auto seg_term = [&](float qq) {
+                for_curvatures<G, SPL>(j, N, tan_smem, [&](uint32_t, float qq) {
                     float r = fmaf(sqrt_approx(qq), kc.kscale, kc.roff);
                     if (r < 0.f) r = 0.f;
                     if (r > kc.rmax) r = kc.rmax;
@@ -396,25 +515,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                     const float el = __ldg(ma.deps + L), er = __ldg(ma.deps + Rb);
                     gmu += fmaf(d, mr - ml, ml) / v;
                     geps += fmaf(d, er - el, el) / v;
-                };
-#pragma unroll
-                for (int m = 0; m < SPL; ++m) {
-                    float tx, ty, tz;
-                    tan_smem(m, tx, ty, tz);
-                    if (m == 0) { t0x = tx; t0y = ty; t0z = tz; }
-                    else if (b0 + m <= N - 1) {
-                        const float dx = tx - px, dy = ty - py, dz = tz - pz;
-                        seg_term(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
-                    }
-                    px = tx; py = ty; pz = tz;
-                }
-                const float nx = __shfl_down_sync(FULL, t0x, 1, G);
-                const float ny = __shfl_down_sync(FULL, t0y, 1, G);
-                const float nz = __shfl_down_sync(FULL, t0z, 1, G);
-                if (b0 + SPL <= N - 1) {
-                    const float dx = nx - px, dy = ny - py, dz = nz - pz;
-                    seg_term(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
-                }
+                });
                 float hi = s, lo = -cc;
                 group_sum_pair<G>(hi, lo);
                 w = (double)hi + (double)lo;
@@ -439,11 +540,9 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                     if (j == 0) acc[5] += wt;
                 }
             } else {
-                w = path_log10<G, SPL, EXACT, CLAMP, uint32_t>(j, N, s_tab, kc, tan_smem, no_bins, clamped);
+                w = path_log10<G, SPL, true, CLAMP>(j, N, s_tab, kc, tan_smem, no_bins, clamped);
             }
             if (MODE == kModeExport) {
-                // positions x_0 + prefix sums of l_s t_s, in double; every lane takes part in
-                // the scan, only active chains write
                 double px = 0.0, py = 0.0, pz = 0.0;
                 double lx[SPL], ly[SPL], lz[SPL];
 #pragma unroll
@@ -456,14 +555,14 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                     pz += l * (double)sz[a];
                     lx[m] = px; ly[m] = py; lz[m] = pz;
                 }
-                double ex = px, ey = py, ez = pz;  // inclusive scan of lane totals
+                double ex = px, ey = py, ez = pz;
 #pragma unroll
                 for (int o = 1; o < G; o <<= 1) {
                     const double ux = __shfl_up_sync(FULL, ex, o, G), uy = __shfl_up_sync(FULL, ey, o, G),
                                  uz = __shfl_up_sync(FULL, ez, o, G);
                     if ((int)j >= o) { ex += ux; ey += uy; ez += uz; }
                 }
-                ex -= px; ey -= py; ez -= pz;  // exclusive
+                ex -= px; ey -= py; ez -= pz;
                 if (active) {
                     const size_t pidx = (size_t)chain * c.steps + wstep;
                     float *dst = ma.exp_pos + pidx * 3 * (size_t)(N + 1);
@@ -516,9 +615,11 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
         if (j == 0 && real_chain)
             for (int i = 0; i < 6; ++i) ma.grad[(size_t)chain * 6 + i] = (double)acc[i];
     }
-    const double chain_log10 = valid ? (double)lse_m + log10((double)lse_s - (double)lse_c) +
-                                       (double)(N - 1) * ma.log10_abs
-                                     : -INFINITY;
+    double chain_log10 = -INFINITY;
+    if (valid) {
+        const double head = FIX ? kc.lw_offset + (double)lse_t * kc.inv_scale : (double)lse_m;
+        chain_log10 = head + log10((double)lse_s - (double)lse_c) + (double)(N - 1) * ma.log10_abs;
+    }
     if (j == 0 && real_chain && out) {
         ChainOut o;
         o.log10_sum = chain_log10;
@@ -544,7 +645,7 @@ __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompCo
     const int tab_f4 = (bins + 1) / 2;  // float2 entries, padded to float4
     float *s_state = reinterpret_cast<float *>(smem4 + tab_f4);
     const int warps = blockDim.x >> 5;
-    double *s_res = reinterpret_cast<double *>(s_state + warps * kWarpStateFloats<SPL>);
+    double *s_res = reinterpret_cast<double *>(s_state + warps * Layout<G, SPL>::WARP);
     stage_table(smem4, tab_g, bins);
     __syncthreads();
 
@@ -553,7 +654,7 @@ __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompCo
     constexpr int CPW = 32 / G;
     const uint32_t chain = (blockIdx.x * warps + warp) * CPW + q;
     const double cl = chain_body<G, SPL, EXACT, CLAMP, SHIFT, MODE>(
-          c, kc, init_seg, s_tab, s_state + warp * kWarpStateFloats<SPL>, q * G, j, chain, chain < c.n_chains, out, ma);
+          c, kc, init_seg, s_tab, s_state + warp * Layout<G, SPL>::WARP, q * G, j, chain, chain < c.n_chains, out, ma);
     if (j == 0) s_res[warp * CPW + q] = cl;
     __syncthreads();
     // Per-CTA log-sum-exp of the chains, rescaled by the block maximum (FP64).
@@ -599,7 +700,7 @@ __global__ void __launch_bounds__(MAXT, 1) batch_kernel(const BatchExp *__restri
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t q = lane / G, j = lane % G;
     constexpr int CPW = 32 / G;
-    float *st = s_state + warp * kWarpStateFloats<SPL>;
+    float *st = s_state + warp * Layout<G, SPL>::WARP;
     for (;;) {
         if (threadIdx.x == 0) s_item = atomicAdd(counter, 1u);
         __syncthreads();
@@ -617,7 +718,7 @@ __global__ void __launch_bounds__(MAXT, 1) batch_kernel(const BatchExp *__restri
         ma.log10_abs = e.log10_abs;
         const uint32_t chain = it.y + warp * CPW + q;
         chain_body<G, SPL, EXACT, true, false, kModeForward>(e.spec, e.kc, e.init_seg, tab, st, q * G, j, chain,
-                                                              chain < e.spec.n_chains, out + e.out_offset, ma);
+                                                             chain < e.spec.n_chains, out + e.out_offset, ma);
         __syncthreads();
     }
 }
@@ -651,7 +752,7 @@ __global__ void __launch_bounds__(256) weigh_comp_kernel(const float *__restrict
         if (brow) brow[i] = b;
     };
     uint32_t clamped = 0;
-    const double w = path_log10<32, SPL, EXACT, true, unsigned long long>(j, N, tab, kc, tan, sink, clamped);
+    const double w = path_log10<32, SPL, EXACT, true>(j, N, tab, kc, tan, sink, clamped);
     if (j == 0) {
         const bool ok = !isnan(w);
         log10w[p] = ok ? w + (double)(N - 1) * log10_absorption : 0.0;
@@ -701,6 +802,8 @@ CompConsts make_consts(float inv_ds, const LutMetaF &m, uint32_t n_segments, con
     k.bins = m.bins;
     k.lw_offset = (double)(n_segments - 1) * lf.c0;
     k.inv_scale = lf.inv_scale;
+    k.fscale = lf.inv_scale > 0.0 ? (float)(1.0 / lf.inv_scale) : 0.0f;
+    k.l2s = (float)(lf.inv_scale * 3.321928094887362);
     return k;
 }
 
@@ -715,17 +818,16 @@ cudaError_t launch_mode(int mode, const ChainSpec &c, const CompTuning &t, const
     if (!comp_tuning_supported(t, c.n_segments, c.k_eff)) return cudaErrorInvalidValue;
     if (c.has_eval_shift && mode != kModeForward) return cudaErrorInvalidValue;
     if (c.n_chains == 0) return cudaSuccess;
-    const bool exact = t.exact_blend || mode == kModeAdjoint || lf.inv_scale == 0.0;
+    const bool shift = c.has_eval_shift != 0;
+    const bool exact = t.exact_blend || mode == kModeAdjoint || lf.inv_scale == 0.0 || shift;
     const CompConsts kc = make_consts(c.inv_ds, m, c.n_segments, lf);
     const size_t smem = comp_smem_bytes(t, (uint32_t)m.bins);
     const uint32_t blocks = comp_blocks(c, t);
     const float2 *tab = exact ? lintab : fixtab;
     const bool clamp = table_needs_clamp(kc);
-    const bool shift = c.has_eval_shift != 0;
-#define TWISTY_CASE(GG, SS)                                                                                             \
-    if (t.group == GG && t.spl == SS)                                                                                   \
-        return launch_g<GG, SS>(mode, exact || shift, clamp, shift, c, kc, t, init_seg, (exact || shift) ? lintab : tab, \
-                                out, block_partials, ma, smem, blocks, st);
+#define TWISTY_CASE(GG, SS) \
+    if (t.group == GG && t.spl == SS) \
+        return launch_g<GG, SS>(mode, exact, clamp, shift, c, kc, t, init_seg, tab, out, block_partials, ma, smem, blocks, st);
     TWISTY_CASE(8, 2)
     TWISTY_CASE(8, 4)
     TWISTY_CASE(8, 8)
@@ -764,7 +866,7 @@ template <int G, int SPL, bool EXACT, bool LS>
 cudaError_t batch_t(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items, uint32_t *counter,
                     ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st)
 {
-    constexpr int MAXT = (SPL >= 16) ? 512 : 1024;
+    constexpr int MAXT = (SPL >= 16 || G == 8) ? 512 : 1024;
     if (s.warps * 32 > MAXT) return cudaErrorInvalidConfiguration;
     auto kern = batch_kernel<G, SPL, EXACT, LS, MAXT>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -819,7 +921,7 @@ uint32_t comp_default_chains(uint32_t n, int sm_count)
 size_t comp_smem_bytes(const CompTuning &t, uint32_t bins)
 {
     const size_t tab = (size_t)((bins + 1) / 2) * sizeof(float4);
-    const size_t state = (size_t)t.warps_per_block * 4 * t.spl * 32 * sizeof(float);
+    const size_t state = (size_t)t.warps_per_block * warp_state_floats(t.group, t.spl) * sizeof(float);
     const size_t res = (size_t)t.warps_per_block * (32 / t.group) * sizeof(double);
     return tab + state + res;
 }
@@ -922,12 +1024,14 @@ void batch_pack_experiments(const BatchExpHost *in, uint32_t n, void *dst)
 bool batch_shape_supported(const BatchShape &s, uint32_t n_max, uint32_t k_eff)
 {
     CompTuning t{s.group, s.spl, s.warps, s.exact};
-    return comp_tuning_supported(t, n_max, k_eff);
+    const int maxt = (s.spl >= 16 || s.group == 8) ? 512 : 1024;
+    return comp_tuning_supported(t, n_max, k_eff) && s.warps * 32 <= maxt;
 }
 
 size_t batch_smem_bytes(const BatchShape &s, uint32_t bins)
 {
-    return (s.lut_smem ? (size_t)((bins + 1) / 2) * sizeof(float4) : 0) + (size_t)s.warps * 4 * s.spl * 32 * sizeof(float);
+    return (s.lut_smem ? (size_t)((bins + 1) / 2) * sizeof(float4) : 0) +
+           (size_t)s.warps * warp_state_floats(s.group, s.spl) * sizeof(float);
 }
 
 int batch_chains_per_block(const BatchShape &s) { return s.warps * (32 / s.group); }

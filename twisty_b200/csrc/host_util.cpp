@@ -384,7 +384,8 @@ bool params_from_node(const Node &root, twisty_params &p, twisty_bc *bc, std::st
     p.scatter = (float)v;
     p.min_bound = 0.0f;
     p.max_bound = 10.0f / p.eps;  // ExperimentRunner.cpp:169-171
-    // Optional B200 block: experimentParams.b200 { form, lutMode, maxSubChain, maxAngle, numChains, device }
+    // Optional B200 block: experimentParams.b200 { form, lutMode, maxSubChain, maxAngle, numChains, device,
+    // compGroup, compSpl, compWarps }
     if (const Node *b = ep->get("b200")) {
         if (b->kind != Node::Object) {
             err = "experimentParams.b200 must be a mapping";
@@ -396,6 +397,9 @@ bool params_from_node(const Node &root, twisty_params &p, twisty_bc *bc, std::st
         if (b->get("maxAngle") && num(b, "maxAngle", "b200.maxAngle", v, err)) p.max_angle = (float)v;
         if (b->get("numChains") && num(b, "numChains", "b200.numChains", v, err)) p.num_chains = (uint32_t)v;
         if (b->get("device") && num(b, "device", "b200.device", v, err)) p.device = (int32_t)v;
+        if (b->get("compGroup") && num(b, "compGroup", "b200.compGroup", v, err)) p.comp_group = (uint32_t)v;
+        if (b->get("compSpl") && num(b, "compSpl", "b200.compSpl", v, err)) p.comp_spl = (uint32_t)v;
+        if (b->get("compWarps") && num(b, "compWarps", "b200.compWarps", v, err)) p.comp_warps = (uint32_t)v;
         if (!err.empty()) return false;
     }
     if (bc) {
@@ -610,7 +614,7 @@ double norm_k4_log10(float z, float ds)
     return std::log10((double)result);
 }
 
-bool compensated_tables(const float *lut, uint32_t bins, float step, uint32_t spl, std::vector<float> &lin,
+bool compensated_tables(const float *lut, uint32_t bins, float step, uint32_t n_segments, std::vector<float> &lin,
                         std::vector<float> &fix, double &c0, double &inv_scale, double &secant_err)
 {
     lin.assign(2 * (size_t)bins, 0.0f);
@@ -642,22 +646,21 @@ bool compensated_tables(const float *lut, uint32_t bins, float step, uint32_t sp
         secant_err = INFINITY;
         return false;
     }
-    // largest s with spl * round(range * 2^s) < 2^32, at most 30
-    const double cap = std::floor(4294967295.0 / (double)(spl ? spl : 1)) - 1.0;
+    // largest s (at most 30) with range * 2^s + 65 <= (2^31 - 1) / (n_segments + 1)
+    const double cap = std::floor(2147483647.0 / (double)(n_segments + 1));
     const double range = hi - lo;
     int s = 30;
-    while (s > 0 && range * std::ldexp(1.0, s) > cap) --s;
+    while (s > 0 && range * std::ldexp(1.0, s) + 65.0 > cap) --s;
     if (secant_err > 1e-7 || s < 22) return false;
-    c0 = lo;
     inv_scale = std::ldexp(1.0, -s);
+    c0 = lo - 64.0 * inv_scale;
     for (uint32_t i = 0; i < bins; ++i) {
-        double e = std::nearbyint((lg[i] - lo) * std::ldexp(1.0, s));
-        e = std::min(std::max(e, 0.0), cap);
-        const uint32_t u = (uint32_t)e;
+        const double e = 64.0 + std::nearbyint((lg[i] - lo) * std::ldexp(1.0, s));
+        const uint32_t u = (uint32_t)std::min(e, cap - 1.0);
         std::memcpy(&fix[2 * i], &u, 4);
-        double slope = 0.0;
-        if (i + 1 < bins) slope = std::log10(1.0 + st * ((double)lut[i + 1] / (double)lut[i] - 1.0)) / st;
-        fix[2 * i + 1] = (float)slope;
+        double delta = 0.0;
+        if (i + 1 < bins) delta = std::log10(1.0 + st * ((double)lut[i + 1] / (double)lut[i] - 1.0));
+        fix[2 * i + 1] = (float)delta;
     }
     return true;
 }

@@ -51,15 +51,17 @@ bool lut_faithful_host(float mu, float eps, float scatter, float min_bound, floa
                        uint32_t num_steps_int, uint32_t bins, float ds, float *out, float minmax[2]);
 
 // Tables of the compensated form, from the float weight table lut[bins] with bin width
-// `step` (curvature units):
+// `step` (curvature units), for paths of n_segments segments:
 //  * lin[2*bins]: per bin (L_i, L_{i+1} - L_i) for the exact blend;
-//  * fix[2*bins]: per bin (round((log10 L_i - c0) 2^s) as uint32 bits, float secant slope
-//    of log10 of the blend over the bin), c0 = min log10 L_i, with spl * max entry < 2^32
-//    so a lane's sum of spl entries stays exact in 32 bits.
+//  * fix[2*bins]: per bin (round((log10 L_i - c0) 2^s) as uint32 bits, the change of log10
+//    of the blend across the bin, log10(1 + step (L_{i+1}/L_i - 1)), as float), with
+//    c0 = min log10 L_i - 64 2^-s so that every entry is at least 64 and a path total
+//    stays positive under rounded corrections, and (n_segments + 1) * max entry < 2^31 so
+//    that a path total and the difference of two totals are exact in 32 bits.
 // secant_err = the worst per-segment error of the secant, (step a)^2 / (8 ln 10) with
 // a = L_{i+1}/L_i - 1. Returns false (fix unusable, the exact blend is needed) when an
 // entry is not positive, secant_err > 1e-7, or fewer than 22 fraction bits fit.
-bool compensated_tables(const float *lut, uint32_t bins, float step, uint32_t spl, std::vector<float> &lin,
+bool compensated_tables(const float *lut, uint32_t bins, float step, uint32_t n_segments, std::vector<float> &lin,
                         std::vector<float> &fix, double &c0, double &inv_scale, double &secant_err);
 
 // K4 (Twisty/PathWeightUtils.cpp:643-651) and the z of Norm (:729-732), float math.

@@ -160,7 +160,7 @@ void build_tables(twisty_ctx *ctx, float ds, bool derivatives)
     std::memcpy(&f[3], &p.bias, 4);
     std::memcpy(&f[4], &p.max_bound, 4);
     std::memcpy(&f[5], &p.min_bound, 4);
-    key[0] = ((uint64_t)dsb << 32) | (uint64_t)(uint32_t)p.lut_mode;
+    key[0] = ((uint64_t)dsb << 32) | ((uint64_t)(p.num_segments & 0xFFFFFFu) << 8) | (uint64_t)(uint32_t)(p.lut_mode & 0xFF);
     key[1] = ((uint64_t)f[0] << 32) | f[1];
     key[2] = ((uint64_t)f[2] << 32) | f[3];
     key[3] = ((uint64_t)f[4] << 32) ^ ((uint64_t)f[5]) ^ ((uint64_t)bins << 8) ^ ((uint64_t)p.num_steps_int << 40) ^
@@ -237,12 +237,13 @@ void build_tables(twisty_ctx *ctx, float ds, bool derivatives)
     }
     for (uint32_t i = 0; i < bins; ++i)
         if (!std::isfinite(host32[i])) fail(TWISTY_ERR_LUT_INVALID, "weight table has non-finite entries");
-    // compensated-form tables, built for lanes of up to 32 segments (every kernel shape).
-    // The fixed-point secant form is used only when its worst-case error is below 1e-7 per
+    // compensated-form tables, the fixed-point one scaled for paths of this N. The
+    // fixed-point secant form is used only when its worst-case error is below 1e-7 per
     // segment; otherwise the exact blend.
     std::vector<float> lin, fix;
     double c0 = 0.0, inv_scale = 0.0, err = 0.0;
-    const bool fixed_ok = compensated_tables(host32.data(), bins, ctx->meta.step, 32, lin, fix, c0, inv_scale, err);
+    const bool fixed_ok =
+          compensated_tables(host32.data(), bins, ctx->meta.step, p.num_segments, lin, fix, c0, inv_scale, err);
     ck(cudaMemcpyAsync(ctx->lintab.p, lin.data(), sizeof(float) * lin.size(), cudaMemcpyHostToDevice, st), "upload linear table");
     if (fixed_ok)
         ck(cudaMemcpyAsync(ctx->fixtab.p, fix.data(), sizeof(float) * fix.size(), cudaMemcpyHostToDevice, st),
@@ -347,11 +348,24 @@ void prepare(twisty_ctx *ctx, const twisty_bc *bcp)
         max_steps = std::min<uint32_t>(max_steps, 1000000u);
     } else if (p.form == TWISTY_FORM_COMPENSATED) {
         ctx->tuning = comp_default_tuning(N);
+        if (p.comp_group || p.comp_spl) {
+            if (!p.comp_group || !p.comp_spl) fail(TWISTY_ERR_INVALID_CONFIG, "comp_group and comp_spl are set together");
+            ctx->tuning.group = (int)p.comp_group;
+            ctx->tuning.spl = (int)p.comp_spl;
+            if (!p.comp_warps) ctx->tuning.warps_per_block = (p.comp_spl >= 16) ? 16 : 32;
+        }
+        if (p.comp_warps) ctx->tuning.warps_per_block = (int)p.comp_warps;
         ctx->tuning.exact_blend = ctx->exact_blend;
         if (!comp_tuning_supported(ctx->tuning, N, c.k_eff)) fail(TWISTY_ERR_UNSUPPORTED, "no compensated kernel shape for this N / max_sub_chain");
-        const size_t smem = comp_smem_bytes(ctx->tuning, p.num_curvature_steps);
-        if (smem > 227 * 1024) fail(TWISTY_ERR_UNSUPPORTED, "weight table too large to stage in shared memory");
-        if (!requested) requested = comp_default_chains(N, 148);
+        // a large table leaves less shared memory for chain state: fewer warps per CTA
+        const size_t smem_cap = 227 * 1024;
+        while (!p.comp_warps && ctx->tuning.warps_per_block > 4 &&
+               comp_smem_bytes(ctx->tuning, p.num_curvature_steps) > smem_cap)
+            ctx->tuning.warps_per_block -= 4;
+        if (comp_smem_bytes(ctx->tuning, p.num_curvature_steps) > smem_cap)
+            fail(TWISTY_ERR_UNSUPPORTED, "weight table too large to stage in shared memory");
+        if (!requested)
+            requested = (uint32_t)ctx->sm_count * (uint32_t)ctx->tuning.warps_per_block * (32u / (uint32_t)ctx->tuning.group);
     } else {
         if (!requested) requested = (uint32_t)ctx->sm_count * 256;
     }
