@@ -8,18 +8,25 @@
 //
 // B200 layout and arithmetic:
 //  * G lanes cooperate on one chain (G = 8, 16 or 32); lane j owns the SPL contiguous
-//    segments j*SPL .. j*SPL+SPL-1. The chain lives in shared memory as its N unit tangents
-//    t_i and segment lengths l_i (four planes). Rotating the points between left and right
-//    about the chord x_right - x_left turns every tangent t_left .. t_{right-1} by the same
-//    rotation (the chord is the axis and stays fixed) and leaves the lengths alone; each
-//    rotated tangent is renormalised by one Newton step, so |t_i| = 1 to an ulp and the
-//    full recompute needs no normalisation: kappa_i = |t_{i+1} - t_i| N/S.
-//  * Shared-memory address of segment s = j*SPL + m of the chain in lanes q*G..q*G+G-1:
-//    m*P + q*G + j with row pitch P = 32 + C, C = max(1, G/SPL) floats. A lane's own
-//    segments are one base register plus immediate offsets; the full recompute (all lanes,
-//    same m) reads 32 consecutive words (conflict-free); the pitch shifts row m by m*C
-//    banks, which spreads the k consecutive segments of a rotation over distinct banks (at
-//    most 2-way conflicts).
+//    segments j*SPL .. j*SPL+SPL-1. The chain lives in shared memory as its unit tangents
+//    t_i and segment lengths l_i. Rotating the points between left and right about the
+//    chord x_right - x_left turns every tangent t_left .. t_{right-1} by the same rotation
+//    (the chord is the axis and stays fixed) and leaves the lengths alone; each rotated
+//    tangent is renormalised by one Newton step, so |t_i| = 1 to an ulp and the full
+//    recompute needs no normalisation: kappa_i = |t_{i+1} - t_i| N/S.
+//  * Three planes per warp: (t.x, t.y) as float2, t.z, and l. Segment s = j*SPL + m of the
+//    chain in lanes q*G..q*G+G-1 sits in row m, column q*G + j of each plane; a lane's own
+//    segments are a base register plus immediate offsets, so a tangent is one 8-byte and
+//    one 4-byte LDS (12 bytes, the shared-memory bandwidth the full recompute needs; the
+//    full recompute reads consecutive columns of one row: conflict-free). Row pitches
+//    (32 + 16/SPL float2, 32 + G/SPL floats) shift successive rows by distinct banks so
+//    the k consecutive segments of a rotation fall in distinct banks (at most 2-way
+//    conflicts). The next lane's first tangent comes by shuffle.
+//  * Rotation: the chord is summed across the group (for full-warp groups as 32-bit fixed
+//    point with the warp reduction instruction, scaled by the chain's longest segment so
+//    that 64 segments cannot overflow; otherwise by float shuffles), normalised, and each
+//    tangent in the sub-chain is turned by Rodrigues' formula with the angle's sin and
+//    1 - cos taken from the proposal's half-angle sine and cosine.
 //  * The table is staged once per CTA in shared memory as float2. In the fixed-point form
 //    entry i holds round((log10 L_i - c0) 2^s) as uint32 bits and the change of log10 of
 //    the blend across the bin (secant): a segment costs one 8-byte LDS, one integer add
@@ -142,9 +149,10 @@ __device__ __forceinline__ float bin_of(float qq, const CompConsts &k, uint32_t 
 
 // Walk the curvatures this lane owns: seg(i, qq) for curvature i = base+m-1 (between
 // segments base+m-1 and base+m), the last one with the next lane's first tangent.
-// tan(m, x, y, z) gives the unit tangent of segment j*SPL+m.
-template <int G, int SPL, class TanFn, class SegFn>
-__device__ __forceinline__ void for_curvatures(uint32_t j, uint32_t N, TanFn tan, SegFn seg)
+// tan(m, x, y, z) gives the unit tangent of segment j*SPL+m; next(t0, n) the next lane's
+// first tangent given this lane's (t0). FULLN: N == G*SPL, every lane's own curvatures exist.
+template <int G, int SPL, bool FULLN, class TanFn, class NextFn, class SegFn>
+__device__ __forceinline__ void for_curvatures(uint32_t j, uint32_t N, TanFn tan, NextFn next, SegFn seg)
 {
     float t0x = 0.f, t0y = 0.f, t0z = 0.f, px = 0.f, py = 0.f, pz = 0.f;
     const uint32_t base = j * SPL;
@@ -154,31 +162,42 @@ __device__ __forceinline__ void for_curvatures(uint32_t j, uint32_t N, TanFn tan
         tan(m, tx, ty, tz);
         if (m == 0) {
             t0x = tx; t0y = ty; t0z = tz;
-        } else if (base + m <= N - 1) {
+        } else if (FULLN || base + m <= N - 1) {
             const float dx = tx - px, dy = ty - py, dz = tz - pz;
             seg(base + m - 1, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
         }
         px = tx; py = ty; pz = tz;
     }
-    const float nx = __shfl_down_sync(FULL, t0x, 1, G);
-    const float ny = __shfl_down_sync(FULL, t0y, 1, G);
-    const float nz = __shfl_down_sync(FULL, t0z, 1, G);
+    float nx, ny, nz;
+    next(t0x, t0y, t0z, nx, ny, nz);
     if (base + SPL <= N - 1) {
         const float dx = nx - px, dy = ny - py, dz = nz - pz;
         seg(base + SPL - 1, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
     }
 }
 
+// next() for tangents held in registers: the next lane's t0 by shuffle.
+template <int G>
+struct ShflNext {
+    __device__ __forceinline__ void operator()(float t0x, float t0y, float t0z, float &nx, float &ny, float &nz) const
+    {
+        nx = __shfl_down_sync(FULL, t0x, 1, G);
+        ny = __shfl_down_sync(FULL, t0y, 1, G);
+        nz = __shfl_down_sync(FULL, t0z, 1, G);
+    }
+};
+
 // Generic full recompute of one path's log10 weight (absorption excluded), for the exact
 // table or, with 64-bit lane sums, for the fixed-point table at any lane width. bin_sink(i,
 // bin) receives every curvature's bin (-1 for NaN).
-template <int G, int SPL, bool EXACT, bool CLAMP, class TanFn, class BinFn>
+template <int G, int SPL, bool EXACT, bool CLAMP, class TanFn, class NextFn, class BinFn>
 __device__ __forceinline__ double path_log10(uint32_t j, uint32_t N, const float2 *__restrict__ tab,
-                                             const CompConsts &k, TanFn tan, BinFn bin_sink, uint32_t &clamped)
+                                             const CompConsts &k, TanFn tan, NextFn next, BinFn bin_sink,
+                                             uint32_t &clamped)
 {
     unsigned long long isum = 0;
     float csum = 0.f, ks = 0.f, kc = 0.f;
-    for_curvatures<G, SPL>(j, N, tan, [&](uint32_t i, float qq) {
+    for_curvatures<G, SPL, false>(j, N, tan, next, [&](uint32_t i, float qq) {
         int32_t L;
         const float r = bin_of<CLAMP>(qq, k, clamped, L);
         bin_sink(i, isnan(r) ? -1 : L);
@@ -204,19 +223,24 @@ __device__ __forceinline__ double path_log10(uint32_t j, uint32_t N, const float
 // Fixed-point full recompute for chains: the group's total of table entries plus rounded
 // interpolation corrections, in units of 2^-s (exact: the table was scaled for N). *bad is
 // set when any curvature of the path is NaN.
-template <int G, int SPL, bool CLAMP, class TanFn>
+template <int G, int SPL, bool CLAMP, class TanFn, class NextFn>
 __device__ __forceinline__ uint32_t path_fixed(uint32_t j, uint32_t gbase, uint32_t N, const float2 *__restrict__ tab,
-                                               const CompConsts &k, TanFn tan, bool &bad, uint32_t &clamped)
+                                               const CompConsts &k, TanFn tan, NextFn next, bool &bad,
+                                               uint32_t &clamped)
 {
     uint32_t isum = 0;
     float csum = 0.f;
-    for_curvatures<G, SPL>(j, N, tan, [&](uint32_t, float qq) {
+    auto seg = [&](uint32_t, float qq) {
         int32_t L;
         const float r = bin_of<CLAMP>(qq, k, clamped, L);
         const float2 e = tab[L];
         isum += __float_as_uint(e.x);
         csum = fmaf(r - (float)L, e.y, csum);
-    });
+    };
+    if (N == (uint32_t)(G * SPL))
+        for_curvatures<G, SPL, true>(j, N, tan, next, seg);
+    else
+        for_curvatures<G, SPL, false>(j, N, tan, next, seg);
     const uint32_t nan_lanes = __ballot_sync(FULL, isnan(csum));
     constexpr uint32_t gmask = (G == 32) ? FULL : ((1u << G) - 1u);
     bad = ((nan_lanes >> gbase) & gmask) != 0u;
@@ -226,17 +250,27 @@ __device__ __forceinline__ uint32_t path_fixed(uint32_t j, uint32_t gbase, uint3
 
 template <int G, int SPL>
 struct Layout {
-    static constexpr int C = (G / SPL) > 1 ? (G / SPL) : 1;
-    static constexpr int P = 32 + C;                 // row pitch (floats)
-    static constexpr int PLANE = SPL * P;            // one plane of a warp (floats)
-    static constexpr int WARP = 4 * PLANE;           // tangents x, y, z and lengths
-    __device__ __forceinline__ static uint32_t addr(uint32_t gbase, uint32_t owner, uint32_t m)
-    {
-        return m * (uint32_t)P + gbase + owner;
-    }
+    static constexpr int PXY = 32 + ((16 / SPL) > 1 ? (16 / SPL) : 1);  // float2 plane pitch
+    static constexpr int PZ = 32 + ((G / SPL) > 1 ? (G / SPL) : 1);     // float plane pitch
+    static constexpr int XY_BYTES = SPL * PXY * 8;
+    static constexpr int Z_BYTES = SPL * PZ * 4;
+    static constexpr int WARP_BYTES = XY_BYTES + 2 * Z_BYTES;           // xy, z, l planes
+    __device__ __forceinline__ static uint32_t xy(uint32_t col, uint32_t m) { return m * (uint32_t)PXY + col; }
+    __device__ __forceinline__ static uint32_t z(uint32_t col, uint32_t m) { return m * (uint32_t)PZ + col; }
 };
 
-constexpr int warp_state_floats(int G, int SPL) { return 4 * SPL * (32 + ((G / SPL) > 1 ? (G / SPL) : 1)); }
+constexpr size_t warp_state_bytes(int G, int SPL)
+{
+    return (size_t)SPL * (32 + ((16 / SPL) > 1 ? (16 / SPL) : 1)) * 8 +
+           2 * (size_t)SPL * (32 + ((G / SPL) > 1 ? (G / SPL) : 1)) * 4;
+}
+
+// The planes of one warp's chains.
+struct Planes {
+    float2 *xy;
+    float *z;
+    float *l;
+};
 
 enum { kModeForward = 0, kModeExport = 1, kModeAdjoint = 2 };
 
@@ -295,25 +329,29 @@ __device__ __forceinline__ void stage_table(float4 *smem4, const float2 *__restr
     if ((bins & 1) && threadIdx.x == 0) reinterpret_cast<float2 *>(smem4)[bins - 1] = tab_g[bins - 1];
 }
 
-// One Markov chain run by the G lanes of one group on its own planes st (tangents x, y, z,
-// lengths): initial state from init_seg (segment vectors), burn_in + steps proposals, a full
-// recompute of every weighted path, and the chain's running log-sum-exp. Writes out[chain]
-// (when out is set and the chain is real) and returns the chain's log10 sum.
+// One Markov chain run by the G lanes of one group on its own records st (tangent, length;
+// warp-local slots): initial state from init_seg (segment vectors), burn_in + steps
+// proposals, a full recompute of every weighted path, and the chain's running log-sum-exp.
+// Writes out[chain] (when out is set and the chain is real) and returns the chain's log10 sum.
 template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MODE>
 __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConsts &kc,
-                                             const float *__restrict__ init_seg, const float2 *s_tab, float *st,
+                                             const float *__restrict__ init_seg, const float2 *s_tab, Planes st,
                                              uint32_t gbase, uint32_t j, uint32_t chain, bool real_chain,
                                              ChainOut *__restrict__ out, const ModeArgs &ma)
 {
     constexpr bool FIX = !EXACT && MODE != kModeAdjoint;
     const uint32_t N = c.n_segments;
     using Lay = Layout<G, SPL>;
-    float *sx = st, *sy = st + Lay::PLANE, *sz = st + 2 * Lay::PLANE, *sl = st + 3 * Lay::PLANE;
+    // segment record (tangent, length) of segment index s = owner*SPL + m
+    auto load_rec = [&](uint32_t owner, uint32_t m) {
+        const float2 a = st.xy[Lay::xy(gbase + owner, m)];
+        return make_float4(a.x, a.y, st.z[Lay::z(gbase + owner, m)], st.l[Lay::z(gbase + owner, m)]);
+    };
 
+    float max_len = 0.f;
 #pragma unroll
     for (int m = 0; m < SPL; ++m) {
         const uint32_t s = j * SPL + m;
-        const uint32_t a = Lay::addr(gbase, j, m);
         float x = 0.f, y = 0.f, z = 0.f, len = 1.f;
         if (s < N) {
             x = init_seg[3 * s];
@@ -325,12 +363,16 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
             x *= r; y *= r; z *= r;
             const float h = fmaf(-0.5f, fmaf(x, x, fmaf(y, y, z * z)), 1.5f);   // one Newton step to |t| = 1
             x *= h; y *= h; z *= h;
+            max_len = fmaxf(max_len, len);
         }
-        sx[a] = x;
-        sy[a] = y;
-        sz[a] = z;
-        sl[a] = len;
+        st.xy[Lay::xy(gbase + j, m)] = make_float2(x, y);
+        st.z[Lay::z(gbase + j, m)] = z;
+        st.l[Lay::z(gbase + j, m)] = len;
     }
+#pragma unroll
+    for (int o = 1; o < G; o <<= 1) max_len = fmaxf(max_len, __shfl_xor_sync(FULL, max_len, o));
+    // fixed-point chord scale: a segment is at most 2^24 units, 64 of them at most 2^30
+    const float chord_scale = 16777216.0f / max_len;
     __syncwarp();
 
     const uint32_t steps_c = real_chain ? ((chain == c.n_chains - 1) ? c.last_steps : c.steps) : 0;
@@ -344,14 +386,15 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
     float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 
     const uint32_t own = gbase + j;
+    // tangent of this lane's segment m; with SHIFT the weights see the receiver moved:
+    // v_{N-2} = l t + shift, renormalised
     auto tan_smem = [&](int m, float &x, float &y, float &z) {
-        const uint32_t a = own + (uint32_t)(m * Lay::P);
-        x = sx[a];
-        y = sy[a];
-        z = sz[a];
+        const float2 a = st.xy[Lay::xy(own, m)];
+        x = a.x;
+        y = a.y;
+        z = st.z[Lay::z(own, m)];
         if (SHIFT && j * SPL + m == N - 2) {
-            // weights evaluated with the receiver moved: v_{N-2} = l t + shift, renormalised
-            const float l = sl[a];
+            const float l = st.l[Lay::z(own, m)];
             x = fmaf(l, x, c.eval_shift[0]);
             y = fmaf(l, y, c.eval_shift[1]);
             z = fmaf(l, z, c.eval_shift[2]);
@@ -359,6 +402,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
             x *= r; y *= r; z *= r;
         }
     };
+    const ShflNext<G> next_smem{};
     auto no_bins = [](uint32_t, int32_t) {};
 
     for (uint32_t base = 0; base < total; base += G) {
@@ -375,30 +419,44 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
             // chord x_right - x_left = sum of l_s t_s over the k segments left .. right-1
             constexpr int R = (kMaxSubChain + G - 1) / G;
             float vx[R], vy[R], vz[R];
-            uint32_t va[R];
+            uint32_t va[R], vb[R];
             float cx = 0.f, cy = 0.f, cz = 0.f;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 if (r > 0 && (uint32_t)r >= rounds) break;
                 const uint32_t s = left + j + r * G;
-                va[r] = Lay::addr(gbase, s / SPL, s % SPL);
+                va[r] = Lay::xy(gbase + s / SPL, s % SPL);
+                vb[r] = Lay::z(gbase + s / SPL, s % SPL);
                 if (s < right) {
-                    vx[r] = sx[va[r]];
-                    vy[r] = sy[va[r]];
-                    vz[r] = sz[va[r]];
-                    const float l = sl[va[r]];
+                    const float2 a = st.xy[va[r]];
+                    vx[r] = a.x;
+                    vy[r] = a.y;
+                    vz[r] = st.z[vb[r]];
+                    const float l = st.l[vb[r]];
                     cx = fmaf(l, vx[r], cx);
                     cy = fmaf(l, vy[r], cy);
                     cz = fmaf(l, vz[r], cz);
                 }
             }
-            group_sum3<G>(cx, cy, cz);
+            if constexpr (G == 32) {
+                int ix = __float2int_rn(cx * chord_scale);
+                int iy = __float2int_rn(cy * chord_scale);
+                int iz = __float2int_rn(cz * chord_scale);
+                ix = __reduce_add_sync(FULL, ix);
+                iy = __reduce_add_sync(FULL, iy);
+                iz = __reduce_add_sync(FULL, iz);
+                cx = (float)ix;
+                cy = (float)iy;
+                cz = (float)iz;
+            } else {
+                group_sum3<G>(cx, cy, cz);
+            }
+            // Rodrigues by +theta about the unit chord a -- the rotation the reference's
+            // quaternion sandwich q^-1 p q applies with its product convention:
+            // v cos + (a x v) sin + a (a.v)(1 - cos), sin = 2 s c, 1 - cos = 2 s^2 (half angle s, c)
             const float inv = rsqrtf(fmaf(cx, cx, fmaf(cy, cy, cz * cz)));
-            const float qx = cx * inv * sn, qy = cy * inv * sn, qz = cz * inv * sn, qw = cs;
-            // rotation of q^-1 p q (the reference's quaternion sandwich), as a matrix
-            const float r00 = 1.f - 2.f * (qy * qy + qz * qz), r01 = 2.f * (qx * qy - qw * qz), r02 = 2.f * (qx * qz + qw * qy);
-            const float r10 = 2.f * (qx * qy + qw * qz), r11 = 1.f - 2.f * (qx * qx + qz * qz), r12 = 2.f * (qy * qz - qw * qx);
-            const float r20 = 2.f * (qx * qz - qw * qy), r21 = 2.f * (qy * qz + qw * qx), r22 = 1.f - 2.f * (qx * qx + qy * qy);
+            const float ax = cx * inv, ay = cy * inv, az = cz * inv;
+            const float sth = 2.f * sn * cs, omc = 2.f * sn * sn;
             __syncwarp();
 #pragma unroll
             for (int r = 0; r < R; ++r) {
@@ -406,13 +464,14 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                 const uint32_t s = left + j + r * G;
                 if (s < right) {
                     const float x = vx[r], y = vy[r], z = vz[r];
-                    float nx = fmaf(r00, x, fmaf(r01, y, r02 * z));
-                    float ny = fmaf(r10, x, fmaf(r11, y, r12 * z));
-                    float nz = fmaf(r20, x, fmaf(r21, y, r22 * z));
+                    const float crx = ay * z - az * y, cry = az * x - ax * z, crz = ax * y - ay * x;
+                    const float ad = (ax * x + ay * y + az * z) * omc;
+                    const float nx = fmaf(ax, ad, fmaf(sth, crx, fmaf(-omc, x, x)));
+                    const float ny = fmaf(ay, ad, fmaf(sth, cry, fmaf(-omc, y, y)));
+                    const float nz = fmaf(az, ad, fmaf(sth, crz, fmaf(-omc, z, z)));
                     const float h = fmaf(-0.5f, fmaf(nx, nx, fmaf(ny, ny, nz * nz)), 1.5f);
-                    sx[va[r]] = nx * h;
-                    sy[va[r]] = ny * h;
-                    sz[va[r]] = nz * h;
+                    st.xy[va[r]] = make_float2(nx * h, ny * h);
+                    st.z[vb[r]] = nz * h;
                 }
             }
             __syncwarp();
@@ -423,7 +482,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
 
             if (FIX) {
                 bool bad;
-                const uint32_t tot = path_fixed<G, SPL, CLAMP>(j, gbase, N, s_tab, kc, tan_smem, bad, clamped);
+                const uint32_t tot = path_fixed<G, SPL, CLAMP>(j, gbase, N, s_tab, kc, tan_smem, next_smem, bad, clamped);
                 if (MODE == kModeExport) {
                     const double w = bad ? NAN : kc.lw_offset + (double)tot * kc.inv_scale;
                     // positions below
@@ -439,12 +498,11 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                     double lx[SPL], ly[SPL], lz[SPL];
 #pragma unroll
                     for (int m = 0; m < SPL; ++m) {
-                        const uint32_t a = Lay::addr(gbase, j, m);
-                        const bool in = j * SPL + m < N;
-                        const double l = in ? (double)sl[a] : 0.0;
-                        px += l * (double)sx[a];
-                        py += l * (double)sy[a];
-                        pz += l * (double)sz[a];
+                        const float4 v = load_rec(j, m);
+                        const double l = (j * SPL + m < N) ? (double)v.w : 0.0;
+                        px += l * (double)v.x;
+                        py += l * (double)v.y;
+                        pz += l * (double)v.z;
                         lx[m] = px; ly[m] = py; lz[m] = pz;
                     }
                     double ex = px, ey = py, ez = pz;  // inclusive scan of lane totals
@@ -501,7 +559,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
             if (MODE == kModeAdjoint) {
                 // log10 weight and d/d(mu_s), d/d(eps) of this lane's segments (exact blend)
                 float s = 0.f, cc = 0.f, gmu = 0.f, geps = 0.f;
-                for_curvatures<G, SPL>(j, N, tan_smem, [&](uint32_t, float qq) {
+                for_curvatures<G, SPL, false>(j, N, tan_smem, next_smem, [&](uint32_t, float qq) {
                     float r = fmaf(sqrt_approx(qq), kc.kscale, kc.roff);
                     if (r < 0.f) r = 0.f;
                     if (r > kc.rmax) r = kc.rmax;
@@ -521,14 +579,11 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                 w = (double)hi + (double)lo;
                 float g3[3] = {0.f, 0.f, 0.f};
                 if (j == 0) {
-                    float t3[3], t2[3], t1[3];
-                    const uint32_t a3 = Lay::addr(gbase, (N - 3) / SPL, (N - 3) % SPL);
-                    const uint32_t a2 = Lay::addr(gbase, (N - 2) / SPL, (N - 2) % SPL);
-                    const uint32_t a1 = Lay::addr(gbase, (N - 1) / SPL, (N - 1) % SPL);
-                    t3[0] = sx[a3]; t3[1] = sy[a3]; t3[2] = sz[a3];
-                    t2[0] = sx[a2]; t2[1] = sy[a2]; t2[2] = sz[a2];
-                    t1[0] = sx[a1]; t1[1] = sy[a1]; t1[2] = sz[a1];
-                    receiver_grad(t3, t2, t1, sl[a2], ma.lut, kc, c.inv_ds, g3);
+                    const float4 v3 = load_rec((N - 3) / SPL, (N - 3) % SPL);
+                    const float4 v2 = load_rec((N - 2) / SPL, (N - 2) % SPL);
+                    const float4 v1 = load_rec((N - 1) / SPL, (N - 1) % SPL);
+                    const float t3[3] = {v3.x, v3.y, v3.z}, t2[3] = {v2.x, v2.y, v2.z}, t1[3] = {v1.x, v1.y, v1.z};
+                    receiver_grad(t3, t2, t1, v2.w, ma.lut, kc, c.inv_ds, g3);
                 }
                 if (active && !isnan(w)) {
                     const float wt = exp2f((float)(w - (double)ma.ref_log10) * kLog2_10);
@@ -540,19 +595,18 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                     if (j == 0) acc[5] += wt;
                 }
             } else {
-                w = path_log10<G, SPL, true, CLAMP>(j, N, s_tab, kc, tan_smem, no_bins, clamped);
+                w = path_log10<G, SPL, true, CLAMP>(j, N, s_tab, kc, tan_smem, next_smem, no_bins, clamped);
             }
             if (MODE == kModeExport) {
                 double px = 0.0, py = 0.0, pz = 0.0;
                 double lx[SPL], ly[SPL], lz[SPL];
 #pragma unroll
                 for (int m = 0; m < SPL; ++m) {
-                    const uint32_t a = Lay::addr(gbase, j, m);
-                    const bool in = j * SPL + m < N;
-                    const double l = in ? (double)sl[a] : 0.0;
-                    px += l * (double)sx[a];
-                    py += l * (double)sy[a];
-                    pz += l * (double)sz[a];
+                    const float4 v = load_rec(j, m);
+                    const double l = (j * SPL + m < N) ? (double)v.w : 0.0;
+                    px += l * (double)v.x;
+                    py += l * (double)v.y;
+                    pz += l * (double)v.z;
                     lx[m] = px; ly[m] = py; lz[m] = pz;
                 }
                 double ex = px, ey = py, ez = pz;
@@ -643,9 +697,10 @@ __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompCo
     const int bins = kc.bins;
     const float2 *s_tab = reinterpret_cast<const float2 *>(smem4);
     const int tab_f4 = (bins + 1) / 2;  // float2 entries, padded to float4
-    float *s_state = reinterpret_cast<float *>(smem4 + tab_f4);
+    unsigned char *s_state = reinterpret_cast<unsigned char *>(smem4 + tab_f4);
     const int warps = blockDim.x >> 5;
-    double *s_res = reinterpret_cast<double *>(s_state + warps * Layout<G, SPL>::WARP);
+    using Lay = Layout<G, SPL>;
+    double *s_res = reinterpret_cast<double *>(s_state + (size_t)warps * Lay::WARP_BYTES);
     stage_table(smem4, tab_g, bins);
     __syncthreads();
 
@@ -653,8 +708,11 @@ __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompCo
     const uint32_t q = lane / G, j = lane % G;
     constexpr int CPW = 32 / G;
     const uint32_t chain = (blockIdx.x * warps + warp) * CPW + q;
-    const double cl = chain_body<G, SPL, EXACT, CLAMP, SHIFT, MODE>(
-          c, kc, init_seg, s_tab, s_state + warp * Layout<G, SPL>::WARP, q * G, j, chain, chain < c.n_chains, out, ma);
+    unsigned char *wb = s_state + (size_t)warp * Lay::WARP_BYTES;
+    const Planes pl{reinterpret_cast<float2 *>(wb), reinterpret_cast<float *>(wb + Lay::XY_BYTES),
+                    reinterpret_cast<float *>(wb + Lay::XY_BYTES + Lay::Z_BYTES)};
+    const double cl = chain_body<G, SPL, EXACT, CLAMP, SHIFT, MODE>(c, kc, init_seg, s_tab, pl, q * G, j, chain,
+                                                                    chain < c.n_chains, out, ma);
     if (j == 0) s_res[warp * CPW + q] = cl;
     __syncthreads();
     // Per-CTA log-sum-exp of the chains, rescaled by the block maximum (FP64).
@@ -696,11 +754,14 @@ __global__ void __launch_bounds__(MAXT, 1) batch_kernel(const BatchExp *__restri
     extern __shared__ float4 smem4[];
     __shared__ uint32_t s_item;
     const int tab_f4 = LUT_SMEM ? (bins + 1) / 2 : 0;
-    float *s_state = reinterpret_cast<float *>(smem4 + tab_f4);
+    unsigned char *s_state = reinterpret_cast<unsigned char *>(smem4 + tab_f4);
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t q = lane / G, j = lane % G;
     constexpr int CPW = 32 / G;
-    float *st = s_state + warp * Layout<G, SPL>::WARP;
+    using Lay = Layout<G, SPL>;
+    unsigned char *wb = s_state + (size_t)warp * Lay::WARP_BYTES;
+    const Planes st{reinterpret_cast<float2 *>(wb), reinterpret_cast<float *>(wb + Lay::XY_BYTES),
+                    reinterpret_cast<float *>(wb + Lay::XY_BYTES + Lay::Z_BYTES)};
     for (;;) {
         if (threadIdx.x == 0) s_item = atomicAdd(counter, 1u);
         __syncthreads();
@@ -752,7 +813,7 @@ __global__ void __launch_bounds__(256) weigh_comp_kernel(const float *__restrict
         if (brow) brow[i] = b;
     };
     uint32_t clamped = 0;
-    const double w = path_log10<32, SPL, EXACT, true>(j, N, tab, kc, tan, sink, clamped);
+    const double w = path_log10<32, SPL, EXACT, true>(j, N, tab, kc, tan, ShflNext<32>{}, sink, clamped);
     if (j == 0) {
         const bool ok = !isnan(w);
         log10w[p] = ok ? w + (double)(N - 1) * log10_absorption : 0.0;
@@ -921,7 +982,7 @@ uint32_t comp_default_chains(uint32_t n, int sm_count)
 size_t comp_smem_bytes(const CompTuning &t, uint32_t bins)
 {
     const size_t tab = (size_t)((bins + 1) / 2) * sizeof(float4);
-    const size_t state = (size_t)t.warps_per_block * warp_state_floats(t.group, t.spl) * sizeof(float);
+    const size_t state = (size_t)t.warps_per_block * warp_state_bytes(t.group, t.spl);
     const size_t res = (size_t)t.warps_per_block * (32 / t.group) * sizeof(double);
     return tab + state + res;
 }
@@ -1031,7 +1092,7 @@ bool batch_shape_supported(const BatchShape &s, uint32_t n_max, uint32_t k_eff)
 size_t batch_smem_bytes(const BatchShape &s, uint32_t bins)
 {
     return (s.lut_smem ? (size_t)((bins + 1) / 2) * sizeof(float4) : 0) +
-           (size_t)s.warps * warp_state_floats(s.group, s.spl) * sizeof(float);
+           (size_t)s.warps * warp_state_bytes(s.group, s.spl);
 }
 
 int batch_chains_per_block(const BatchShape &s) { return s.warps * (32 / s.group); }
