@@ -75,6 +75,11 @@ def make_bc(start_pos, start_dir, end_pos, end_dir, arclength) -> _abi.BC:
                    _abi.Vec3(*map(float, end_pos)), _abi.Vec3(*map(float, unit(end_dir))), float(arclength))
 
 
+def make_experiment(bc: _abi.BC, num_segments: int, scatter: float, eps: float, paths: int) -> _abi.Experiment:
+    """One entry of a batch (twisty_experiment): its own geometry, N, mu_s and phase eps."""
+    return _abi.Experiment(bc, int(num_segments), float(scatter), float(eps), int(paths))
+
+
 class Context:
     """One runner context (twisty_create / twisty_destroy)."""
 

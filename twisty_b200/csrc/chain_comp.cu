@@ -936,6 +936,24 @@ cudaError_t batch_t(const BatchShape &s, const BatchExp *exps, const uint2 *item
     return cudaGetLastError();
 }
 
+template <int G, int SPL, bool EXACT, bool LS>
+int batch_occ_t(const BatchShape &s, size_t smem)
+{
+    constexpr int MAXT = (SPL >= 16 || G == 8) ? 512 : 1024;
+    auto kern = batch_kernel<G, SPL, EXACT, LS, MAXT>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, s.warps * 32, smem) != cudaSuccess) return 0;
+    return nb;
+}
+
+template <int G, int SPL>
+int batch_occ_g(const BatchShape &s, size_t smem)
+{
+    if (s.exact) return s.lut_smem ? batch_occ_t<G, SPL, true, true>(s, smem) : batch_occ_t<G, SPL, true, false>(s, smem);
+    return s.lut_smem ? batch_occ_t<G, SPL, false, true>(s, smem) : batch_occ_t<G, SPL, false, false>(s, smem);
+}
+
 template <int G, int SPL>
 cudaError_t batch_g(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items, uint32_t *counter,
                     ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st)
@@ -1096,6 +1114,26 @@ size_t batch_smem_bytes(const BatchShape &s, uint32_t bins)
 }
 
 int batch_chains_per_block(const BatchShape &s) { return s.warps * (32 / s.group); }
+
+int batch_blocks_per_sm(const BatchShape &s, int bins)
+{
+    const size_t smem = batch_smem_bytes(s, (uint32_t)bins);
+#define TWISTY_O(GG, SS) \
+    if (s.group == GG && s.spl == SS) return batch_occ_g<GG, SS>(s, smem);
+    TWISTY_O(8, 2)
+    TWISTY_O(8, 4)
+    TWISTY_O(8, 8)
+    TWISTY_O(8, 16)
+    TWISTY_O(16, 4)
+    TWISTY_O(16, 8)
+    TWISTY_O(16, 16)
+    TWISTY_O(32, 4)
+    TWISTY_O(32, 8)
+    TWISTY_O(32, 16)
+    TWISTY_O(32, 32)
+#undef TWISTY_O
+    return 0;
+}
 
 cudaError_t launch_batch(const BatchShape &s, const void *d_exps, const uint2 *d_items, uint32_t n_items,
                          uint32_t *d_counter, ChainOut *out, int bins, int grid, cudaStream_t st)

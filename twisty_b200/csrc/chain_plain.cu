@@ -227,9 +227,17 @@ __global__ void __launch_bounds__(kPlainThreads) fp64_chain_kernel(ChainSpec c, 
 // of that sum from the spread of the chain sums (chains are independent; their within-
 // chain correlation is absorbed by treating each chain sum as one observation).
 // ------------------------------------------------------------------------------------
+// With ranges set, CTA x reduces the chains ranges[x] = (first, count) into out[x] (one
+// experiment of a batch per CTA).
 __global__ void __launch_bounds__(1024) reduce_kernel(const ChainOut *__restrict__ chains, uint32_t n,
-                                                       ReduceOut *__restrict__ out)
+                                                       ReduceOut *__restrict__ out, const uint2 *__restrict__ ranges)
 {
+    if (ranges) {
+        const uint2 rg = ranges[blockIdx.x];
+        chains += rg.x;
+        n = rg.y;
+        out += blockIdx.x;
+    }
     __shared__ double sd[32], sd2[32], sd3[32];
     __shared__ unsigned long long su[3][32];
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -370,7 +378,15 @@ cudaError_t launch_fp64_chains(const ChainSpec &c, const float *init_pos, double
 
 cudaError_t launch_reduce(const ChainOut *chains, uint32_t n, ReduceOut *out, cudaStream_t st)
 {
-    reduce_kernel<<<1, 1024, 0, st>>>(chains, n, out);
+    reduce_kernel<<<1, 1024, 0, st>>>(chains, n, out, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_segments(const ChainOut *chains, const uint2 *ranges, uint32_t n_segments, ReduceOut *out,
+                                   cudaStream_t st)
+{
+    if (n_segments == 0) return cudaSuccess;
+    reduce_kernel<<<n_segments, 1024, 0, st>>>(chains, 0, out, ranges);
     return cudaGetLastError();
 }
 

@@ -69,6 +69,18 @@ cudaError_t launch_lut_build(const LutBuildSpec &s, double *out64, double *d_mus
 // Non-positive entries replaced by the smallest non-negative one (PathWeightUtils.cpp:
 // 327-344); min/max returned through minmax[2]; float copy written to out32.
 cudaError_t launch_lut_finalize(uint32_t bins, double *lut64, float *out32, double *minmax, cudaStream_t st);
+// Batches of n tables of `bins` entries, table x at offset x*bins: build (specs in device
+// memory, derivatives off), finalize (minmax + 3x), and the compensated-form tables (struct
+// LogFixed below; steps[x] = bin width, nsegs[x] = N of the paths the fixed point is scaled
+// for, ok[x] = 1 when the fixed-point form is usable).
+cudaError_t launch_lut_build_batch(const LutBuildSpec *d_specs, uint32_t n, uint32_t bins, double *out64,
+                                   cudaStream_t st);
+cudaError_t launch_lut_finalize_batch(uint32_t n, uint32_t bins, double *lut64, float *out32, double *minmax,
+                                      cudaStream_t st);
+struct LogFixed;
+cudaError_t launch_comp_tables_batch(uint32_t n, uint32_t bins, const float *lut32, const float *steps,
+                                     const uint32_t *nsegs, float2 *fix, float2 *lin, LogFixed *lf, int *ok,
+                                     cudaStream_t st);
 
 // ------------------------------------------------------------- chains (chain_*.cu)
 cudaError_t launch_plain_chains(const ChainSpec &c, const float *init_pos, float *state,
@@ -146,11 +158,16 @@ void batch_pack_experiments(const BatchExpHost *in, uint32_t n, void *dst);
 bool batch_shape_supported(const BatchShape &s, uint32_t n_max, uint32_t k_eff);
 size_t batch_smem_bytes(const BatchShape &s, uint32_t bins);
 int batch_chains_per_block(const BatchShape &s);
+// Resident CTAs per SM of the shape's kernel (0 when it cannot launch).
+int batch_blocks_per_sm(const BatchShape &s, int bins);
 cudaError_t launch_batch(const BatchShape &s, const void *d_exps, const uint2 *d_items, uint32_t n_items,
                          uint32_t *d_counter, ChainOut *out, int bins, int grid, cudaStream_t st);
 
 // ----------------------------------------------------------- reduction (chain_plain.cu)
 cudaError_t launch_reduce(const ChainOut *chains, uint32_t n, ReduceOut *out, cudaStream_t st);
+// One reduction per range: ranges[x] = (first chain, count) -> out[x].
+cudaError_t launch_reduce_segments(const ChainOut *chains, const uint2 *ranges, uint32_t n_segments, ReduceOut *out,
+                                   cudaStream_t st);
 
 // ------------------------------------------------------------- weighting of given paths
 cudaError_t launch_weigh_plain(const float *pos, uint64_t n_paths, uint32_t n_segments, float inv_ds,

@@ -98,11 +98,10 @@ __device__ double block_sum(double v, double *red)
     return r;  // valid in thread 0
 }
 
-__global__ void __launch_bounds__(kLutThreads) lut_build_kernel(LutBuildSpec s, double *out64,
-                                                                 double *d_mus, double *d_eps)
+// One bin of one table, integrated by the whole CTA.
+__device__ __forceinline__ void build_bin(const LutBuildSpec &s, uint32_t bin, double *out64, double *d_mus,
+                                          double *d_eps, double *red)
 {
-    __shared__ double red[kLutThreads / 32];
-    const uint32_t bin = blockIdx.x;
     const uint32_t n = s.num_steps_int;
     Integrand g;
     g.faithful = s.faithful;
@@ -170,11 +169,31 @@ __global__ void __launch_bounds__(kLutThreads) lut_build_kernel(LutBuildSpec s, 
     }
 }
 
+__global__ void __launch_bounds__(kLutThreads) lut_build_kernel(LutBuildSpec s, double *out64,
+                                                                 double *d_mus, double *d_eps)
+{
+    __shared__ double red[kLutThreads / 32];
+    build_bin(s, blockIdx.x, out64, d_mus, d_eps, red);
+}
+
+// Tables of many experiments: blockIdx.y selects the experiment, its table at out64 + y*bins.
+__global__ void __launch_bounds__(kLutThreads) lut_build_batch_kernel(const LutBuildSpec *__restrict__ specs,
+                                                                       uint32_t bins, double *out64)
+{
+    __shared__ double red[kLutThreads / 32];
+    const LutBuildSpec s = specs[blockIdx.y];
+    build_bin(s, blockIdx.x, out64 + (size_t)blockIdx.y * bins, nullptr, nullptr, red);
+}
+
 // Replace non-positive entries by the smallest non-negative one and emit the float copy
-// (WeightLookupTableIntegral::Initialize, PathWeightUtils.cpp:305-347).
+// (WeightLookupTableIntegral::Initialize, PathWeightUtils.cpp:305-347). One CTA per table:
+// blockIdx.x selects table x of a batch (lut + x*bins, out32 + x*bins, minmax + 3x).
 __global__ void __launch_bounds__(1024) lut_finalize_kernel(uint32_t bins, double *lut, float *out32,
                                                             double *minmax)
 {
+    lut += (size_t)blockIdx.x * bins;
+    if (out32) out32 += (size_t)blockIdx.x * bins;
+    if (minmax) minmax += 3 * (size_t)blockIdx.x;
     __shared__ double smin[32], smax[32];
     __shared__ int sarg[32];
     // The reference keeps entries in float, so min/max selection runs on the float values.
@@ -223,7 +242,113 @@ __global__ void __launch_bounds__(1024) lut_finalize_kernel(uint32_t bins, doubl
     }
 }
 
+// Compensated-form tables of one experiment per CTA, the device twin of the host's
+// compensated_tables (same rules): lin = (L_i, L_{i+1} - L_i); fix = (round((log10 L_i - c0)
+// 2^s) as uint32, log10(1 + step (L_{i+1}/L_i - 1))) with c0 = min log10 L - 64 2^-s and the
+// largest s <= 30 keeping (N+1) (range 2^s + 65) below 2^31. ok[x] = 1 when the fixed form is
+// usable: every entry positive, secant error <= 1e-7 per segment, s >= 22.
+__global__ void __launch_bounds__(1024) comp_tables_kernel(uint32_t bins, const float *__restrict__ lut32,
+                                                           const float *__restrict__ steps,
+                                                           const uint32_t *__restrict__ nsegs, float2 *fix,
+                                                           float2 *lin, LogFixed *lf, int *ok)
+{
+    __shared__ double s_lo[32], s_hi[32], s_err[32];
+    __shared__ int s_bad[32];
+    const uint32_t x = blockIdx.x;
+    const float *L = lut32 + (size_t)x * bins;
+    fix += (size_t)x * bins;
+    lin += (size_t)x * bins;
+    const double st = (double)steps[x];
+    double lo = DBL_MAX, hi = -DBL_MAX, err = 0.0;
+    int bad = 0;
+    for (uint32_t i = threadIdx.x; i < bins; i += blockDim.x) {
+        const float a = L[i], b = L[i + 1 < bins ? i + 1 : i];
+        lin[i] = make_float2(a, b - a);
+        if (!(a > 0.0f) || !isfinite(a)) {
+            bad = 1;
+            continue;
+        }
+        const double lg = log10((double)a);
+        lo = fmin(lo, lg);
+        hi = fmax(hi, lg);
+        if (i + 1 < bins) {
+            const double r = (double)b / (double)a - 1.0;
+            err = fmax(err, (st * r) * (st * r) / (8.0 * 2.302585092994046));
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        err = fmax(err, __shfl_xor_sync(0xffffffffu, err, o));
+        bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    if (l == 0) { s_lo[w] = lo; s_hi[w] = hi; s_err[w] = err; s_bad[w] = bad; }
+    __syncthreads();
+    if (w == 0) {
+        lo = l < nw ? s_lo[l] : DBL_MAX;
+        hi = l < nw ? s_hi[l] : -DBL_MAX;
+        err = l < nw ? s_err[l] : 0.0;
+        bad = l < nw ? s_bad[l] : 0;
+        for (int o = 16; o > 0; o >>= 1) {
+            lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+            err = fmax(err, __shfl_xor_sync(0xffffffffu, err, o));
+            bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+        }
+        if (l == 0) { s_lo[0] = lo; s_hi[0] = hi; s_err[0] = err; s_bad[0] = bad; }
+    }
+    __syncthreads();
+    lo = s_lo[0];
+    hi = s_hi[0];
+    err = s_err[0];
+    bad = s_bad[0];
+    const double cap = floor(2147483647.0 / (double)(nsegs[x] + 1));
+    int s = 30;
+    while (s > 0 && (hi - lo) * ldexp(1.0, s) + 65.0 > cap) --s;
+    const bool usable = !bad && err <= 1e-7 && s >= 22;
+    const double inv_scale = ldexp(1.0, -s);
+    if (threadIdx.x == 0) {
+        lf[x] = usable ? LogFixed{lo - 64.0 * inv_scale, inv_scale} : LogFixed{0.0, 0.0};
+        ok[x] = usable ? 1 : 0;
+    }
+    if (!usable) return;
+    for (uint32_t i = threadIdx.x; i < bins; i += blockDim.x) {
+        const double e = 64.0 + rint((log10((double)L[i]) - lo) * ldexp(1.0, s));
+        const uint32_t u = (uint32_t)fmin(e, cap - 1.0);
+        double delta = 0.0;
+        if (i + 1 < bins) delta = log10(1.0 + st * ((double)L[i + 1] / (double)L[i] - 1.0));
+        fix[i] = make_float2(__uint_as_float(u), (float)delta);
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_lut_build_batch(const LutBuildSpec *d_specs, uint32_t n, uint32_t bins, double *out64,
+                                   cudaStream_t st)
+{
+    if (n == 0) return cudaSuccess;
+    if (bins < 2 || n > 65535u) return cudaErrorInvalidValue;
+    lut_build_batch_kernel<<<dim3(bins, n), kLutThreads, 0, st>>>(d_specs, bins, out64);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lut_finalize_batch(uint32_t n, uint32_t bins, double *lut64, float *out32, double *minmax,
+                                      cudaStream_t st)
+{
+    if (n == 0) return cudaSuccess;
+    lut_finalize_kernel<<<n, 1024, 0, st>>>(bins, lut64, out32, minmax);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_comp_tables_batch(uint32_t n, uint32_t bins, const float *lut32, const float *steps,
+                                     const uint32_t *nsegs, float2 *fix, float2 *lin, LogFixed *lf, int *ok,
+                                     cudaStream_t st)
+{
+    if (n == 0) return cudaSuccess;
+    comp_tables_kernel<<<n, 1024, 0, st>>>(bins, lut32, steps, nsegs, fix, lin, lf, ok);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_lut_build(const LutBuildSpec &s, double *out64, double *d_mus, double *d_eps, cudaStream_t st)
 {

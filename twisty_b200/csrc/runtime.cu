@@ -14,6 +14,7 @@
 #include <cstring>
 #include <filesystem>
 #include <fstream>
+#include <algorithm>
 #include <functional>
 #include <limits>
 #include <new>
@@ -862,12 +863,330 @@ twisty_status twisty_bootstrap_curve(const twisty_params *p, const twisty_bc *bc
 
 float twisty_min_arclength(const twisty_bc *bc, uint32_t n) { return bc ? twisty::min_arclength(*bc, n) : 0.0f; }
 
+namespace {
+
+// Buffers of one batched pass, released however the pass ends.
+struct BatchBufs {
+    DevBuf specs, lut64, lut32, fix, lin, steps, nsegs, lf, ok, init_seg, exps, items, counters, chain_out, ranges, red;
+    ~BatchBufs()
+    {
+        DevBuf *all[] = {&specs, &lut64, &lut32, &fix, &lin, &steps, &nsegs, &lf, &ok, &init_seg, &exps, &items,
+                         &counters, &chain_out, &ranges, &red};
+        for (DevBuf *b : all) b->release();
+    }
+};
+
+// Streams, events and the graph of one batched pass.
+struct BatchGraph {
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> events;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~BatchGraph()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (cudaEvent_t e : events) cudaEventDestroy(e);
+        for (cudaStream_t st : streams) cudaStreamDestroy(st);
+    }
+};
+
+std::string exp_msg(uint32_t e, const std::string &m)
+{
+    std::ostringstream o;
+    o << "experiment " << e << ": " << m;
+    return o.str();
+}
+
+// Many experiments in one pass (the receiver / pixel loops of the reference's drivers, e.g.
+// Experiments/NoisyCircleExperiment.cpp:259-361, each a RunExperiment call there):
+//  1. per experiment on the host: validation, initial curve, normaliser, chain layout;
+//  2. on the device, all tables at once: FP64 quadrature (one CTA per bin per experiment),
+//     finalisation and the compensated-form tables (one CTA per experiment);
+//  3. experiments bucketed by kernel shape (lanes per chain x segments per lane, exact or
+//     fixed-point table); work items = (experiment, first chain of a CTA), sorted by cost
+//     (steps x N) so the longest start first; each bucket is one persistent launch on its
+//     own stream taking items from a device counter, so one bucket's tail overlaps the next;
+//  4. one segmented FP64 reduction (a CTA per experiment).
+// Steps 3-4 are captured once as a CUDA graph and replayed `iters` times; results are those
+// of the last replay, perturb_ms the mean replay time.
+void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_t iters, twisty_result *res)
+{
+    const double t0 = now_ms();
+    const twisty_params p = ctx->p;
+    {
+        twisty_params pv = p;  // num_segments comes from each experiment
+        pv.num_segments = 4;
+        validate(pv);
+    }
+    if (p.form != TWISTY_FORM_COMPENSATED) fail(TWISTY_ERR_UNSUPPORTED, "batched runs use the compensated form");
+    if (p.lut_mode != TWISTY_LUT_FP64)
+        fail(TWISTY_ERR_UNSUPPORTED, "batched runs build their tables on the device (lut_mode FP64)");
+    if (n > 65535u) fail(TWISTY_ERR_INVALID_ARGUMENT, "at most 65535 experiments per batch");
+    set_device(ctx);
+    for (uint32_t e = 0; e < n; ++e) std::memset(&res[e], 0, sizeof(twisty_result));
+    if (n == 0) return;
+    const uint32_t bins = p.num_curvature_steps;
+    cudaStream_t st = ctx->stream;
+
+    struct ExpHost {
+        uint32_t N;
+        float ds;
+        CompTuning t;
+        ChainSpec spec;
+        uint32_t seg_off, chain_off;
+        double log10_norm;
+        LutMetaF meta;
+    };
+    std::vector<ExpHost> eh(n);
+    std::vector<LutBuildSpec> specs(n);
+    std::vector<float> steps(n), segs;
+    std::vector<uint32_t> nsegs(n);
+    uint32_t total_chains = 0;
+    for (uint32_t e = 0; e < n; ++e) {
+        const twisty_experiment &x = ex[e];
+        ExpHost &h = eh[e];
+        const uint32_t N = x.num_segments;
+        if (N < 4 || N > 1024) fail(TWISTY_ERR_INVALID_CONFIG, exp_msg(e, "numSegments must be in [4, 1024]"));
+        try {
+            validate_bc(&x.bc);
+        } catch (const Failure &f) {
+            fail(f.s, exp_msg(e, f.msg));
+        }
+        if (!(x.eps > 0.0f)) fail(TWISTY_ERR_INVALID_CONFIG, exp_msg(e, "eps must be positive"));
+        if (!(x.scatter >= 0.0f)) fail(TWISTY_ERR_INVALID_CONFIG, exp_msg(e, "scatter must be non-negative"));
+        h.N = N;
+        h.ds = x.bc.arclength / (float)N;
+        // the table of WeightLookupTableIntegral for this ds (PathWeightUtils.cpp:281-289),
+        // maxBound = 10/eps per experiment (ExperimentRunner.cpp:169-171)
+        const float max_k = (float)((2.0 / (double)h.ds) * (double)1.01f);
+        h.meta = LutMetaF{0.0f, max_k, max_k / (float)(bins - 1), (int32_t)bins};
+        LutBuildSpec &ls = specs[e];
+        ls = LutBuildSpec{};
+        ls.mu = p.mu;
+        ls.eps = x.eps;
+        ls.scatter = x.scatter;
+        ls.min_bound = p.min_bound;
+        ls.max_bound = 10.0f / x.eps;
+        ls.bias = p.bias;
+        ls.num_steps_int = p.num_steps_int;
+        ls.bins = bins;
+        ls.ds = h.ds;
+        ls.min_k = 0.0f;
+        ls.step = h.meta.step;
+        ls.step64 = ((2.0 / (double)h.ds) * 1.01) / (double)(bins - 1);
+        steps[e] = h.meta.step;
+        nsegs[e] = N;
+        // initial curve
+        std::vector<float> pos;
+        std::string err;
+        if (!bootstrap_arc(x.bc, N, p.bootstrap_seed + e, pos, err)) fail(TWISTY_ERR_INFEASIBLE_GEOMETRY, exp_msg(e, err));
+        h.seg_off = (uint32_t)segs.size();
+        for (uint32_t i = 0; i < N; ++i)
+            for (int k = 0; k < 3; ++k) segs.push_back(pos[3 * (i + 1) + k] - pos[3 * i + k]);
+        h.log10_norm = normalizer_log10(ctx, N, h.ds, x.bc);
+        // kernel shape and chain layout: whole CTAs of chains, ~2048 steps per chain
+        h.t = comp_default_tuning(N);
+        ChainSpec &c = h.spec;
+        c = ChainSpec{};
+        c.n_segments = N;
+        c.arclength = x.bc.arclength;
+        c.ds = h.ds;
+        c.inv_ds = (float)N / x.bc.arclength;
+        c.seed = seed_of(p.perturb_seed);
+        c.experiment = p.experiment_id + e;
+        c.chain0 = p.chain_offset;
+        c.burn_in = (uint32_t)std::min<uint64_t>(p.paths_to_skip, 0xFFFFFFFFull);
+        c.k_eff = std::min<uint32_t>(p.max_sub_chain, N - 2);
+        c.max_angle = p.max_angle;
+        c.absorption_factor = (double)std::exp(-p.absorption * h.ds);
+        if (!comp_tuning_supported(h.t, N, c.k_eff))
+            fail(TWISTY_ERR_UNSUPPORTED, exp_msg(e, "no compensated kernel shape for this N / max_sub_chain"));
+        const int maxt = (h.t.spl >= 16 || h.t.group == 8) ? 512 : 1024;
+        h.t.warps_per_block = std::min(h.t.warps_per_block, maxt / 32);
+        const uint64_t cpb = (uint64_t)h.t.warps_per_block * (32u / (uint32_t)h.t.group);
+        uint64_t chains = p.num_chains;
+        if (!chains) chains = cpb * std::max<uint64_t>(1, (x.paths + cpb * 1024) / (cpb * 2048));
+        if (x.paths == 0) {
+            c.n_chains = 0;
+        } else {
+            chains = std::min<uint64_t>(chains, x.paths);
+            const uint64_t L = (x.paths + chains - 1) / chains;
+            if (L > 0xFFFFFFFFull - c.burn_in) fail(TWISTY_ERR_INVALID_CONFIG, exp_msg(e, "too many paths per chain"));
+            chains = (x.paths + L - 1) / L;
+            c.n_chains = (uint32_t)chains;
+            c.steps = (uint32_t)L;
+            c.last_steps = (uint32_t)(x.paths - (chains - 1) * L);
+        }
+        h.chain_off = total_chains;
+        if ((uint64_t)total_chains + c.n_chains > 0xFFFFFFFFull) fail(TWISTY_ERR_INVALID_CONFIG, "too many chains in the batch");
+        total_chains += c.n_chains;
+    }
+
+    BatchBufs B;
+    // ---- tables, all experiments at once
+    ck(B.specs.ensure(sizeof(LutBuildSpec) * n), "alloc batch");
+    ck(B.lut64.ensure(sizeof(double) * (size_t)bins * n), "alloc batch tables");
+    ck(B.lut32.ensure(sizeof(float) * (size_t)bins * n), "alloc batch tables");
+    ck(B.fix.ensure(sizeof(float2) * (size_t)bins * n), "alloc batch tables");
+    ck(B.lin.ensure(sizeof(float2) * (size_t)bins * n), "alloc batch tables");
+    ck(B.steps.ensure(sizeof(float) * n), "alloc batch");
+    ck(B.nsegs.ensure(sizeof(uint32_t) * n), "alloc batch");
+    ck(B.lf.ensure(sizeof(LogFixed) * n), "alloc batch");
+    ck(B.ok.ensure(sizeof(int) * n), "alloc batch");
+    ck(cudaMemcpyAsync(B.specs.p, specs.data(), sizeof(LutBuildSpec) * n, cudaMemcpyHostToDevice, st), "upload specs");
+    ck(cudaMemcpyAsync(B.steps.p, steps.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st), "upload");
+    ck(cudaMemcpyAsync(B.nsegs.p, nsegs.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, st), "upload");
+    ck(launch_lut_build_batch(B.specs.as<LutBuildSpec>(), n, bins, B.lut64.as<double>(), st), "batch table build");
+    ck(launch_lut_finalize_batch(n, bins, B.lut64.as<double>(), B.lut32.as<float>(), nullptr, st), "batch table finalize");
+    ck(launch_comp_tables_batch(n, bins, B.lut32.as<float>(), B.steps.as<float>(), B.nsegs.as<uint32_t>(),
+                                B.fix.as<float2>(), B.lin.as<float2>(), B.lf.as<LogFixed>(), B.ok.as<int>(), st),
+       "batch compensated tables");
+    std::vector<LogFixed> lf(n);
+    std::vector<int> okv(n);
+    ck(cudaMemcpyAsync(lf.data(), B.lf.p, sizeof(LogFixed) * n, cudaMemcpyDeviceToHost, st), "read tables");
+    ck(cudaMemcpyAsync(okv.data(), B.ok.p, sizeof(int) * n, cudaMemcpyDeviceToHost, st), "read tables");
+    ck(B.init_seg.ensure(sizeof(float) * segs.size()), "alloc batch curves");
+    ck(cudaMemcpyAsync(B.init_seg.p, segs.data(), sizeof(float) * segs.size(), cudaMemcpyHostToDevice, st), "upload curves");
+    ck(cudaStreamSynchronize(st), "batch tables");
+
+    // ---- experiments packed for the device, buckets by shape and table form
+    std::vector<BatchExpHost> bh(n);
+    struct Bucket {
+        BatchShape shape;
+        std::vector<uint32_t> exps;
+        std::vector<uint2> items;
+        int grid = 0;
+        uint32_t item_off = 0;
+    };
+    std::vector<Bucket> buckets;
+    auto bucket_of = [&](const BatchShape &sh) -> Bucket & {
+        for (Bucket &b : buckets)
+            if (b.shape.group == sh.group && b.shape.spl == sh.spl && b.shape.warps == sh.warps && b.shape.exact == sh.exact)
+                return b;
+        buckets.push_back(Bucket{});
+        buckets.back().shape = sh;
+        return buckets.back();
+    };
+    for (uint32_t e = 0; e < n; ++e) {
+        ExpHost &h = eh[e];
+        const bool exact = okv[e] == 0;
+        BatchExpHost &b = bh[e];
+        b.spec = h.spec;
+        b.meta = h.meta;
+        b.lf = exact ? LogFixed{0.0, 0.0} : lf[e];
+        b.tab = (exact ? B.lin.as<float2>() : B.fix.as<float2>()) + (size_t)e * bins;
+        b.init_seg = B.init_seg.as<float>() + h.seg_off;
+        b.out_offset = h.chain_off;
+        BatchShape sh{h.t.group, h.t.spl, h.t.warps_per_block, exact ? 1 : 0, 1};
+        if (batch_smem_bytes(sh, bins) > 227 * 1024) sh.lut_smem = 0;
+        if (!batch_shape_supported(sh, h.N, h.spec.k_eff) || batch_smem_bytes(sh, bins) > 227 * 1024)
+            fail(TWISTY_ERR_UNSUPPORTED, exp_msg(e, "no batched kernel shape fits"));
+        Bucket &bk = bucket_of(sh);
+        bk.exps.push_back(e);
+        const uint32_t cpb = (uint32_t)batch_chains_per_block(sh);
+        for (uint32_t c0 = 0; c0 < h.spec.n_chains; c0 += cpb) bk.items.push_back(make_uint2(e, c0));
+    }
+    std::vector<uint2> items;
+    for (Bucket &bk : buckets) {
+        // longest work first: cost of an item ~ (burn-in + steps) x N
+        std::stable_sort(bk.items.begin(), bk.items.end(), [&](const uint2 &a, const uint2 &b) {
+            const ExpHost &x = eh[a.x], &y = eh[b.x];
+            return (double)(x.spec.burn_in + x.spec.steps) * x.N > (double)(y.spec.burn_in + y.spec.steps) * y.N;
+        });
+        bk.item_off = (uint32_t)items.size();
+        items.insert(items.end(), bk.items.begin(), bk.items.end());
+        const int occ = batch_blocks_per_sm(bk.shape, (int)bins);
+        if (occ <= 0) fail(TWISTY_ERR_UNSUPPORTED, "batched kernel shape cannot launch");
+        bk.grid = (int)std::min<uint64_t>((uint64_t)ctx->sm_count * occ, std::max<size_t>(1, bk.items.size()));
+    }
+    std::vector<unsigned char> packed(batch_exp_bytes() * n);
+    batch_pack_experiments(bh.data(), n, packed.data());
+    std::vector<uint2> ranges(n);
+    for (uint32_t e = 0; e < n; ++e) ranges[e] = make_uint2(eh[e].chain_off, eh[e].spec.n_chains);
+    ck(B.exps.ensure(packed.size()), "alloc batch");
+    ck(B.items.ensure(sizeof(uint2) * std::max<size_t>(1, items.size())), "alloc batch");
+    ck(B.counters.ensure(sizeof(uint32_t) * buckets.size()), "alloc batch");
+    ck(B.chain_out.ensure(sizeof(ChainOut) * std::max<uint32_t>(1, total_chains)), "alloc batch results");
+    ck(B.ranges.ensure(sizeof(uint2) * n), "alloc batch");
+    ck(B.red.ensure(sizeof(ReduceOut) * n), "alloc batch results");
+    ck(cudaMemcpyAsync(B.exps.p, packed.data(), packed.size(), cudaMemcpyHostToDevice, st), "upload batch");
+    if (!items.empty())
+        ck(cudaMemcpyAsync(B.items.p, items.data(), sizeof(uint2) * items.size(), cudaMemcpyHostToDevice, st), "upload batch");
+    ck(cudaMemcpyAsync(B.ranges.p, ranges.data(), sizeof(uint2) * n, cudaMemcpyHostToDevice, st), "upload batch");
+    ck(cudaStreamSynchronize(st), "batch upload");
+
+    // ---- the pass as a graph: counters reset, one launch per bucket on forked streams, reduction
+    BatchGraph G;
+    G.streams.resize(buckets.size(), nullptr);
+    G.events.resize(buckets.size() + 3, nullptr);
+    for (auto &x : G.streams) ck(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking), "stream");
+    for (auto &x : G.events) ck(cudaEventCreateWithFlags(&x, cudaEventDisableTiming), "event");
+    cudaEvent_t fork = G.events[buckets.size()];
+    ck(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed), "capture");
+    {
+        cudaError_t ce = cudaMemsetAsync(B.counters.p, 0, sizeof(uint32_t) * buckets.size(), st);
+        if (ce == cudaSuccess) ce = cudaEventRecord(fork, st);
+        for (size_t b = 0; b < buckets.size() && ce == cudaSuccess; ++b) {
+            const Bucket &bk = buckets[b];
+            ce = cudaStreamWaitEvent(G.streams[b], fork, 0);
+            if (ce == cudaSuccess)
+                ce = launch_batch(bk.shape, B.exps.p, B.items.as<uint2>() + bk.item_off, (uint32_t)bk.items.size(),
+                                  B.counters.as<uint32_t>() + b, B.chain_out.as<ChainOut>(), (int)bins, bk.grid,
+                                  G.streams[b]);
+            if (ce == cudaSuccess) ce = cudaEventRecord(G.events[b], G.streams[b]);
+            if (ce == cudaSuccess) ce = cudaStreamWaitEvent(st, G.events[b], 0);
+        }
+        if (ce == cudaSuccess) ce = launch_reduce_segments(B.chain_out.as<ChainOut>(), B.ranges.as<uint2>(), n,
+                                                           B.red.as<ReduceOut>(), st);
+        const cudaError_t ee = cudaStreamEndCapture(st, &G.graph);
+        ck(ce, "batched pass capture");
+        ck(ee, "end capture");
+    }
+    ck(cudaGraphInstantiate(&G.exec, G.graph, 0), "graph instantiate");
+    const double setup_ms = now_ms() - t0;
+
+    // ---- replays, each timed on the stream
+    double sum_ms = 0.0;
+    for (uint32_t it = 0; it < iters; ++it) {
+        ck(cudaEventRecord(ctx->ev[0], st), "event");
+        ck(cudaGraphLaunch(G.exec, st), "graph launch");
+        ck(cudaEventRecord(ctx->ev[1], st), "event");
+        ck(cudaEventSynchronize(ctx->ev[1]), "batched pass");
+        float ms = 0.f;
+        ck(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]), "event time");
+        sum_ms += ms;
+    }
+    std::vector<ReduceOut> red(n);
+    ck(cudaMemcpyAsync(red.data(), B.red.p, sizeof(ReduceOut) * n, cudaMemcpyDeviceToHost, st), "read batch results");
+    ck(cudaStreamSynchronize(st), "read batch results");
+    const double total_ms = now_ms() - t0;
+    for (uint32_t e = 0; e < n; ++e) {
+        twisty_result &r = res[e];
+        const ReduceOut &o = red[e];
+        r.log10_normalizer = eh[e].log10_norm;
+        r.log10_weight = o.log10_sum + eh[e].log10_norm;
+        r.total_paths = o.valid;
+        r.failed_paths = o.failed;
+        r.clamped_curvatures = o.clamped;
+        r.log10_mean_weight = o.valid ? r.log10_weight - std::log10((double)o.valid) : -std::numeric_limits<double>::infinity();
+        r.rel_std_error = o.rel_se;
+        r.num_chains = eh[e].spec.n_chains;
+        r.steps_per_chain = eh[e].spec.steps;
+        r.setup_ms = setup_ms;
+        r.perturb_ms = sum_ms / iters;
+        r.weighting_ms = 0.0;
+        r.total_ms = total_ms;
+    }
+}
+
+}  // namespace
+
 twisty_status twisty_run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_t iterations,
                                twisty_result *res)
 {
     if (!ctx || (!ex && n) || (!res && n)) return TWISTY_ERR_INVALID_ARGUMENT;
-    (void)iterations;
-    return guard(ctx, [&] { fail(TWISTY_ERR_UNSUPPORTED, "batched runs are not built yet"); });
+    return guard(ctx, [&] { run_batch(ctx, ex, n, iterations ? iterations : 1, res); });
 }
 
 twisty_status twisty_export_paths(twisty_ctx *ctx, const twisty_bc *bc, const char *dir, uint64_t max_paths, float *pos,
