@@ -33,6 +33,8 @@ import tempfile
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -114,6 +116,52 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
                 "samples": len(sm)}
+
+
+# Batching workload: 4096 experiments, N log-uniform in [16, 1024], receivers uniform on spheres
+# of radius U(2, 10) around the source at the origin (source tangent (0,0,1)), receiver tangents
+# uniform on the sphere, S = r U(1.05, 2.0) (redrawn while S is below the minimum arclength),
+# sigma ~ U(0.05, 0.3) (eps = sigma^2), mu_s ~ U(5, 50), a 4096-bin table per experiment, 2^16
+# paths each; generator seed 1234.
+BATCH = dict(n=4096, paths=1 << 16, bins=4096, num_steps_int=2000, mu=1.0, k_max=32, max_angle=0.05,
+             burn_in=64, seed=1234)
+BATCH_NAME = ("batching: 4096 experiments, N log-uniform [16,1024], receivers on spheres r~U(2,10), S=r*U(1.05,2), "
+              "sigma~U(0.05,0.3), mu_s~U(5,50), 4096-bin table each, 2^16 paths each, k~U{2..32}, "
+              "angle~U(-0.05,0.05), Philox seed 1234")
+# DRAM bytes of one comp_chain_kernel launch (ncu dram__bytes_read.sum + dram__bytes_write.sum
+# on the precision workload at 2^20 paths; the traffic is per chain, not per path: the table
+# and initial curve are read once per CTA and one record is written per chain, so a launch of
+# the full workload, with the same chains, moves the same bytes)
+TRAFFIC_PER_LAUNCH = 93184
+
+
+def batch_experiments(T, n=None, seed=None):
+    n = BATCH["n"] if n is None else n
+    rng = np.random.default_rng(BATCH["seed"] if seed is None else seed)
+    out = []
+    while len(out) < n:
+        N = int(round(math.exp(rng.uniform(math.log(16), math.log(1024)))))
+        r = rng.uniform(2.0, 10.0)
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        t = rng.normal(size=3)
+        t /= np.linalg.norm(t)
+        S = r * rng.uniform(1.05, 2.0)
+        sigma = rng.uniform(0.05, 0.3)
+        mus = rng.uniform(5.0, 50.0)
+        bc = T.make_bc((0.0, 0.0, 0.0), (0.0, 0.0, 1.0), r * d, t, S)
+        if T.min_arclength(bc, N) >= S:
+            continue
+        out.append(T.make_experiment(bc, N, mus, sigma * sigma, BATCH["paths"]))
+    return out
+
+
+def batch_params(T, device=0):
+    return T.default_params(num_segments=16, mu=BATCH["mu"], eps=0.01, scatter=10.0, absorption=0.0,
+                            num_steps_int=BATCH["num_steps_int"], num_curvature_steps=BATCH["bins"],
+                            paths_to_skip=BATCH["burn_in"], perturb_seed=BATCH["seed"], bootstrap_seed=7,
+                            max_sub_chain=BATCH["k_max"], max_angle=BATCH["max_angle"], form=T.FORM_COMPENSATED,
+                            lut_mode=T.LUT_FP64, device=device)
 
 
 def workload_params(T, form, num_chains=0, chain_offset=0, device=0):
@@ -223,6 +271,61 @@ def run_reference_arm(args):
     return 0
 
 
+def run_batch_workload(args, T, torch, device, ws, rank, pg):
+    """The batching workload through twisty_run_batch: every rank runs all experiments on its own
+    chain range (chain_offset), and the per-experiment results combine across ranks."""
+    exps = batch_experiments(T)
+    segs = sum(x.paths * x.num_segments for x in exps)
+    params = batch_params(T, device=device)
+    with T.Context(params) as probe:   # the chain layout every rank uses
+        chains = probe.run_batch(exps[:1])[0].num_chains
+    params.chain_offset = rank * 1_000_000
+    ctx = T.Context(params)
+    ctx.run_batch(exps, iterations=max(1, args.warmup))
+    with ClockSampler(device) as clk:
+        res = ctx.run_batch(exps, iterations=args.steps)
+    launches = ctx.kernels_per_launch()
+    per_step = res[0].perturb_ms
+    setup_ms = res[0].setup_ms
+    if pg:
+        pg.barrier()
+    t0 = time.perf_counter()
+    e2e = ctx.run_batch(exps, iterations=1)
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+    if pg:
+        t = torch.tensor([per_step, e2e_ms], dtype=torch.float64, device=f"cuda:{device}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        per_step, e2e_ms = t.tolist()
+    ctx.close()
+    done = sum(r.total_paths * x.num_segments for r, x in zip(res, exps))
+    value = done * ws / (per_step / 1e3)
+    peaks = load_peaks()
+    sm_max = peaks.get("sm_max_mhz", 1965.0)
+    peak_ti = SMS * LANES_PER_SM * sm_max * 1e6 / 1e12
+    achieved_ti = INSTR_PER_SEGMENT * done / (per_step / 1e3) / 1e12
+    if rank == 0:
+        import ctypes
+        h2d = ctypes.sizeof(T._abi.Experiment) * len(exps)   # the experiment array; tables are built on the device
+        d2h = ctypes.sizeof(T._abi.Result) * len(exps)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": per_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32 (f64 cross-chain)", "data": "synthetic",
+                "config": {"workload": BATCH_NAME, "form": "compensated", "experiments": len(exps),
+                           "path_segments_per_step": segs, "chains_first_experiment": chains,
+                           "l2": "inputs larger than L2 (4096 tables of 4096 bins, 134 MB fixed-point + 134 MB linear)",
+                           "parallelism": f"independent chains x{ws}"},
+                "e2e": {"value": done * ws / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms,
+                        "setup_ms": setup_ms, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "roofline": {"bound": "fp32", "kernel": "batch_kernel", "achieved": achieved_ti, "peak": peak_ti,
+                             "unit": "Tinstr/s", "frac": achieved_ti / peak_ti, "traffic": None,
+                             "basis": f"{INSTR_PER_SEGMENT:g} FP32 instructions per path-segment"},
+                "cpu_baseline": None, "clocks": clk.summary(), "gpu_launches": launches * args.steps}
+        print(json.dumps(line))
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -234,7 +337,12 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP32 drop-in")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--paths", type=int, default=0, help="paths per pass (default 2^26; smaller for profiling)")
+    ap.add_argument("--workload", default="precision", choices=["precision", "batch"],
+                    help="precision: one N=256 experiment (the headline); batch: 4096 uneven experiments")
+    ap.add_argument("--experiments", type=int, default=0, help="batch workload: number of experiments (default 4096)")
     args = ap.parse_args()
+    if args.experiments:
+        BATCH["n"] = args.experiments
     if args.paths:
         W["paths"] = args.paths
     if args.impl == "reference":
@@ -252,6 +360,8 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device(f"cuda:{device}"))
         pg = dist
+    if args.workload == "batch":
+        return run_batch_workload(args, T, torch, device, ws, rank, pg)
     form = {"compensated": T.FORM_COMPENSATED, "plain": T.FORM_PLAIN_FP32, "fp64": T.FORM_FP64}[args.form]
     bc = workload_bc(T)
 
@@ -324,8 +434,10 @@ def main():
     achieved_ti = INSTR_PER_SEGMENT * segs / (kernel_ms / 1e3) / 1e12
     roofline = {"bound": "fp32", "kernel": "comp_chain_kernel" if form == T.FORM_COMPENSATED else args.form,
                 "achieved": achieved_ti, "peak": peak_ti, "unit": "Tinstr/s", "frac": achieved_ti / peak_ti,
-                "traffic": None, "basis": f"{INSTR_PER_SEGMENT:g} FP32 instructions per path-segment; peak = "
-                f"{SMS} SMs x {LANES_PER_SM} lanes x {sm_max:g} MHz (max SM clock of MEASURED_PEAKS.json)",
+                "traffic": TRAFFIC_PER_LAUNCH if form == T.FORM_COMPENSATED else None,
+                "basis": f"{INSTR_PER_SEGMENT:g} FP32 instructions per path-segment; peak = "
+                f"{SMS} SMs x {LANES_PER_SM} lanes x {sm_max:g} MHz (max SM clock of MEASURED_PEAKS.json); "
+                "traffic = DRAM bytes per launch from ncu (per chain, not per path)",
                 "segments_per_s_kernel_only": segs / (kernel_ms / 1e3)}
 
     cpu = None

@@ -1145,6 +1145,7 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
     }
     ck(cudaGraphInstantiate(&G.exec, G.graph, 0), "graph instantiate");
     const double setup_ms = now_ms() - t0;
+    ctx->kernels_per_launch = (uint32_t)buckets.size() + 1;   // one persistent launch per bucket + the reduction
 
     // ---- replays, each timed on the stream
     double sum_ms = 0.0;
