@@ -147,6 +147,25 @@ def test_compensated_within_1e4_of_fp64(name):
     assert rel < 1e-4, rel
 
 
+@pytest.mark.parametrize("N", [300, 700, 1024])
+def test_long_paths_compensated_within_1e4_of_fp64(N):
+    """Long paths: N = 300 keeps 32-bit fixed-point path totals, 700 and 1024 need the wide
+    (64-bit total) form; both agree with the FP64 form on the same proposals."""
+    res = {}
+    for form in (T.FORM_COMPENSATED, T.FORM_FP64):
+        p = T.default_params(num_segments=N, mu=1.0, eps=0.01, scatter=10.0, num_steps_int=2000,
+                             num_curvature_steps=4096, form=form, perturb_seed=5, num_chains=1024,
+                             paths_to_generate=1024 * 200, paths_to_skip=50, max_sub_chain=32, max_angle=0.05,
+                             lut_mode=T.LUT_FP64)
+        with T.Context(p) as ctx:
+            res[form] = ctx.run(T.make_bc((0, 0, 0), (0, 0, 1), (0, 0, 12), (0, 0, 1), 20.0))
+    a, b = res[T.FORM_COMPENSATED], res[T.FORM_FP64]
+    assert a.total_paths == b.total_paths == 1024 * 200
+    assert a.failed_paths == 0
+    rel = abs(10 ** (a.log10_weight - b.log10_weight) - 1)
+    assert rel < 1e-4, rel
+
+
 @pytest.mark.parametrize("N", [10, 18, 66])
 @pytest.mark.parametrize("form", [T.FORM_COMPENSATED, T.FORM_PLAIN_FP32])
 def test_statistics_match_reference_runner(N, form):

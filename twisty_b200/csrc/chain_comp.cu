@@ -66,6 +66,7 @@ struct CompConsts {
     int32_t bins;
     float fscale;        // 2^s of the fixed-point table
     float l2s;           // 2^-s log2(10): fixed-point units -> log2
+    int32_t wide;        // 64-bit path totals (the table's LogFixed.wide)
     double lw_offset;    // (N-1) c0 of the fixed-point table
     double inv_scale;    // 2^-s of the fixed-point table
 };
@@ -221,10 +222,12 @@ __device__ __forceinline__ double path_log10(uint32_t j, uint32_t N, const float
 }
 
 // Fixed-point full recompute for chains: the group's total of table entries plus rounded
-// interpolation corrections, in units of 2^-s (exact: the table was scaled for N). *bad is
-// set when any curvature of the path is NaN.
+// interpolation corrections, in units of 2^-s. Each lane's sum is exact in 32 bits (its true
+// value lies in [0, 2^32) by the table's scale); the group total is added in 32 bits for a
+// narrow table, in 64 bits for a wide one (both exact). *bad is set when any curvature of
+// the path is NaN.
 template <int G, int SPL, bool CLAMP, class TanFn, class NextFn>
-__device__ __forceinline__ uint32_t path_fixed(uint32_t j, uint32_t gbase, uint32_t N, const float2 *__restrict__ tab,
+__device__ __forceinline__ unsigned long long path_fixed(uint32_t j, uint32_t gbase, uint32_t N, const float2 *__restrict__ tab,
                                                const CompConsts &k, TanFn tan, NextFn next, bool &bad,
                                                uint32_t &clamped)
 {
@@ -245,7 +248,8 @@ __device__ __forceinline__ uint32_t path_fixed(uint32_t j, uint32_t gbase, uint3
     constexpr uint32_t gmask = (G == 32) ? FULL : ((1u << G) - 1u);
     bad = ((nan_lanes >> gbase) & gmask) != 0u;
     isum += (uint32_t)__float2int_rn(csum * k.fscale);
-    return group_sum<G>(isum);
+    if (k.wide) return group_sum<G>((unsigned long long)isum);
+    return (unsigned long long)group_sum<G>(isum);
 }
 
 template <int G, int SPL>
@@ -381,7 +385,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
     // rotation rounds actually needed: sub-chains have at most k_eff segments
     const uint32_t rounds = (c.k_eff + G - 1) / G;
     float lse_m = 0.f, lse_s = 0.f, lse_c = 0.f;  // exact form: running max (float) and Kahan sum
-    uint32_t lse_t = 0;                             // fixed form: running max as a path total
+    unsigned long long lse_t = 0;                   // fixed form: running max as a path total
     uint32_t valid = 0, failed = 0, clamped = 0;
     float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 
@@ -482,7 +486,8 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
 
             if (FIX) {
                 bool bad;
-                const uint32_t tot = path_fixed<G, SPL, CLAMP>(j, gbase, N, s_tab, kc, tan_smem, next_smem, bad, clamped);
+                const unsigned long long tot =
+                      path_fixed<G, SPL, CLAMP>(j, gbase, N, s_tab, kc, tan_smem, next_smem, bad, clamped);
                 if (MODE == kModeExport) {
                     const double w = bad ? NAN : kc.lw_offset + (double)tot * kc.inv_scale;
                     // positions below
@@ -538,8 +543,10 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                     lse_s = 1.f;
                     lse_c = 0.f;
                 } else {
-                    // exact integer difference: totals stay below 2^31
-                    const float x = (float)(int32_t)(tot - lse_t) * kc.l2s;
+                    // exact integer difference: narrow totals stay below 2^31, wide ones are 64-bit
+                    const float dt = kc.wide ? (float)(long long)(tot - lse_t)
+                                             : (float)(int32_t)((uint32_t)tot - (uint32_t)lse_t);
+                    const float x = dt * kc.l2s;
                     float term = 1.f;
                     if (x > 0.f) {
                         const float f = ex2_approx(-x);
@@ -865,6 +872,7 @@ CompConsts make_consts(float inv_ds, const LutMetaF &m, uint32_t n_segments, con
     k.inv_scale = lf.inv_scale;
     k.fscale = lf.inv_scale > 0.0 ? (float)(1.0 / lf.inv_scale) : 0.0f;
     k.l2s = (float)(lf.inv_scale * 3.321928094887362);
+    k.wide = lf.wide;
     return k;
 }
 

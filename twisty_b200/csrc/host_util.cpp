@@ -615,8 +615,9 @@ double norm_k4_log10(float z, float ds)
 }
 
 bool compensated_tables(const float *lut, uint32_t bins, float step, uint32_t n_segments, std::vector<float> &lin,
-                        std::vector<float> &fix, double &c0, double &inv_scale, double &secant_err)
+                        std::vector<float> &fix, double &c0, double &inv_scale, int &wide, double &secant_err)
 {
+    wide = 0;
     lin.assign(2 * (size_t)bins, 0.0f);
     fix.assign(2 * (size_t)bins, 0.0f);
     c0 = 0.0;
@@ -646,12 +647,22 @@ bool compensated_tables(const float *lut, uint32_t bins, float step, uint32_t n_
         secant_err = INFINITY;
         return false;
     }
-    // largest s (at most 30) with range * 2^s + 65 <= (2^31 - 1) / (n_segments + 1)
-    const double cap = std::floor(2147483647.0 / (double)(n_segments + 1));
+    // largest s (at most 30) with range * 2^s + 65 <= (2^31 - 1) / (n_segments + 1); else the
+    // wide form, range * 2^s + 65 <= (2^32 - 1) / 32
     const double range = hi - lo;
+    double cap = std::floor(2147483647.0 / (double)(n_segments + 1));
     int s = 30;
     while (s > 0 && range * std::ldexp(1.0, s) + 65.0 > cap) --s;
-    if (secant_err > 1e-7 || s < 22) return false;
+    if (s < 22) {
+        wide = 1;
+        cap = std::floor(4294967295.0 / 32.0);
+        s = 30;
+        while (s > 0 && range * std::ldexp(1.0, s) + 65.0 > cap) --s;
+    }
+    if (secant_err > 1e-7 || s < 22) {
+        wide = 0;
+        return false;
+    }
     inv_scale = std::ldexp(1.0, -s);
     c0 = lo - 64.0 * inv_scale;
     for (uint32_t i = 0; i < bins; ++i) {

@@ -57,12 +57,14 @@ bool lut_faithful_host(float mu, float eps, float scatter, float min_bound, floa
 //    of the blend across the bin, log10(1 + step (L_{i+1}/L_i - 1)), as float), with
 //    c0 = min log10 L_i - 64 2^-s so that every entry is at least 64 and a path total
 //    stays positive under rounded corrections, and (n_segments + 1) * max entry < 2^31 so
-//    that a path total and the difference of two totals are exact in 32 bits.
+//    that a path total and the difference of two totals are exact in 32 bits (narrow);
+//    when that leaves fewer than 22 fraction bits, 32 * max entry < 2^32 (wide = 1: exact
+//    32-bit lane sums of up to 32 entries, 64-bit path totals).
 // secant_err = the worst per-segment error of the secant, (step a)^2 / (8 ln 10) with
 // a = L_{i+1}/L_i - 1. Returns false (fix unusable, the exact blend is needed) when an
-// entry is not positive, secant_err > 1e-7, or fewer than 22 fraction bits fit.
+// entry is not positive, secant_err > 1e-7, or fewer than 22 fraction bits fit either way.
 bool compensated_tables(const float *lut, uint32_t bins, float step, uint32_t n_segments, std::vector<float> &lin,
-                        std::vector<float> &fix, double &c0, double &inv_scale, double &secant_err);
+                        std::vector<float> &fix, double &c0, double &inv_scale, int &wide, double &secant_err);
 
 // K4 (Twisty/PathWeightUtils.cpp:643-651) and the z of Norm (:729-732), float math.
 double norm_k4_log10(float z, float ds);

@@ -101,14 +101,18 @@ cudaError_t launch_fp64_chains(const ChainSpec &c, const float *init_pos, double
 // Compensated form. init_seg holds the N initial segment vectors (float3, x_{i+1}-x_i).
 //
 // Fixed-point form of the compensated log table: entry i of the float2 table holds
-// round((log10 L_i - c0) * 2^s) as uint32 bits in .x (c0 = the smallest log10 L_i, so every
-// entry is non-negative) and the float secant slope in .y; a path's log10 weight is
-// (N-1) c0 + (sum of the uint32 entries) * 2^-s + (sum of the slope corrections). A lane
-// sums at most `spl` entries in 32 bits, so the table is built with spl * max entry < 2^32.
-// inv_scale = 0 selects the exact (L_i, L_{i+1}-L_i) table instead.
+// round((log10 L_i - c0) * 2^s) as uint32 bits in .x (every entry at least 64) and the change
+// of log10 of the blend across the bin in .y; a path's log10 weight is (N-1) c0 + (its integer
+// total) * 2^-s, the total being the sum of its entries plus its rounded interpolation
+// corrections. Narrow tables (wide = 0) keep (N+1) * max entry < 2^31: path totals and their
+// differences are exact in 32 bits. Wide tables (wide = 1, long paths or wide-ranging tables)
+// keep 32 * max entry < 2^32: a lane's sum of at most 32 entries is exact in 32 bits, path
+// totals and differences are 64-bit. inv_scale = 0 selects the exact (L_i, L_{i+1}-L_i) table.
 struct LogFixed {
     double c0;
     double inv_scale;
+    int32_t wide;
+    int32_t pad;
 };
 struct CompTuning {
     int group;               // lanes per chain (4, 8, 16, 32)

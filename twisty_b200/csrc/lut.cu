@@ -245,8 +245,9 @@ __global__ void __launch_bounds__(1024) lut_finalize_kernel(uint32_t bins, doubl
 // Compensated-form tables of one experiment per CTA, the device twin of the host's
 // compensated_tables (same rules): lin = (L_i, L_{i+1} - L_i); fix = (round((log10 L_i - c0)
 // 2^s) as uint32, log10(1 + step (L_{i+1}/L_i - 1))) with c0 = min log10 L - 64 2^-s and the
-// largest s <= 30 keeping (N+1) (range 2^s + 65) below 2^31. ok[x] = 1 when the fixed form is
-// usable: every entry positive, secant error <= 1e-7 per segment, s >= 22.
+// largest s <= 30 keeping (N+1) (range 2^s + 65) below 2^31, else the wide form with
+// 32 (range 2^s + 65) below 2^32. ok[x] = 1 when the fixed form is usable: every entry
+// positive, secant error <= 1e-7 per segment, s >= 22.
 __global__ void __launch_bounds__(1024) comp_tables_kernel(uint32_t bins, const float *__restrict__ lut32,
                                                            const float *__restrict__ steps,
                                                            const uint32_t *__restrict__ nsegs, float2 *fix,
@@ -303,13 +304,20 @@ __global__ void __launch_bounds__(1024) comp_tables_kernel(uint32_t bins, const 
     hi = s_hi[0];
     err = s_err[0];
     bad = s_bad[0];
-    const double cap = floor(2147483647.0 / (double)(nsegs[x] + 1));
+    double cap = floor(2147483647.0 / (double)(nsegs[x] + 1));
     int s = 30;
     while (s > 0 && (hi - lo) * ldexp(1.0, s) + 65.0 > cap) --s;
+    int wide = 0;
+    if (s < 22) {
+        wide = 1;
+        cap = floor(4294967295.0 / 32.0);
+        s = 30;
+        while (s > 0 && (hi - lo) * ldexp(1.0, s) + 65.0 > cap) --s;
+    }
     const bool usable = !bad && err <= 1e-7 && s >= 22;
     const double inv_scale = ldexp(1.0, -s);
     if (threadIdx.x == 0) {
-        lf[x] = usable ? LogFixed{lo - 64.0 * inv_scale, inv_scale} : LogFixed{0.0, 0.0};
+        lf[x] = usable ? LogFixed{lo - 64.0 * inv_scale, inv_scale, wide, 0} : LogFixed{0.0, 0.0, 0, 0};
         ok[x] = usable ? 1 : 0;
     }
     if (!usable) return;

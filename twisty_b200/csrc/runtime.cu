@@ -93,7 +93,7 @@ struct twisty_ctx {
     LutMetaF meta{};
     double min_w = 0, max_w = 0, secant_err = 0;
     int exact_blend = 0;
-    LogFixed lf{0.0, 0.0};   // fixed-point form of fixtab; inv_scale 0 when exact_blend
+    LogFixed lf{0.0, 0.0, 0, 0};   // fixed-point form of fixtab; inv_scale 0 when exact_blend
     std::vector<float> ext_lut;
     twisty_lut_info ext_info{};
 
@@ -243,8 +243,9 @@ void build_tables(twisty_ctx *ctx, float ds, bool derivatives)
     // segment; otherwise the exact blend.
     std::vector<float> lin, fix;
     double c0 = 0.0, inv_scale = 0.0, err = 0.0;
+    int wide = 0;
     const bool fixed_ok =
-          compensated_tables(host32.data(), bins, ctx->meta.step, p.num_segments, lin, fix, c0, inv_scale, err);
+          compensated_tables(host32.data(), bins, ctx->meta.step, p.num_segments, lin, fix, c0, inv_scale, wide, err);
     ck(cudaMemcpyAsync(ctx->lintab.p, lin.data(), sizeof(float) * lin.size(), cudaMemcpyHostToDevice, st), "upload linear table");
     if (fixed_ok)
         ck(cudaMemcpyAsync(ctx->fixtab.p, fix.data(), sizeof(float) * fix.size(), cudaMemcpyHostToDevice, st),
@@ -252,7 +253,7 @@ void build_tables(twisty_ctx *ctx, float ds, bool derivatives)
     ck(cudaStreamSynchronize(st), "tables");
     ctx->secant_err = err;
     ctx->exact_blend = fixed_ok ? 0 : 1;
-    ctx->lf = fixed_ok ? LogFixed{c0, inv_scale} : LogFixed{0.0, 0.0};
+    ctx->lf = fixed_ok ? LogFixed{c0, inv_scale, wide, 0} : LogFixed{0.0, 0.0, 0, 0};
     std::memcpy(ctx->lut_key, key, sizeof(key));
     ctx->lut_ready = true;
 }
@@ -1074,7 +1075,7 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
         BatchExpHost &b = bh[e];
         b.spec = h.spec;
         b.meta = h.meta;
-        b.lf = exact ? LogFixed{0.0, 0.0} : lf[e];
+        b.lf = exact ? LogFixed{0.0, 0.0, 0, 0} : lf[e];
         b.tab = (exact ? B.lin.as<float2>() : B.fix.as<float2>()) + (size_t)e * bins;
         b.init_seg = B.init_seg.as<float>() + h.seg_off;
         b.out_offset = h.chain_off;
