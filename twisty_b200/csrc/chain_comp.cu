@@ -134,13 +134,13 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float x)
 // propagates through the interpolation fraction); the bound on the bin also keeps a
 // non-finite tangent, which only a degenerate zero-length chord can produce, in the table.
 template <bool CLAMP>
-__device__ __forceinline__ float bin_of(float qq, const CompConsts &k, uint32_t &clamped, int32_t &L)
+__device__ __forceinline__ float bin_of(float qq, const CompConsts &k, bool valid, uint32_t &clamped, int32_t &L)
 {
     float r = fmaf(sqrt_approx(qq), k.kscale, k.roff);
     if (CLAMP) {
         if (r < 0.0f) r = 0.0f;
         if (r > k.rmax) {
-            clamped += (r - k.rmax >= k.rsnap) ? 1u : 0u;
+            clamped += (valid && r - k.rmax >= k.rsnap) ? 1u : 0u;
             r = k.rmax;
         }
     }
@@ -148,10 +148,13 @@ __device__ __forceinline__ float bin_of(float qq, const CompConsts &k, uint32_t 
     return r;
 }
 
-// Walk the curvatures this lane owns: seg(i, qq) for curvature i = base+m-1 (between
+// Walk the curvatures this lane owns: seg(i, qq, valid) for curvature i = base+m-1 (between
 // segments base+m-1 and base+m), the last one with the next lane's first tangent.
-// tan(m, x, y, z) gives the unit tangent of segment j*SPL+m; next(t0, n) the next lane's
-// first tangent given this lane's (t0). FULLN: N == G*SPL, every lane's own curvatures exist.
+// tan(m, x, y, z) gives the unit tangent of segment j*SPL+m (zero past the last segment);
+// next(t0, n) the next lane's first tangent given this lane's (t0). Every slot is evaluated,
+// with valid = false past curvature N-2, so no table load hides behind a branch (padding
+// tangents are zero: their |t_{i+1}-t_i|^2 is 0 or 1, a bin in the table). FULLN: N == G*SPL,
+// only the group's last boundary is invalid.
 template <int G, int SPL, bool FULLN, class TanFn, class NextFn, class SegFn>
 __device__ __forceinline__ void for_curvatures(uint32_t j, uint32_t N, TanFn tan, NextFn next, SegFn seg)
 {
@@ -163,18 +166,16 @@ __device__ __forceinline__ void for_curvatures(uint32_t j, uint32_t N, TanFn tan
         tan(m, tx, ty, tz);
         if (m == 0) {
             t0x = tx; t0y = ty; t0z = tz;
-        } else if (FULLN || base + m <= N - 1) {
+        } else {
             const float dx = tx - px, dy = ty - py, dz = tz - pz;
-            seg(base + m - 1, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+            seg(base + m - 1, fmaf(dx, dx, fmaf(dy, dy, dz * dz)), FULLN || base + m <= N - 1);
         }
         px = tx; py = ty; pz = tz;
     }
     float nx, ny, nz;
     next(t0x, t0y, t0z, nx, ny, nz);
-    if (base + SPL <= N - 1) {
-        const float dx = nx - px, dy = ny - py, dz = nz - pz;
-        seg(base + SPL - 1, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
-    }
+    const float dx = nx - px, dy = ny - py, dz = nz - pz;
+    seg(base + SPL - 1, fmaf(dx, dx, fmaf(dy, dy, dz * dz)), base + SPL <= N - 1);
 }
 
 // next() for tangents held in registers: the next lane's t0 by shuffle.
@@ -198,17 +199,18 @@ __device__ __forceinline__ double path_log10(uint32_t j, uint32_t N, const float
 {
     unsigned long long isum = 0;
     float csum = 0.f, ks = 0.f, kc = 0.f;
-    for_curvatures<G, SPL, false>(j, N, tan, next, [&](uint32_t i, float qq) {
+    for_curvatures<G, SPL, false>(j, N, tan, next, [&](uint32_t i, float qq, bool valid) {
         int32_t L;
-        const float r = bin_of<CLAMP>(qq, k, clamped, L);
-        bin_sink(i, isnan(r) ? -1 : L);
+        const float r = bin_of<CLAMP>(qq, k, valid, clamped, L);
+        if (valid) bin_sink(i, isnan(r) ? -1 : L);
         const float frac = r - (float)L;
         const float2 e = tab[L];
         if (EXACT) {
-            kahan_add(ks, kc, __log2f(fmaf(frac * k.step, e.y, e.x)) * kLog10_2);
+            const float term = __log2f(fmaf(frac * k.step, e.y, e.x)) * kLog10_2;
+            kahan_add(ks, kc, valid ? term : 0.0f);
         } else {
-            isum += __float_as_uint(e.x);
-            csum = fmaf(frac, e.y, csum);
+            isum += valid ? __float_as_uint(e.x) : 0u;
+            csum = fmaf(valid ? frac : 0.0f, e.y, csum);
         }
     });
     if (EXACT) {
@@ -233,12 +235,12 @@ __device__ __forceinline__ unsigned long long path_fixed(uint32_t j, uint32_t gb
 {
     uint32_t isum = 0;
     float csum = 0.f;
-    auto seg = [&](uint32_t, float qq) {
+    auto seg = [&](uint32_t, float qq, bool valid) {
         int32_t L;
-        const float r = bin_of<CLAMP>(qq, k, clamped, L);
+        const float r = bin_of<CLAMP>(qq, k, valid, clamped, L);
         const float2 e = tab[L];
-        isum += __float_as_uint(e.x);
-        csum = fmaf(r - (float)L, e.y, csum);
+        isum += valid ? __float_as_uint(e.x) : 0u;
+        csum = fmaf(valid ? r - (float)L : 0.0f, e.y, csum);
     };
     if (N == (uint32_t)(G * SPL))
         for_curvatures<G, SPL, true>(j, N, tan, next, seg);
@@ -566,7 +568,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
             if (MODE == kModeAdjoint) {
                 // log10 weight and d/d(mu_s), d/d(eps) of this lane's segments (exact blend)
                 float s = 0.f, cc = 0.f, gmu = 0.f, geps = 0.f;
-                for_curvatures<G, SPL, false>(j, N, tan_smem, next_smem, [&](uint32_t, float qq) {
+                for_curvatures<G, SPL, false>(j, N, tan_smem, next_smem, [&](uint32_t, float qq, bool valid) {
                     float r = fmaf(sqrt_approx(qq), kc.kscale, kc.roff);
                     if (r < 0.f) r = 0.f;
                     if (r > kc.rmax) r = kc.rmax;
@@ -575,11 +577,11 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                     const float d = (r - (float)L) * kc.step;
                     const float lv = __ldg(ma.lut + L), rv = __ldg(ma.lut + Rb);
                     const float v = fmaf(d, rv - lv, lv);
-                    kahan_add(s, cc, __log2f(v) * kLog10_2);
+                    kahan_add(s, cc, valid ? __log2f(v) * kLog10_2 : 0.0f);
                     const float ml = __ldg(ma.dmu + L), mr = __ldg(ma.dmu + Rb);
                     const float el = __ldg(ma.deps + L), er = __ldg(ma.deps + Rb);
-                    gmu += fmaf(d, mr - ml, ml) / v;
-                    geps += fmaf(d, er - el, el) / v;
+                    gmu += valid ? fmaf(d, mr - ml, ml) / v : 0.0f;
+                    geps += valid ? fmaf(d, er - el, el) / v : 0.0f;
                 });
                 float hi = s, lo = -cc;
                 group_sum_pair<G>(hi, lo);
