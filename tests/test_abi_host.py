@@ -142,3 +142,10 @@ def test_no_device_is_an_error_not_a_fallback():
     with pytest.raises(T.TwistyError) as e:
         T.Context(T.default_params(num_segments=8))
     assert e.value.status == _abi.ERR_NO_DEVICE
+
+
+def test_autograd_binding_imports_without_a_gpu():
+    """The torch binding is importable on a CPU host (it calls the library only when run)."""
+    from twisty_b200 import autograd
+    assert callable(autograd.experiment_log10_weight)
+    assert issubclass(autograd.ExperimentLog10Weight, __import__("torch").autograd.Function)
