@@ -58,3 +58,36 @@ def test_all_combine_gloo_two_ranks():
         assert p.exitcode == 0
     ref = D.combine([D.local_tuple(R(**p)) for p in PARTS])
     assert out[0] == out[1] == ref
+
+
+BATCH = [[dict(PARTS[0]), dict(PARTS[1], log10_weight=-12.5)],
+         [dict(PARTS[1]), dict(PARTS[0], log10_weight=-12.0, rel_std_error=0.03)]]   # [rank][experiment]
+
+
+def _batch_worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        q.put((rank, D.all_combine_batch([R(**e) for e in BATCH[rank]])))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_all_combine_batch_gloo_two_ranks():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_batch_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = dict(q.get(timeout=120) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for i in range(2):
+        ref = D.combine([D.local_tuple(R(**BATCH[r][i])) for r in range(2)])
+        assert out[0][i] == out[1][i] == ref

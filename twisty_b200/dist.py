@@ -49,3 +49,16 @@ def all_combine(result, group=None, device=None) -> dict:
     parts = [torch.empty_like(t) for _ in range(dist.get_world_size(group))]
     dist.all_gather(parts, t, group=group)
     return combine([p.tolist() for p in parts])
+
+
+def all_combine_batch(results, group=None, device=None) -> list:
+    """The batched form: every rank ran the same experiments (twisty_run_batch) on its own chain
+    range; one all-gather of an n x 6 tensor, then experiment i combines the ranks' i-th tuples.
+    Every rank must pass the same number of results."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([local_tuple(r) for r in results], dtype=torch.float64, device=device).reshape(-1, len(FIELDS))
+    parts = [torch.empty_like(t) for _ in range(dist.get_world_size(group))]
+    dist.all_gather(parts, t, group=group)
+    rows = [p.tolist() for p in parts]
+    return [combine([rows[r][i] for r in range(len(rows))]) for i in range(t.shape[0])]
