@@ -254,6 +254,29 @@ twisty_status twisty_export_paths(twisty_ctx *ctx, const twisty_bc *bc, const ch
 twisty_status twisty_adjoint(twisty_ctx *ctx, const twisty_bc *bc, const twisty_result *fwd,
                              double grad[5]);
 
+/* ---------------------------------------------------------------- autotuner */
+/* No counterpart in the reference. Times every supported compensated-form kernel shape
+ * (lanes per chain x segments per lane x warps per CTA) for the context's N and table on a
+ * short pass of trial_paths paths (0: 2^22) with the context's other parameters, records
+ * the fastest in the process-wide tuning cache and returns it. Every later pass (twisty_run,
+ * twisty_run_batch) on a device of the same name, with the same N and table size and the
+ * shape knobs (comp_group, comp_spl, comp_warps) left at zero, uses the recorded shape. */
+typedef struct twisty_tuning {
+    uint32_t num_segments;
+    uint32_t bins;
+    uint32_t group;              /* lanes per chain */
+    uint32_t spl;                /* segments per lane */
+    uint32_t warps;              /* warps per CTA */
+    double path_segments_per_s;  /* measured rate of that shape */
+} twisty_tuning;
+
+twisty_status twisty_autotune(twisty_ctx *ctx, const twisty_bc *bc, uint64_t trial_paths, twisty_tuning *best);
+/* The tuning cache as JSON: {"entries": [{"device", "n", "bins", "group", "spl", "warps",
+ * "path_segments_per_s"}, ...]}. Loading merges into the cache (an entry replaces one with
+ * the same device, n and bins); a malformed file or unsupported shape is rejected whole. */
+twisty_status twisty_tuning_cache_save(const char *path);
+twisty_status twisty_tuning_cache_load(const char *path);
+
 /* ------------------------------------------------------- allocation-free pass */
 /* No counterpart in the reference. For callers that cannot allocate device memory when
  * they run a pass: an application whose own caching allocator holds nearly all of the

@@ -149,3 +149,25 @@ def test_autograd_binding_imports_without_a_gpu():
     from twisty_b200 import autograd
     assert callable(autograd.experiment_log10_weight)
     assert issubclass(autograd.ExperimentLog10Weight, __import__("torch").autograd.Function)
+
+
+def test_tuning_cache_roundtrip_and_rejects_bad_files(tmp_path):
+    """The tuning cache file is host-side JSON: save, reload, and refuse malformed input."""
+    import twisty_b200 as T
+    good = tmp_path / "tune.json"
+    good.write_text('{"entries": [{"device": "X", "n": 256, "bins": 8192, "group": 32, "spl": 8, '
+                    '"warps": 32, "path_segments_per_s": 6.6e11}]}')
+    T.tuning_cache_load(str(good))
+    out = tmp_path / "out.json"
+    T.tuning_cache_save(str(out))
+    import json
+    e = [x for x in json.loads(out.read_text())["entries"] if x["device"] == "X"]
+    assert e == [{"device": "X", "n": 256, "bins": 8192, "group": 32, "spl": 8, "warps": 32,
+                  "path_segments_per_s": 6.6e11}]
+    bad_shape = tmp_path / "bad1.json"
+    bad_shape.write_text('{"entries": [{"device": "X", "n": 256, "bins": 8192, "group": 7, "spl": 8, "warps": 32}]}')
+    bad_json = tmp_path / "bad2.json"
+    bad_json.write_text('{"entries": [ {"device": "X", "n": ')
+    for f in (bad_shape, bad_json, tmp_path / "missing.json"):
+        with pytest.raises(T.TwistyError):
+            T.tuning_cache_load(str(f))

@@ -1,0 +1,40 @@
+"""twisty_autotune: times the compensated kernel shapes for one N and records the fastest."""
+import math
+
+import pytest
+
+import twisty_b200 as T
+
+pytestmark = pytest.mark.gpu
+
+
+def _params(N, **kw):
+    base = dict(num_segments=N, mu=1.0, eps=0.01, scatter=10.0, num_steps_int=2000, num_curvature_steps=2048,
+                form=T.FORM_COMPENSATED, lut_mode=T.LUT_FP64, perturb_seed=3, paths_to_generate=1 << 20,
+                paths_to_skip=16, max_sub_chain=32, max_angle=0.05)
+    base.update(kw)
+    return T.default_params(**base)
+
+
+def test_autotune_records_a_shape_that_later_runs_use(tmp_path):
+    N = 100
+    bc = T.make_bc((0, 0, 0), (0, 0, 1), (0, 0, 6), (0, 0, 1), 10.0)
+    with T.Context(_params(N)) as ctx:
+        best = ctx.autotune(bc, 1 << 19)
+        assert best["num_segments"] == N and best["bins"] == 2048
+        assert best["group"] * best["spl"] >= N and best["path_segments_per_s"] > 1e9
+        r = ctx.run(bc)   # knobs at zero: the recorded shape, default chain count for it
+    requested = 148 * best["warps"] * (32 // best["group"])   # the shape's default chain count
+    steps = -(-(1 << 20) // requested)
+    assert r.num_chains == -(-(1 << 20) // steps)
+    assert r.total_paths == 1 << 20 and r.failed_paths == 0 and math.isfinite(r.log10_weight)
+    out = tmp_path / "tune.json"
+    T.tuning_cache_save(str(out))
+    assert '"n": 100' in out.read_text()
+
+
+def test_autotune_rejects_other_forms():
+    bc = T.make_bc((0, 0, 0), (0, 0, 1), (0, 0, 6), (0, 0, 1), 10.0)
+    with T.Context(_params(100, form=T.FORM_PLAIN_FP32)) as ctx:
+        with pytest.raises(T.TwistyError):
+            ctx.autotune(bc, 1 << 16)

@@ -194,12 +194,29 @@ class Context:
         _check(_lib().twisty_adjoint(self._h, C.byref(bc), C.byref(fwd), g), self._h)
         return np.array(list(g))
 
+    def autotune(self, bc: _abi.BC, trial_paths: int = 0) -> dict:
+        """Time every compensated-form kernel shape for this context's N; the fastest is
+        recorded in the process-wide tuning cache and used by later passes."""
+        t = _abi.Tuning()
+        _check(_lib().twisty_autotune(self._h, C.byref(bc), int(trial_paths), C.byref(t)), self._h)
+        return {f: getattr(t, f) for f, _ in _abi.Tuning._fields_}
+
     def run_batch(self, experiments: Sequence[_abi.Experiment], iterations: int = 1):
         n = len(experiments)
         arr = (_abi.Experiment * n)(*experiments)
         res = (_abi.Result * n)()
         _check(_lib().twisty_run_batch(self._h, arr, n, iterations, res), self._h)
         return list(res)
+
+
+def tuning_cache_save(path: str):
+    """Write the process-wide tuning cache (shapes found by Context.autotune) as JSON."""
+    _check(_lib().twisty_tuning_cache_save(path.encode()))
+
+
+def tuning_cache_load(path: str):
+    """Merge a JSON tuning cache into the process-wide one."""
+    _check(_lib().twisty_tuning_cache_load(path.encode()))
 
 
 def bootstrap_curve(params: _abi.Params, bc: _abi.BC) -> np.ndarray:

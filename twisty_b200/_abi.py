@@ -106,6 +106,11 @@ class Experiment(C.Structure):
                 ("paths", C.c_uint64)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("num_segments", C.c_uint32), ("bins", C.c_uint32), ("group", C.c_uint32), ("spl", C.c_uint32),
+                ("warps", C.c_uint32), ("path_segments_per_s", C.c_double)]
+
+
 NOALLOC_MAX_CHAINS = 16384
 
 
@@ -152,6 +157,9 @@ SIGNATURES = [
                                       C.POINTER(Result)]),
     ("twisty_adjoint", C.c_int, [_P, C.POINTER(BC), C.POINTER(Result), C.POINTER(C.c_double)]),
     ("twisty_run_noalloc", C.c_int, [C.POINTER(NoAllocArgs), _P]),
+    ("twisty_autotune", C.c_int, [_P, C.POINTER(BC), C.c_uint64, C.POINTER(Tuning)]),
+    ("twisty_tuning_cache_save", C.c_int, [C.c_char_p]),
+    ("twisty_tuning_cache_load", C.c_int, [C.c_char_p]),
 ]
 
 _lib = None

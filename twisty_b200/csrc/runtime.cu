@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <functional>
 #include <limits>
+#include <mutex>
 #include <new>
 #include <sstream>
 #include <string>
@@ -82,6 +83,7 @@ struct twisty_ctx {
     twisty_params p{};
     int device = 0;
     int sm_count = 148;
+    std::string device_name;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     std::string err;
@@ -145,6 +147,44 @@ void validate_bc(const twisty_bc *bc)
 }
 
 void set_device(twisty_ctx *ctx) { ck(cudaSetDevice(ctx->device), "cudaSetDevice"); }
+
+// ------------------------------------------------------------ tuning cache
+// Compensated-form kernel shapes measured by twisty_autotune (or loaded from a cache file),
+// keyed by device name, N and table size; consulted whenever the shape knobs are zero.
+struct TuneEntry {
+    std::string device;
+    uint32_t n, bins, group, spl, warps;
+    double rate;
+};
+std::mutex g_tune_mu;
+std::vector<TuneEntry> g_tune;
+
+void tune_record(const TuneEntry &e)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (TuneEntry &x : g_tune)
+        if (x.device == e.device && x.n == e.n && x.bins == e.bins) {
+            x = e;
+            return;
+        }
+    g_tune.push_back(e);
+}
+
+bool tune_lookup(const std::string &device, uint32_t n, uint32_t bins, CompTuning &t)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (const TuneEntry &x : g_tune)
+        if (x.device == device && x.n == n && x.bins == bins) {
+            CompTuning c = t;
+            c.group = (int)x.group;
+            c.spl = (int)x.spl;
+            c.warps_per_block = (int)x.warps;
+            if (!comp_tuning_supported(c, n, 2)) return false;
+            t = c;
+            return true;
+        }
+    return false;
+}
 
 // ------------------------------------------------------------------ tables
 void build_tables(twisty_ctx *ctx, float ds, bool derivatives)
@@ -350,6 +390,7 @@ void prepare(twisty_ctx *ctx, const twisty_bc *bcp)
         max_steps = std::min<uint32_t>(max_steps, 1000000u);
     } else if (p.form == TWISTY_FORM_COMPENSATED) {
         ctx->tuning = comp_default_tuning(N);
+        if (!p.comp_group && !p.comp_spl && !p.comp_warps) tune_lookup(ctx->device_name, N, p.num_curvature_steps, ctx->tuning);
         if (p.comp_group || p.comp_spl) {
             if (!p.comp_group || !p.comp_spl) fail(TWISTY_ERR_INVALID_CONFIG, "comp_group and comp_spl are set together");
             ctx->tuning.group = (int)p.comp_group;
@@ -676,6 +717,9 @@ twisty_status twisty_create(const twisty_params *p, twisty_ctx **out)
         int sms = 0;
         ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device), "device query");
         ctx->sm_count = sms;
+        cudaDeviceProp prop{};
+        ck(cudaGetDeviceProperties(&prop, ctx->device), "device query");
+        ctx->device_name = prop.name;
         ck(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "stream");
         for (auto &e : ctx->ev) ck(cudaEventCreate(&e), "event");
     });
@@ -988,6 +1032,7 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
         h.log10_norm = normalizer_log10(ctx, N, h.ds, x.bc);
         // kernel shape and chain layout: whole CTAs of chains, ~2048 steps per chain
         h.t = comp_default_tuning(N);
+        tune_lookup(ctx->device_name, N, bins, h.t);
         ChainSpec &c = h.spec;
         c = ChainSpec{};
         c.n_segments = N;
@@ -1334,3 +1379,156 @@ twisty_status twisty_set_initial_curve(twisty_ctx *ctx, const float *pos, uint32
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ autotuner
+twisty_status twisty_autotune(twisty_ctx *ctx, const twisty_bc *bc, uint64_t trial_paths, twisty_tuning *best)
+{
+    if (!ctx || !bc || !best) return TWISTY_ERR_INVALID_ARGUMENT;
+    return guard(ctx, [&] {
+        const twisty_params saved = ctx->p;
+        validate(saved);
+        if (saved.form != TWISTY_FORM_COMPENSATED) fail(TWISTY_ERR_UNSUPPORTED, "the autotuner times the compensated form");
+        const uint32_t N = saved.num_segments, bins = saved.num_curvature_steps;
+        const uint64_t paths = trial_paths ? trial_paths : (1ull << 22);
+        struct Cand {
+            int group, spl, warps;
+        };
+        std::vector<Cand> cands;
+        const CompTuning def = comp_default_tuning(N);
+        for (int g : {8, 16, 32})
+            for (int spl : {2, 4, 8, 16, 32})
+                for (int w = 4; w <= 32; w += 4) {
+                    CompTuning t{g, spl, w, 0};
+                    const uint32_t k_eff = std::min<uint32_t>(saved.max_sub_chain, N - 2);
+                    if (!comp_tuning_supported(t, N, k_eff)) continue;
+                    // shapes much wider than N waste their lanes; keep the default shape's width
+                    if ((uint32_t)(g * spl) >= 4 * N && g * spl > def.group * def.spl) continue;
+                    if (comp_smem_bytes(t, bins) > 227 * 1024) continue;
+                    cands.push_back(Cand{g, spl, w});
+                }
+        if (cands.empty()) fail(TWISTY_ERR_UNSUPPORTED, "no compensated kernel shape for this N / max_sub_chain");
+        double best_rate = -1.0;
+        Cand bestc = cands.front();
+        std::string last_err;
+        try {
+            for (const Cand &cd : cands) {
+                ctx->p = saved;
+                ctx->p.comp_group = (uint32_t)cd.group;
+                ctx->p.comp_spl = (uint32_t)cd.spl;
+                ctx->p.comp_warps = (uint32_t)cd.warps;
+                ctx->p.paths_to_generate = paths;
+                ctx->p.paths_to_skip = 0;   // burn-in scales with the chain count, not the shape
+                ctx->p.num_chains = 0;
+                try {
+                    prepare(ctx, bc);
+                    launch(ctx, ctx->stream);   // warm
+                    twisty_result r{};
+                    collect(ctx, &r);
+                    launch(ctx, ctx->stream);
+                    collect(ctx, &r);
+                    const double rate = (double)r.total_paths * N / (r.perturb_ms * 1e-3);
+                    if (r.perturb_ms > 0 && rate > best_rate) {
+                        best_rate = rate;
+                        bestc = cd;
+                    }
+                } catch (const Failure &f) {
+                    if (f.s != TWISTY_ERR_UNSUPPORTED && f.s != TWISTY_ERR_INVALID_CONFIG) throw;
+                    last_err = f.msg;
+                }
+            }
+        } catch (...) {
+            ctx->p = saved;
+            ctx->prepared = false;
+            throw;
+        }
+        ctx->p = saved;
+        ctx->prepared = false;
+        if (best_rate < 0) fail(TWISTY_ERR_UNSUPPORTED, "no shape ran: " + last_err);
+        tune_record(TuneEntry{ctx->device_name, N, bins, (uint32_t)bestc.group, (uint32_t)bestc.spl,
+                              (uint32_t)bestc.warps, best_rate});
+        best->num_segments = N;
+        best->bins = bins;
+        best->group = (uint32_t)bestc.group;
+        best->spl = (uint32_t)bestc.spl;
+        best->warps = (uint32_t)bestc.warps;
+        best->path_segments_per_s = best_rate;
+    });
+}
+
+twisty_status twisty_tuning_cache_save(const char *path)
+{
+    if (!path) return TWISTY_ERR_INVALID_ARGUMENT;
+    std::ostringstream o;
+    o.precision(17);
+    o << "{\n  \"entries\": [";
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        for (size_t i = 0; i < g_tune.size(); ++i) {
+            const TuneEntry &e = g_tune[i];
+            std::string dev;
+            for (char ch : e.device) {
+                if (ch == '"' || ch == '\\') dev.push_back('\\');
+                dev.push_back(ch);
+            }
+            o << (i ? "," : "") << "\n    {\"device\": \"" << dev << "\", \"n\": " << e.n << ", \"bins\": " << e.bins
+              << ", \"group\": " << e.group << ", \"spl\": " << e.spl << ", \"warps\": " << e.warps
+              << ", \"path_segments_per_s\": " << e.rate << "}";
+        }
+    }
+    o << "\n  ]\n}\n";
+    std::ofstream f(path);
+    if (!f) {
+        g_free_err = std::string("cannot write ") + path;
+        return TWISTY_ERR_IO;
+    }
+    f << o.str();
+    return f.good() ? TWISTY_OK : TWISTY_ERR_IO;
+}
+
+twisty_status twisty_tuning_cache_load(const char *path)
+{
+    if (!path) return TWISTY_ERR_INVALID_ARGUMENT;
+    std::ifstream f(path);
+    if (!f) {
+        g_free_err = std::string("cannot read ") + path;
+        return TWISTY_ERR_IO;
+    }
+    std::stringstream ss;
+    ss << f.rdbuf();
+    Node root;
+    std::string err;
+    if (!parse_json(ss.str(), root, err)) {
+        g_free_err = "tuning cache: " + err;
+        return TWISTY_ERR_INVALID_CONFIG;
+    }
+    const Node *es = root.get("entries");
+    if (!es || es->kind != Node::Array) {
+        g_free_err = "tuning cache: no entries array";
+        return TWISTY_ERR_INVALID_CONFIG;
+    }
+    std::vector<TuneEntry> got;
+    for (const Node &e : es->arr) {
+        const Node *dv = e.get("device");
+        const char *keys[] = {"n", "bins", "group", "spl", "warps"};
+        uint32_t v[5];
+        bool ok = dv && dv->kind == Node::String;
+        for (int i = 0; i < 5 && ok; ++i) {
+            const Node *x = e.get(keys[i]);
+            ok = x && x->kind == Node::Number && x->num >= 0 && x->num < 4294967296.0;
+            if (ok) v[i] = (uint32_t)x->num;
+        }
+        if (!ok) {
+            g_free_err = "tuning cache: malformed entry";
+            return TWISTY_ERR_INVALID_CONFIG;
+        }
+        CompTuning t{(int)v[2], (int)v[3], (int)v[4], 0};
+        if (!comp_tuning_supported(t, v[0], 2)) {
+            g_free_err = "tuning cache: unsupported shape";
+            return TWISTY_ERR_INVALID_CONFIG;
+        }
+        const Node *rt = e.get("path_segments_per_s");
+        got.push_back(TuneEntry{dv->str, v[0], v[1], v[2], v[3], v[4], (rt && rt->kind == Node::Number) ? rt->num : 0.0});
+    }
+    for (const TuneEntry &e : got) tune_record(e);
+    return TWISTY_OK;
+}
