@@ -118,6 +118,11 @@ typedef struct twisty_params {
     uint32_t comp_group;
     uint32_t comp_spl;
     uint32_t comp_warps;
+    /* compensated form, single runs: 0 recomputes every curvature of every weighted path (the
+       reference's definition); R > 1 updates a path's weight incrementally from the two
+       curvatures a rotation changes and recomputes it in full every R-th weighted step
+       (an algorithmic shortcut, reported separately; fixed-point tables without clamping) */
+    uint32_t incremental_resync;
 } twisty_params;
 
 /* ExperimentRunner::ExperimentResults (Twisty/ExperimentRunner.h:73-82). */

@@ -74,6 +74,7 @@ class Params(C.Structure):
         ("comp_group", C.c_uint32),
         ("comp_spl", C.c_uint32),
         ("comp_warps", C.c_uint32),
+        ("incremental_resync", C.c_uint32),
     ]
 
 

@@ -39,6 +39,12 @@
 //    than ~1e-7 per segment, the host selects the exact form instead: (L_i, L_{i+1} - L_i),
 //    a log2 per segment, a Kahan-compensated FP32 sum combined across lanes by TwoSum and
 //    a log-sum-exp over (hi, lo) float pairs.
+//  * Incremental variant (ChainSpec.incr_resync = R > 0, fixed-point tables only): a rotation
+//    turns the tangents of its sub-chain together, so of the path's curvatures only the two
+//    at its ends change (interior ones are invariant up to rounding). Each weighted step
+//    evaluates those two terms before and after the rotation and adds the difference to the
+//    path's integer total; every R-th weighted step recomputes the total in full. This is an
+//    algorithmic change of the recompute-everything definition and is reported separately.
 //  * FP64 appears only per chain (assembling its log10 sum), in the per-CTA log-sum-exp of
 //    the chains and in the global reduction (and per path in the exact form).
 //  * Proposals: lane j of a group draws the Philox proposal of step base+j (one draw per
@@ -339,7 +345,7 @@ __device__ __forceinline__ void stage_table(float4 *smem4, const float2 *__restr
 // warp-local slots): initial state from init_seg (segment vectors), burn_in + steps
 // proposals, a full recompute of every weighted path, and the chain's running log-sum-exp.
 // Writes out[chain] (when out is set and the chain is real) and returns the chain's log10 sum.
-template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MODE>
+template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MODE, bool INCR = false>
 __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConsts &kc,
                                              const float *__restrict__ init_seg, const float2 *s_tab, Planes st,
                                              uint32_t gbase, uint32_t j, uint32_t chain, bool real_chain,
@@ -390,6 +396,29 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
     unsigned long long lse_t = 0;                   // fixed form: running max as a path total
     uint32_t valid = 0, failed = 0, clamped = 0;
     float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    // incremental form: the current path's integer total and whether a NaN curvature was met
+    // since the last full recompute
+    unsigned long long inc_tot = 0;
+    bool inc_bad = false;
+    uint32_t inc_since_full = 0;   // incremental steps since the last full recompute
+    // tangent of segment s (any lane's) and the fixed-point term of the curvature between two
+    // tangents, with its interpolation correction rounded on its own
+    auto tan_at = [&](uint32_t s, float &x, float &y, float &z) {
+        const float2 a = st.xy[Lay::xy(gbase + s / SPL, s % SPL)];
+        x = a.x;
+        y = a.y;
+        z = st.z[Lay::z(gbase + s / SPL, s % SPL)];
+    };
+    auto term = [&](float ax, float ay, float az, float bx, float by, float bz, bool &nan) -> uint32_t {
+        const float dx = bx - ax, dy = by - ay, dz = bz - az;
+        int32_t L;
+        uint32_t unused = 0;
+        const float r = bin_of<CLAMP>(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), kc, false, unused, L);
+        const float2 e = s_tab[L];
+        const float frac = r - (float)L;
+        nan |= isnan(frac);
+        return __float_as_uint(e.x) + (uint32_t)__float2int_rn(frac * e.y * kc.fscale);
+    };
 
     const uint32_t own = gbase + j;
     // tangent of this lane's segment m; with SHIFT the weights see the receiver moved:
@@ -422,6 +451,22 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
             const float sn = __shfl_sync(FULL, psn, jj, G);
             const float cs = __shfl_sync(FULL, pcs, jj, G);
             const uint32_t right = left + k;
+            // incremental form: the two end curvatures before the rotation (kappa_{left-1} and
+            // kappa_{right-1}; left >= 1 and right <= N-1, so all four tangents exist)
+            bool incr_now = false;
+            uint32_t t_old = 0;
+            float e0x = 0.f, e0y = 0.f, e0z = 0.f, e3x = 0.f, e3y = 0.f, e3z = 0.f;
+            if constexpr (INCR) {
+                incr_now = base + jj > c.burn_in && inc_since_full + 1 < c.incr_resync;
+                if (incr_now) {
+                    float a1x, a1y, a1z, b0x, b0y, b0z;
+                    tan_at(left - 1, e0x, e0y, e0z);
+                    tan_at(left, a1x, a1y, a1z);
+                    tan_at(right - 1, b0x, b0y, b0z);
+                    tan_at(right, e3x, e3y, e3z);
+                    t_old = term(e0x, e0y, e0z, a1x, a1y, a1z, inc_bad) + term(b0x, b0y, b0z, e3x, e3y, e3z, inc_bad);
+                }
+            }
             // chord x_right - x_left = sum of l_s t_s over the k segments left .. right-1
             constexpr int R = (kMaxSubChain + G - 1) / G;
             float vx[R], vy[R], vz[R];
@@ -488,8 +533,24 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
 
             if (FIX) {
                 bool bad;
-                const unsigned long long tot =
-                      path_fixed<G, SPL, CLAMP>(j, gbase, N, s_tab, kc, tan_smem, next_smem, bad, clamped);
+                unsigned long long tot;
+                if (INCR && incr_now) {
+                    // the two end curvatures after the rotation; the interior ones keep their terms
+                    float a1x, a1y, a1z, b0x, b0y, b0z;
+                    tan_at(left, a1x, a1y, a1z);
+                    tan_at(right - 1, b0x, b0y, b0z);
+                    const uint32_t t_new =
+                          term(e0x, e0y, e0z, a1x, a1y, a1z, inc_bad) + term(b0x, b0y, b0z, e3x, e3y, e3z, inc_bad);
+                    inc_tot += (unsigned long long)(long long)(int32_t)(t_new - t_old);
+                    tot = inc_tot;
+                    bad = inc_bad;
+                    ++inc_since_full;
+                } else {
+                    tot = path_fixed<G, SPL, CLAMP>(j, gbase, N, s_tab, kc, tan_smem, next_smem, bad, clamped);
+                    inc_tot = tot;
+                    inc_bad = bad;
+                    inc_since_full = 0;
+                }
                 if (MODE == kModeExport) {
                     const double w = bad ? NAN : kc.lw_offset + (double)tot * kc.inv_scale;
                     // positions below
@@ -695,7 +756,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
     return real_chain ? chain_log10 : -INFINITY;
 }
 
-template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MAXT, int MODE>
+template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MAXT, int MODE, bool INCR>
 __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompConsts kc,
                                                              const float *__restrict__ init_seg,
                                                              const float2 *__restrict__ tab_g,
@@ -720,8 +781,8 @@ __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompCo
     unsigned char *wb = s_state + (size_t)warp * Lay::WARP_BYTES;
     const Planes pl{reinterpret_cast<float2 *>(wb), reinterpret_cast<float *>(wb + Lay::XY_BYTES),
                     reinterpret_cast<float *>(wb + Lay::XY_BYTES + Lay::Z_BYTES)};
-    const double cl = chain_body<G, SPL, EXACT, CLAMP, SHIFT, MODE>(c, kc, init_seg, s_tab, pl, q * G, j, chain,
-                                                                    chain < c.n_chains, out, ma);
+    const double cl = chain_body<G, SPL, EXACT, CLAMP, SHIFT, MODE, INCR>(c, kc, init_seg, s_tab, pl, q * G, j, chain,
+                                                                          chain < c.n_chains, out, ma);
     if (j == 0) s_res[warp * CPW + q] = cl;
     __syncthreads();
     // Per-CTA log-sum-exp of the chains, rescaled by the block maximum (FP64).
@@ -831,13 +892,13 @@ __global__ void __launch_bounds__(256) weigh_comp_kernel(const float *__restrict
 }
 
 // ------------------------------------------------------------------------------ launchers
-template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MODE>
+template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MODE, bool INCR = false>
 cudaError_t launch_t(const ChainSpec &c, const CompConsts &kc, int warps, const float *init_seg, const float2 *tab,
                      ChainOut *out, double2 *partials, const ModeArgs &ma, size_t smem, uint32_t blocks, cudaStream_t st)
 {
     constexpr int MAXT = (SPL >= 16) ? 512 : 1024;
     if (warps * 32 > MAXT) return cudaErrorInvalidConfiguration;
-    auto kern = comp_chain_kernel<G, SPL, EXACT, CLAMP, SHIFT, MAXT, MODE>;
+    auto kern = comp_chain_kernel<G, SPL, EXACT, CLAMP, SHIFT, MAXT, MODE, INCR>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     kern<<<blocks, warps * 32, smem, st>>>(c, kc, init_seg, tab, out, partials, ma);
@@ -857,7 +918,11 @@ cudaError_t launch_g(int mode, bool exact, bool clamp, bool shift, const ChainSp
     if (mode == kModeExport) return exact ? TWISTY_L(true, true, false, kModeExport) : TWISTY_L(false, true, false, kModeExport);
     if (shift) return TWISTY_L(true, true, true, kModeForward);
     if (exact) return clamp ? TWISTY_L(true, true, false, kModeForward) : TWISTY_L(true, false, false, kModeForward);
-    return clamp ? TWISTY_L(false, true, false, kModeForward) : TWISTY_L(false, false, false, kModeForward);
+    if (clamp) return TWISTY_L(false, true, false, kModeForward);
+    if (c.incr_resync > 1)
+        return launch_t<G, SPL, false, false, false, kModeForward, true>(c, kc, w, init_seg, tab, out, partials, ma, smem,
+                                                                         blocks, st);
+    return TWISTY_L(false, false, false, kModeForward);
 #undef TWISTY_L
 }
 

@@ -385,7 +385,7 @@ bool params_from_node(const Node &root, twisty_params &p, twisty_bc *bc, std::st
     p.min_bound = 0.0f;
     p.max_bound = 10.0f / p.eps;  // ExperimentRunner.cpp:169-171
     // Optional B200 block: experimentParams.b200 { form, lutMode, maxSubChain, maxAngle, numChains, device,
-    // compGroup, compSpl, compWarps }
+    // compGroup, compSpl, compWarps, incrementalResync }
     if (const Node *b = ep->get("b200")) {
         if (b->kind != Node::Object) {
             err = "experimentParams.b200 must be a mapping";
@@ -400,6 +400,8 @@ bool params_from_node(const Node &root, twisty_params &p, twisty_bc *bc, std::st
         if (b->get("compGroup") && num(b, "compGroup", "b200.compGroup", v, err)) p.comp_group = (uint32_t)v;
         if (b->get("compSpl") && num(b, "compSpl", "b200.compSpl", v, err)) p.comp_spl = (uint32_t)v;
         if (b->get("compWarps") && num(b, "compWarps", "b200.compWarps", v, err)) p.comp_warps = (uint32_t)v;
+        if (b->get("incrementalResync") && num(b, "incrementalResync", "b200.incrementalResync", v, err))
+            p.incremental_resync = (uint32_t)v;
         if (!err.empty()) return false;
     }
     if (bc) {

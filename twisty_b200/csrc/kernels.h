@@ -25,6 +25,9 @@ struct ChainSpec {
     double absorption_factor;// exp(-mu_a * ds) as the reference computes it (float exp, promoted)
     float eval_shift[3];     // receiver shift applied only when weighting
     int has_eval_shift;
+    uint32_t incr_resync;    // compensated form: > 1 selects incremental weight updates with a
+                             // full recompute every incr_resync-th weighted step (fixed-point,
+                             // unclamped tables, forward passes); 0 or 1: full recompute every step
 };
 
 // Float table metadata (BaseWeightLookupTable accessors).

@@ -381,6 +381,7 @@ void prepare(twisty_ctx *ctx, const twisty_bc *bcp)
     c.eval_shift[1] = p.eval_end_shift.y;
     c.eval_shift[2] = p.eval_end_shift.z;
     c.has_eval_shift = (p.eval_end_shift.x != 0.f || p.eval_end_shift.y != 0.f || p.eval_end_shift.z != 0.f) ? 1 : 0;
+    c.incr_resync = p.form == TWISTY_FORM_COMPENSATED ? p.incremental_resync : 0;
 
     uint32_t requested = p.num_chains;
     uint32_t max_steps = 0xFFFFFFFFu - c.burn_in;
