@@ -110,7 +110,11 @@ typedef struct twisty_params {
     int32_t device;              /* CUDA device ordinal */
     uint32_t chain_offset;       /* first global chain id (shards one experiment over GPUs) */
     uint32_t experiment_id;      /* Philox stream id of this experiment */
-    int32_t bootstrap_kind;      /* 0 auto, 1 reference recursion (N-2 in {4,6,8,12,16,24,...}), 2 arc */
+    int32_t bootstrap_kind;      /* initial curve: 0 the reference's recursive bootstrapper
+                                    (PathGeneration.cpp:47-414, the reference's curve for the
+                                    same bootstrap_seed) where it resolves N (N-2 in {4, 6, 8,
+                                    12, 16, 24, 32, 48, ...}), else the arc; 1 the reference's
+                                    only; 2 the arc (any N >= 4) */
     twisty_vec3 eval_end_shift;  /* weights evaluated with the receiver moved by this vector,
                                     the chain itself unchanged (finite-difference checks) */
     /* compensated-form kernel shape; 0 = chosen from N. comp_group lanes per chain (8, 16,

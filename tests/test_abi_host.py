@@ -171,3 +171,26 @@ def test_tuning_cache_roundtrip_and_rejects_bad_files(tmp_path):
     for f in (bad_shape, bad_json, tmp_path / "missing.json"):
         with pytest.raises(T.TwistyError):
             T.tuning_cache_load(str(f))
+
+
+@pytest.mark.parametrize("N,S", [(10, 5.0), (18, 6.0), (34, 12.0), (66, 10.0)])
+def test_reference_bootstrapper_bit_exact_with_reference(N, S):
+    """bootstrap_kind 1 reproduces the reference's ResolveEvenNumberOfSegments curves (golden
+    fixtures from the reference build, bootstrapSeed 7) bit for bit."""
+    from conftest import GEOM
+    g = GEOM[N]
+    bc = T.make_bc(g[0], g[1], g[2], g[3], S)
+    ref = np.load(os.path.join(ROOT, "tests", "golden", f"boot_{N}.npy"))
+    for kind in (1, 0):   # auto picks the reference's bootstrapper for these N
+        pos = T.bootstrap_curve(T.default_params(num_segments=N, bootstrap_seed=7, bootstrap_kind=kind), bc)
+        assert pos.shape == ref.shape
+        assert np.array_equal(pos.view(np.uint32), ref.view(np.uint32)), (kind, np.abs(pos - ref).max())
+
+
+def test_reference_bootstrapper_refuses_other_n():
+    bc = T.make_bc((0, 0, 0), (1, 0, 0), (8, 0, 0), (1, 0, 0), 10.0)
+    with pytest.raises(T.TwistyError):
+        T.bootstrap_curve(T.default_params(num_segments=64, bootstrap_kind=1), bc)   # N-2 = 62
+    pos = T.bootstrap_curve(T.default_params(num_segments=64, bootstrap_kind=0), bc)   # auto: the arc
+    seg = np.linalg.norm(np.diff(pos.astype(np.float64), axis=0), axis=1)
+    assert np.allclose(seg, 10.0 / 64, rtol=1e-5)

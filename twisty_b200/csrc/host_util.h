@@ -41,6 +41,16 @@ float min_arclength(const twisty_bc &bc, uint32_t n);
 // |x_{N-1} - x_1| > (N-2) ds.
 bool bootstrap_arc(const twisty_bc &bc, uint32_t n, uint32_t seed, std::vector<float> &pos, std::string &err);
 
+// The reference's recursive bootstrapper (Twisty/PathGeneration.cpp:47-414 from the call at
+// FullExperimentRunnerOptimalPerturb.cpp:122-131) for N with N-2 in {4, 6, 8, 12, 16, 24, 32,
+// 48, ...}: the same random stream and arithmetic, the reference's curve for the same
+// bootstrapSeed. Returns false (err set) for other N or when the placement fails.
+bool bootstrap_resolvable(uint32_t n);
+bool bootstrap_reference(const twisty_bc &bc, uint32_t n, uint32_t seed, std::vector<float> &pos, std::string &err);
+// kind 0: the reference bootstrapper where it resolves N, else the arc; 1: the reference's
+// only; 2: the arc.
+bool bootstrap_curve(const twisty_bc &bc, uint32_t n, uint32_t seed, int kind, std::vector<float> &pos, std::string &err);
+
 // The reference's table, rounding for rounding: WeightLookupTableIntegral ctor + Initialize
 // (Twisty/PathWeightUtils.cpp:281-348) with Integrate's sorted sum (:371-433) and the float
 // phase function (:19-33), on host threads. Bins whose integral cancels to a tiny fraction

@@ -133,6 +133,7 @@ void validate(const twisty_params &p)
     if (p.weight_function != 0) fail(TWISTY_ERR_UNSUPPORTED, "only weightFunction 0 (radiative transfer) is implemented on the device");
     if (p.max_sub_chain < 2) fail(TWISTY_ERR_INVALID_CONFIG, "max_sub_chain must be at least 2");
     if (!(p.max_angle >= 0.0f) || p.max_angle > 3.1415927f) fail(TWISTY_ERR_INVALID_CONFIG, "max_angle must be in [0, pi]");
+    if (p.bootstrap_kind < 0 || p.bootstrap_kind > 2) fail(TWISTY_ERR_INVALID_CONFIG, "bootstrap_kind must be 0, 1 or 2");
 }
 
 void validate_bc(const twisty_bc *bc)
@@ -357,7 +358,7 @@ void prepare(twisty_ctx *ctx, const twisty_bc *bcp)
         pos = ctx->user_curve;
     } else {
         std::string e;
-        if (!bootstrap_arc(bc, N, p.bootstrap_seed, pos, e)) fail(TWISTY_ERR_INFEASIBLE_GEOMETRY, e);
+        if (!bootstrap_curve(bc, N, p.bootstrap_seed, p.bootstrap_kind, pos, e)) fail(TWISTY_ERR_INFEASIBLE_GEOMETRY, e);
     }
     ctx->init_pos_host = pos;
     std::vector<float> seg(3 * (size_t)N);
@@ -899,7 +900,7 @@ twisty_status twisty_bootstrap_curve(const twisty_params *p, const twisty_bc *bc
     std::string e;
     if (p->num_segments < 4) return TWISTY_ERR_INVALID_CONFIG;
     if (!(bc->arclength > 0.0f)) return TWISTY_ERR_INVALID_CONFIG;
-    if (!twisty::bootstrap_arc(*bc, p->num_segments, p->bootstrap_seed, v, e)) {
+    if (!twisty::bootstrap_curve(*bc, p->num_segments, p->bootstrap_seed, p->bootstrap_kind, v, e)) {
         g_free_err = e;
         return TWISTY_ERR_INFEASIBLE_GEOMETRY;
     }
@@ -1026,7 +1027,8 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
         // initial curve
         std::vector<float> pos;
         std::string err;
-        if (!bootstrap_arc(x.bc, N, p.bootstrap_seed + e, pos, err)) fail(TWISTY_ERR_INFEASIBLE_GEOMETRY, exp_msg(e, err));
+        if (!bootstrap_curve(x.bc, N, p.bootstrap_seed + e, p.bootstrap_kind, pos, err))
+            fail(TWISTY_ERR_INFEASIBLE_GEOMETRY, exp_msg(e, err));
         h.seg_off = (uint32_t)segs.size();
         for (uint32_t i = 0; i < N; ++i)
             for (int k = 0; k < 3; ++k) segs.push_back(pos[3 * (i + 1) + k] - pos[3 * i + k]);
