@@ -209,6 +209,15 @@ uint32_t twisty_launch_kernel_count(const twisty_ctx *ctx);
 twisty_status twisty_run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n,
                                uint32_t iterations, twisty_result *res);
 
+/* Independent-sample M-segment Monte Carlo: MSegmentPathGenerationMC
+ * (Experiments/ExperimentBase.cpp:1246-1386). params.paths_to_generate fresh random curves from
+ * the recursive bootstrapper (N-2 in {4, 6, 8, 12, 16, 24, 32, 48, ...}) between the fixed points
+ * of bc, drawn on the device from Philox (seed perturb_seed, stream experiment_id, paths
+ * numbered from chain_offset * paths_to_generate), weighed in the plain (reference FP32) or
+ * compensated form. The estimate is the MEAN weight times the normaliser: res->log10_weight =
+ * res->log10_mean_weight; rel_std_error from the spread of the independent paths. */
+twisty_status twisty_run_msegment(twisty_ctx *ctx, const twisty_bc *bc, twisty_result *res);
+
 /* ------------------------------------------------------------- weighting */
 /* Weigh exported paths: UpdateTangentsFromPos + UpdateCurvaturesFromTangents_RadiativeTransfer
  * + WeightCurveViaCurvatureLog10_CudaSafe (CurvePerturbUtils.cpp:147-166,

@@ -26,6 +26,9 @@
 //   bootstrap <N> <arclength> <12 floats> <seed> <out>
 //             Curve::SetBoundaryConditions + ResolveEvenNumberOfSegments (patched P2)
 //             out: f32 pos[N+1][3]
+//   msegment  <lut> <N> <arclength> <12 floats> <absorption> <seed> <paths> <threads> - <out>
+//             MSegmentPathGenerationMC's per-path work (Experiments/ExperimentBase.cpp:1246-1386)
+//             through the reference's functions; out per path: u8 valid; f64 log10w
 //   chain     <config.json> <initcurve|-> <threads> <paths> <out.json>
 //             The reference's per-thread Markov-chain loop GeometryRandom
 //             (Twisty/FullExperimentRunnerOptimalPerturb.cpp:437-597), orchestrated exactly as
@@ -269,6 +272,63 @@ int mode_bootstrap(int argc, char **argv)
     return 0;
 }
 
+// The reference's independent-sample estimator MSegmentPathGenerationMC
+// (Experiments/ExperimentBase.cpp:1246-1386) driven through the reference's own functions: per
+// thread t a std::mt19937_64(seed + t) and a contiguous block of paths; per path the fixed points
+// of :1253-1260, ResolveEvenNumberOfSegments (patched P2), tangents, curvatures (patched P3)
+// and the reference weigher. A placement the reference would throw on marks the path invalid.
+int mode_msegment(int argc, char **argv)
+{
+    if (argc != 23) return 2;
+    Lut l = load_lut(argv[2]);
+    const uint32_t N = (uint32_t)atoi(argv[3]);
+    const float S = (float)atof(argv[4]);
+    twisty::PerturbUtils::BoundaryConditions bc = bc_from(argv + 5, S);
+    const float absorption = (float)atof(argv[17]);
+    const uint64_t seed = strtoull(argv[18], nullptr, 10);
+    const uint64_t P = strtoull(argv[19], nullptr, 10);
+    const int T = atoi(argv[20]);
+    (void)argv[21];
+    const float ds = bc.arclength / N;
+    const Farlor::Vector3 p0 = bc.m_startPos, p1 = bc.m_startPos + ds * bc.m_startDir;
+    const Farlor::Vector3 pm = bc.m_endPos, pm1 = bc.m_endPos - ds * bc.m_endDir;
+    std::vector<uint8_t> valid(P, 0);
+    std::vector<double> w(P, 0.0);
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; ++t) {
+        th.emplace_back([&, t] {
+            std::mt19937_64 rng(seed + (uint64_t)t);
+            const uint64_t a = P * (uint64_t)t / (uint64_t)T, b = P * (uint64_t)(t + 1) / (uint64_t)T;
+            std::vector<Farlor::Vector3> pts(N + 1), tan(N);
+            std::vector<float> curv(N - 1);
+            for (uint64_t p = a; p < b; ++p) {
+                pts[0] = p0;
+                pts[1] = p1;
+                pts[N - 1] = pm1;
+                pts[N] = pm;
+                try {
+                    twisty::PathGeneration::ResolveEvenNumberOfSegments((int)N - 2, pts, 1, N - 1, ds, rng);
+                } catch (const std::exception &) {
+                    continue;
+                }
+                twisty::PerturbUtils::UpdateTangentsFromPos(pts.data(), tan.data(), N, bc);
+                twisty::PerturbUtils::UpdateCurvaturesFromTangents_RadiativeTransfer(tan.data(), curv.data(), N, bc);
+                twisty::PathWeighting::PathWeightValue r = twisty::PathWeighting::WeightCurveViaCurvatureLog10_CudaSafe(
+                      curv.data(), N - 1, l.v.data(), (int32_t)l.bins, l.ds, l.minK, l.maxK, l.step, absorption);
+                valid[p] = r.isValid ? 1 : 0;
+                w[p] = r.weight;
+            }
+        });
+    }
+    for (auto &x : th) x.join();
+    std::ofstream o(argv[22], std::ios::binary);
+    for (uint64_t p = 0; p < P; ++p) {
+        writev(o, &valid[p], 1);
+        writev(o, &w[p], 1);
+    }
+    return 0;
+}
+
 int mode_chain(int argc, char **argv)
 {
     if (argc != 7) return 2;
@@ -409,6 +469,7 @@ int main(int argc, char **argv)
         else if (m == "norm") rc = mode_norm(argc, argv);
         else if (m == "bootstrap") rc = mode_bootstrap(argc, argv);
         else if (m == "chain") rc = mode_chain(argc, argv);
+        else if (m == "msegment") rc = mode_msegment(argc, argv);
         if (rc == 2) fprintf(stderr, "bad arguments for mode %s\n", m.c_str());
         return rc;
     } catch (std::exception &e) {

@@ -15,6 +15,9 @@ oracle/_ref/ref_harness:
   boot_*.npy       reference bootstrap curves (ResolveEvenNumberOfSegments)
   chain_*.json     full runs of the reference's Markov-chain loop (GeometryRandom) for the
                    statistical comparison, with per-1e6-path chunk sums
+  msegment_*.json  the reference's independent-sample estimator (MSegmentPathGenerationMC's
+                   per-path work through its own functions): mean weight and relative SE
+                   (`--msegment-only` regenerates just these)
 The path batches are perturbed with the oracle's chain runner so they cover curved
 configurations; their weights still come from the reference weigher. This script reads
 the reference tree only through oracle/_ref, and is never run by the tests themselves.
@@ -22,6 +25,7 @@ the reference tree only through oracle/_ref, and is never run by the tests thems
 from __future__ import annotations
 
 import json
+import math
 import os
 import struct
 import subprocess
@@ -100,6 +104,24 @@ def ref_bootstrap(tmp, N, S, seed):
     return np.fromfile(f, F32).reshape(N + 1, 3)
 
 
+def ref_msegment(tmp, N, S, seed, paths, threads, mu, eps, scatter, absorption, nsteps, bins):
+    """The reference's M-segment estimator (harness mode msegment): mean weight and its
+    relative standard error from the spread of the independent paths."""
+    ds = F32(S) / F32(N)
+    ref_lut(tmp, mu, eps, scatter, absorption, nsteps, bins, ds)
+    out = os.path.join(tmp, "ms.bin")
+    run(["msegment", os.path.join(tmp, "lut.bin"), N, repr(float(S)), *bc12(N), repr(absorption), seed, paths,
+         threads, "-", out])
+    b = np.fromfile(out, dtype=np.dtype([("v", "u1"), ("w", "<f8")]))
+    w = b["w"][b["v"] == 1]
+    m = float(w.max())
+    x = 10.0 ** (w - m)
+    mean = float(x.mean())
+    return {"N": N, "S": S, "seed": seed, "paths": paths, "valid": int(w.size), "mu": mu, "eps": eps,
+            "scatter": scatter, "absorption": absorption, "num_steps_int": nsteps, "bins": bins,
+            "log10_mean": m + math.log10(mean), "rel_se": float(x.std(ddof=1) / math.sqrt(x.size) / mean)}
+
+
 def make_config(N, S, paths, skip, seed, mu, eps, scatter, absorption, nsteps, bins, threads):
     g = GEOM[N]
     return {"experiment": {
@@ -115,6 +137,13 @@ def make_config(N, S, paths, skip, seed, mu, eps, scatter, absorption, nsteps, b
                                            "scatter": scatter}}}}
 
 
+def make_msegment(tmp):
+    for N, S in ((10, 5.0), (34, 12.0), (66, 10.0)):
+        ms = ref_msegment(tmp, N, S, 12345, 1 << 22, os.cpu_count() or 1, 1.0, 0.01, 10.0, 0.0, 2000, 1024)
+        with open(os.path.join(OUT, f"msegment_{N}.json"), "w") as f:
+            json.dump(ms, f, indent=1)
+
+
 def main():
     if not os.path.exists(H):
         sys.exit("build the reference first: make -C oracle ref")
@@ -125,6 +154,10 @@ def main():
         for N, S in ((10, 5.0), (18, 6.0), (34, 12.0), (66, 10.0)):
             boots[N] = ref_bootstrap(tmp, N, S, 7)
             np.save(os.path.join(OUT, f"boot_{N}.npy"), boots[N])
+        # ---- independent-sample M-segment estimates (2^22 paths each)
+        make_msegment(tmp)
+        if "--msegment-only" in sys.argv:
+            return
         # ---- tables and weighed path batches
         for name, mu, eps, scatter, absorption, nsteps, bins, N, S in LUTS:
             ds = F32(S) / F32(N)

@@ -125,6 +125,12 @@ class Context:
         _check(_lib().twisty_run(self._h, C.byref(bc), C.byref(r)), self._h)
         return r
 
+    def run_msegment(self, bc: _abi.BC) -> _abi.Result:
+        """Independent-sample M-segment MC: paths_to_generate fresh bootstrap curves, mean weight."""
+        r = _abi.Result()
+        _check(_lib().twisty_run_msegment(self._h, C.byref(bc), C.byref(r)), self._h)
+        return r
+
     def prepare(self, bc: _abi.BC):
         _check(_lib().twisty_prepare(self._h, C.byref(bc)), self._h)
 

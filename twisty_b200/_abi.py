@@ -147,6 +147,7 @@ SIGNATURES = [
     ("twisty_collect", C.c_int, [_P, C.POINTER(Result)]),
     ("twisty_launch_kernel_count", C.c_uint32, [_P]),
     ("twisty_run_batch", C.c_int, [_P, C.POINTER(Experiment), C.c_uint32, C.c_uint32, C.POINTER(Result)]),
+    ("twisty_run_msegment", C.c_int, [_P, C.POINTER(BC), C.POINTER(Result)]),
     ("twisty_weight_paths", C.c_int, [_P, C.POINTER(BC), _P, C.c_uint64, C.c_int32, _P, _P, _P]),
     ("twisty_build_lut", C.c_int, [_P, C.c_float, _P, C.POINTER(LutInfo)]),
     ("twisty_set_lut", C.c_int, [_P, _P, C.POINTER(LutInfo)]),

@@ -185,6 +185,15 @@ cudaError_t launch_weigh_comp(const float *pos, uint64_t n_paths, uint32_t n_seg
                               double log10_absorption, double *log10w, uint8_t *valid, int32_t *bins,
                               cudaStream_t st, LogFixed lf = LogFixed{0.0, 0.0});
 
+// --------------------------------------------- independent-sample paths (msegment.cu)
+// n_paths fresh random curves (the reference's recursive bootstrapper, Philox draws keyed by
+// seed and path0 + i) into pos[n_paths][N+1][3]; N - 2 must be resolvable (4, 6, 8, 12, ...).
+cudaError_t launch_msegment_paths(uint32_t n_segments, float ds, const float p0[3], const float p1[3],
+                                  const float pm1[3], const float pm[3], uint64_t seed, uint32_t experiment,
+                                  uint64_t path0, uint64_t n_paths, float *pos, cudaStream_t st);
+// Per-path weights as one ChainOut each (invalid paths: -inf, failed = 1).
+cudaError_t launch_pack_paths(const double *w, const uint8_t *valid, uint64_t n, ChainOut *out, cudaStream_t st);
+
 // ------------------------------------------------------------ normaliser (norm.cu)
 uint32_t norm_partial_blocks();
 cudaError_t launch_norm_k56(float z, float ds, double *partials, double *out, cudaStream_t st);

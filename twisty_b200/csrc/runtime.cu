@@ -795,6 +795,116 @@ twisty_status twisty_run(twisty_ctx *ctx, const twisty_bc *bc, twisty_result *re
     });
 }
 
+// Independent-sample M-segment Monte Carlo (MSegmentPathGenerationMC,
+// Experiments/ExperimentBase.cpp:1246-1386): fresh random curves from the recursive
+// bootstrapper, weighed with the context's table (plain form: the reference's FP32 semantics;
+// compensated: the fixed-point weigher), the estimate being their mean weight. Paths are built
+// and weighed in chunks of at most 1 GB of positions; each chunk's FP64 reduction treats its
+// paths as independent samples, and the chunks combine by log-sum-exp, errors in quadrature.
+twisty_status twisty_run_msegment(twisty_ctx *ctx, const twisty_bc *bc, twisty_result *res)
+{
+    if (!ctx || !bc || !res) return TWISTY_ERR_INVALID_ARGUMENT;
+    return guard(ctx, [&] {
+        const double t0 = now_ms();
+        const twisty_params p = ctx->p;
+        validate(p);
+        validate_bc(bc);
+        if (p.form == TWISTY_FORM_FP64) fail(TWISTY_ERR_UNSUPPORTED, "M-segment runs weigh in the plain or compensated form");
+        const uint32_t N = p.num_segments;
+        if (!bootstrap_resolvable(N))
+            fail(TWISTY_ERR_UNSUPPORTED, "M-segment paths come from the recursive bootstrapper: N-2 in {4, 6, 8, 12, 16, 24, 32, 48, ...}");
+        set_device(ctx);
+        const float ds = bc->arclength / (float)N;
+        build_tables(ctx, ds, false);
+        const double log10_norm = normalizer_log10(ctx, N, ds, *bc);
+        // the fixed points (ExperimentBase.cpp:1253-1260)
+        const float sp[3] = {bc->start_pos.x, bc->start_pos.y, bc->start_pos.z};
+        const float sd[3] = {bc->start_dir.x, bc->start_dir.y, bc->start_dir.z};
+        const float ep[3] = {bc->end_pos.x, bc->end_pos.y, bc->end_pos.z};
+        const float ed[3] = {bc->end_dir.x, bc->end_dir.y, bc->end_dir.z};
+        float p1[3], pm1[3];
+        for (int k = 0; k < 3; ++k) {
+            p1[k] = sp[k] + ds * sd[k];
+            pm1[k] = ep[k] - ds * ed[k];
+        }
+        const uint64_t total = p.paths_to_generate;
+        const uint64_t per_path = 3 * sizeof(float) * (uint64_t)(N + 1);
+        const uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(total, (1ull << 30) / per_path));
+        cudaStream_t st = ctx->stream;
+        DevBuf dpos, dw, dv, dch, dred;
+        struct Release {
+            DevBuf *b[5];
+            ~Release()
+            {
+                for (DevBuf *x : b) x->release();
+            }
+        } rel{{&dpos, &dw, &dv, &dch, &dred}};
+        ck(dpos.ensure(per_path * chunk), "alloc paths");
+        ck(dw.ensure(sizeof(double) * chunk), "alloc weights");
+        ck(dv.ensure(chunk), "alloc validity");
+        ck(dch.ensure(sizeof(ChainOut) * chunk), "alloc samples");
+        ck(dred.ensure(sizeof(ReduceOut)), "alloc result");
+        const double af = (double)std::exp(-p.absorption * ds);
+        const float inv_ds = (float)N / bc->arclength;
+        const uint64_t seed = seed_of(p.perturb_seed);
+        double m = -std::numeric_limits<double>::infinity(), sum = 0.0, var = 0.0;
+        uint64_t valid = 0, failed = 0;
+        float gpu_ms = 0.f;
+        for (uint64_t done = 0; done < total; done += chunk) {
+            const uint64_t n = std::min(chunk, total - done);
+            ck(cudaEventRecord(ctx->ev[0], st), "event");
+            ck(launch_msegment_paths(N, ds, sp, p1, pm1, ep, seed, p.experiment_id, p.chain_offset * total + done, n,
+                                     dpos.as<float>(), st),
+               "path generation");
+            if (p.form == TWISTY_FORM_PLAIN_FP32)
+                ck(launch_weigh_plain(dpos.as<float>(), n, N, inv_ds, ctx->lut32.as<float>(), ctx->meta, af,
+                                      dw.as<double>(), dv.as<uint8_t>(), nullptr, st),
+                   "weigh kernel");
+            else
+                ck(launch_weigh_comp(dpos.as<float>(), n, N, inv_ds, ctx->fixtab.as<float2>(), ctx->lintab.as<float2>(),
+                                     ctx->exact_blend, ctx->meta, std::log10(af), dw.as<double>(), dv.as<uint8_t>(),
+                                     nullptr, st, ctx->lf),
+                   "weigh kernel");
+            ck(launch_pack_paths(dw.as<double>(), dv.as<uint8_t>(), n, dch.as<ChainOut>(), st), "pack");
+            ck(launch_reduce(dch.as<ChainOut>(), (uint32_t)n, dred.as<ReduceOut>(), st), "reduction");
+            ck(cudaEventRecord(ctx->ev[1], st), "event");
+            ReduceOut r{};
+            ck(cudaMemcpyAsync(&r, dred.p, sizeof(r), cudaMemcpyDeviceToHost, st), "read result");
+            ck(cudaStreamSynchronize(st), "M-segment chunk");
+            float ms = 0.f;
+            ck(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]), "event time");
+            gpu_ms += ms;
+            valid += r.valid;
+            failed += r.failed;
+            if (r.valid && r.log10_sum > -std::numeric_limits<double>::infinity()) {
+                // running log-sum-exp of the chunk sums, absolute standard errors in quadrature
+                const double se = std::isnan(r.rel_se) ? 0.0 : r.rel_se;
+                if (r.log10_sum > m) {
+                    const double f = std::pow(10.0, m - r.log10_sum);
+                    sum *= f;
+                    var *= f * f;
+                    m = r.log10_sum;
+                }
+                const double x = std::pow(10.0, r.log10_sum - m);
+                sum += x;
+                var += (se * x) * (se * x);
+            }
+        }
+        std::memset(res, 0, sizeof(*res));
+        res->log10_normalizer = log10_norm;
+        const double log10_sum = sum > 0 ? m + std::log10(sum) : -std::numeric_limits<double>::infinity();
+        res->log10_mean_weight = valid ? log10_sum - std::log10((double)valid) + log10_norm : -std::numeric_limits<double>::infinity();
+        res->log10_weight = res->log10_mean_weight;   // the estimator is the mean (ExperimentBase.cpp:1378-1381)
+        res->rel_std_error = sum > 0 ? std::sqrt(var) / sum : NAN;
+        res->total_paths = valid;
+        res->failed_paths = failed;
+        res->num_chains = 0;
+        res->steps_per_chain = 0;
+        res->perturb_ms = gpu_ms;
+        res->total_ms = now_ms() - t0;
+    });
+}
+
 twisty_status twisty_weight_paths(twisty_ctx *ctx, const twisty_bc *bc, const float *pos, uint64_t n_paths, int32_t form,
                                   double *log10w, uint8_t *valid, int32_t *bins)
 {
