@@ -64,7 +64,9 @@ typedef enum twisty_lut_mode {
     TWISTY_LUT_FAITHFUL = 0, /* the reference's mixed precision: float phase function, double
                                 Simpson, float table (PathWeightUtils.cpp:19-33,371-433) */
     TWISTY_LUT_FP64 = 1,     /* the same quadrature entirely in double */
-    TWISTY_LUT_EXTERNAL = 2  /* the caller's table, set with twisty_set_lut */
+    TWISTY_LUT_EXTERNAL = 2, /* the caller's table, set with twisty_set_lut */
+    TWISTY_LUT_MULTI_DS = 3  /* the table of the multi-arclength set (twisty_multi_ds_tables)
+                                whose ds is closest to the run's */
 } twisty_lut_mode;
 
 typedef struct twisty_vec3 {
@@ -271,6 +273,15 @@ twisty_status twisty_export_paths(twisty_ctx *ctx, const twisty_bc *bc, const ch
  * (pathwise estimator). grad has 5 entries. */
 twisty_status twisty_adjoint(twisty_ctx *ctx, const twisty_bc *bc, const twisty_result *fwd,
                              double grad[5]);
+
+/* CachedMultiArclengthWeightLookupTable (Twisty/PathWeightUtils.cpp:123-278): n_ds tables for
+ * ds_i = min_ds + i (max_ds - min_ds) / (n_ds - 1) (float arithmetic, :170-173) with the
+ * context's weighting parameters, built in one batched FP64 quadrature on the device, or read
+ * from cache_path when that file holds the same set (written there otherwise; NULL: no file).
+ * Runs and batches with lut_mode TWISTY_LUT_MULTI_DS then take the table whose ds is closest to
+ * their own (GetWeightLookupTable, :230-243: the first of equally close ones), as the
+ * reference's image drivers do; their weighting parameters must be the set's. */
+twisty_status twisty_multi_ds_tables(twisty_ctx *ctx, float min_ds, float max_ds, uint32_t n_ds, const char *cache_path);
 
 /* ---------------------------------------------------------------- autotuner */
 /* No counterpart in the reference. Times every supported compensated-form kernel shape

@@ -21,7 +21,7 @@ from typing import Optional, Sequence
 import numpy as np
 
 from . import _abi
-from ._abi import (FORM_COMPENSATED, FORM_FP64, FORM_PLAIN_FP32, LUT_EXTERNAL, LUT_FAITHFUL,
+from ._abi import (FORM_COMPENSATED, FORM_FP64, FORM_PLAIN_FP32, LUT_EXTERNAL, LUT_FAITHFUL, LUT_MULTI_DS,
                    LUT_FP64)
 
 __all__ = [
@@ -199,6 +199,11 @@ class Context:
         g = (C.c_double * 5)()
         _check(_lib().twisty_adjoint(self._h, C.byref(bc), C.byref(fwd), g), self._h)
         return np.array(list(g))
+
+    def multi_ds_tables(self, min_ds: float, max_ds: float, n_ds: int, cache_path: Optional[str] = None):
+        """Build (or load from cache_path) the multi-arclength table set used by lut_mode LUT_MULTI_DS."""
+        _check(_lib().twisty_multi_ds_tables(self._h, float(min_ds), float(max_ds), int(n_ds),
+                                             cache_path.encode() if cache_path else None), self._h)
 
     def autotune(self, bc: _abi.BC, trial_paths: int = 0) -> dict:
         """Time every compensated-form kernel shape for this context's N; the fastest is

@@ -31,6 +31,7 @@ FORM_FP64 = 2
 LUT_FAITHFUL = 0
 LUT_FP64 = 1
 LUT_EXTERNAL = 2
+LUT_MULTI_DS = 3
 
 
 class Vec3(C.Structure):
@@ -160,6 +161,7 @@ SIGNATURES = [
     ("twisty_adjoint", C.c_int, [_P, C.POINTER(BC), C.POINTER(Result), C.POINTER(C.c_double)]),
     ("twisty_run_noalloc", C.c_int, [C.POINTER(NoAllocArgs), _P]),
     ("twisty_autotune", C.c_int, [_P, C.POINTER(BC), C.c_uint64, C.POINTER(Tuning)]),
+    ("twisty_multi_ds_tables", C.c_int, [_P, C.c_float, C.c_float, C.c_uint32, C.c_char_p]),
     ("twisty_tuning_cache_save", C.c_int, [C.c_char_p]),
     ("twisty_tuning_cache_load", C.c_int, [C.c_char_p]),
 ]

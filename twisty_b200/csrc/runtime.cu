@@ -98,6 +98,19 @@ struct twisty_ctx {
     LogFixed lf{0.0, 0.0, 0, 0};   // fixed-point form of fixtab; inv_scale 0 when exact_blend
     std::vector<float> ext_lut;
     twisty_lut_info ext_info{};
+    // multi-arclength table set (twisty_multi_ds_tables)
+    struct MultiDs {
+        bool ready = false;
+        uint32_t gen = 0;          // bumped on every rebuild: part of the table cache key
+        uint32_t n = 0, bins = 0;
+        float min_ds = 0, max_ds = 0;
+        float wp[9] = {};          // the weighting parameters the set was built for
+        std::vector<float> ds;     // per table
+        std::vector<LutMetaF> meta;
+        std::vector<double> min_w, max_w;
+        std::vector<float> host;   // [n][bins]
+        DevBuf dev;                // [n][bins] float
+    } multi;
 
     // the prepared experiment
     bool prepared = false;
@@ -128,7 +141,7 @@ void validate(const twisty_params &p)
         fail(TWISTY_ERR_INVALID_CONFIG, "numStepsInt must be even and at least 4");
     if (p.lut_mode != TWISTY_LUT_EXTERNAL && !(p.eps > 0.0f)) fail(TWISTY_ERR_INVALID_CONFIG, "weighting.eps must be positive");
     if (p.form < 0 || p.form > 2) fail(TWISTY_ERR_INVALID_CONFIG, "unknown form");
-    if (p.lut_mode < 0 || p.lut_mode > 2) fail(TWISTY_ERR_INVALID_CONFIG, "unknown lut_mode");
+    if (p.lut_mode < 0 || p.lut_mode > 3) fail(TWISTY_ERR_INVALID_CONFIG, "unknown lut_mode");
     if (p.perturb_method != 0) fail(TWISTY_ERR_UNSUPPORTED, "only perturbMethod 0 (GeometricRandom) runs; the reference exits on the others");
     if (p.weight_function != 0) fail(TWISTY_ERR_UNSUPPORTED, "only weightFunction 0 (radiative transfer) is implemented on the device");
     if (p.max_sub_chain < 2) fail(TWISTY_ERR_INVALID_CONFIG, "max_sub_chain must be at least 2");
@@ -188,6 +201,44 @@ bool tune_lookup(const std::string &device, uint32_t n, uint32_t bins, CompTunin
 }
 
 // ------------------------------------------------------------------ tables
+void weighting_fingerprint(const twisty_params &p, float wp[9])
+{
+    wp[0] = p.mu;
+    wp[1] = p.eps;
+    wp[2] = p.scatter;
+    wp[3] = p.absorption;
+    wp[4] = (float)p.num_steps_int;
+    wp[5] = (float)p.num_curvature_steps;
+    wp[6] = p.min_bound;
+    wp[7] = p.max_bound;
+    wp[8] = p.bias;
+}
+
+// GetWeightLookupTable (Twisty/PathWeightUtils.cpp:230-243): the first table with the smallest
+// |ds_i - ds| (float).
+uint32_t multi_closest(const twisty_ctx *ctx, float ds)
+{
+    float best = std::numeric_limits<float>::max();
+    uint32_t arg = 0;
+    for (uint32_t i = 0; i < ctx->multi.n; ++i) {
+        const float d = std::abs(ctx->multi.ds[i] - ds);
+        if (d < best) {
+            best = d;
+            arg = i;
+        }
+    }
+    return arg;
+}
+
+void check_multi(const twisty_ctx *ctx, const twisty_params &p)
+{
+    if (!ctx->multi.ready) fail(TWISTY_ERR_LUT_INVALID, "lut_mode MULTI_DS needs twisty_multi_ds_tables first");
+    float wp[9];
+    weighting_fingerprint(p, wp);
+    if (std::memcmp(wp, ctx->multi.wp, sizeof(wp)) != 0)
+        fail(TWISTY_ERR_LUT_INVALID, "the multi-ds tables were built for other weighting parameters");
+}
+
 void build_tables(twisty_ctx *ctx, float ds, bool derivatives)
 {
     const twisty_params &p = ctx->p;
@@ -206,7 +257,7 @@ void build_tables(twisty_ctx *ctx, float ds, bool derivatives)
     key[1] = ((uint64_t)f[0] << 32) | f[1];
     key[2] = ((uint64_t)f[2] << 32) | f[3];
     key[3] = ((uint64_t)f[4] << 32) ^ ((uint64_t)f[5]) ^ ((uint64_t)bins << 8) ^ ((uint64_t)p.num_steps_int << 40) ^
-             (derivatives ? 1ull : 0ull);
+             (derivatives ? 1ull : 0ull) ^ (p.lut_mode == TWISTY_LUT_MULTI_DS ? ((uint64_t)ctx->multi.gen << 1) : 0ull);
     if (ctx->lut_ready && std::memcmp(key, ctx->lut_key, sizeof(key)) == 0) return;
     ctx->lut_ready = false;
     cudaStream_t st = ctx->stream;
@@ -215,7 +266,20 @@ void build_tables(twisty_ctx *ctx, float ds, bool derivatives)
     ck(ctx->lintab.ensure(sizeof(float2) * bins), "alloc linear table");
     ck(ctx->lutaux.ensure(sizeof(double) * 4), "alloc table scratch");
     std::vector<float> host32(bins);
-    if (p.lut_mode == TWISTY_LUT_EXTERNAL) {
+    if (p.lut_mode == TWISTY_LUT_MULTI_DS) {
+        if (derivatives) fail(TWISTY_ERR_UNSUPPORTED, "derivative tables need lut_mode FP64");
+        check_multi(ctx, p);
+        const uint32_t i = multi_closest(ctx, ds);
+        std::memcpy(host32.data(), ctx->multi.host.data() + (size_t)i * bins, sizeof(float) * bins);
+        ctx->meta = ctx->multi.meta[i];
+        ctx->min_w = ctx->multi.min_w[i];
+        ctx->max_w = ctx->multi.max_w[i];
+        ck(ctx->lut64.ensure(sizeof(double) * bins), "alloc table");
+        std::vector<double> h64(host32.begin(), host32.end());
+        ck(cudaMemcpyAsync(ctx->lut32.p, host32.data(), sizeof(float) * bins, cudaMemcpyHostToDevice, st), "upload table");
+        ck(cudaMemcpyAsync(ctx->lut64.p, h64.data(), sizeof(double) * bins, cudaMemcpyHostToDevice, st), "upload table");
+        ck(cudaStreamSynchronize(st), "sync");
+    } else if (p.lut_mode == TWISTY_LUT_EXTERNAL) {
         if (ctx->ext_lut.size() != bins) fail(TWISTY_ERR_LUT_INVALID, "no external table of numCurvatureSteps entries was set (twisty_set_lut)");
         host32 = ctx->ext_lut;
         ctx->meta = LutMetaF{ctx->ext_info.min_curvature, ctx->ext_info.max_curvature, ctx->ext_info.curvature_step, (int32_t)bins};
@@ -741,7 +805,7 @@ void twisty_destroy(twisty_ctx *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     DevBuf *bufs[] = {&ctx->lut64, &ctx->lut32, &ctx->fixtab, &ctx->lintab, &ctx->dmus, &ctx->deps, &ctx->lutaux,
                       &ctx->init_pos, &ctx->init_seg, &ctx->state, &ctx->chain_out, &ctx->partials, &ctx->reduce_out,
-                      &ctx->norm_scratch};
+                      &ctx->norm_scratch, &ctx->multi.dev};
     for (DevBuf *b : bufs) b->release();
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
@@ -1077,8 +1141,11 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
         validate(pv);
     }
     if (p.form != TWISTY_FORM_COMPENSATED) fail(TWISTY_ERR_UNSUPPORTED, "batched runs use the compensated form");
-    if (p.lut_mode != TWISTY_LUT_FP64)
-        fail(TWISTY_ERR_UNSUPPORTED, "batched runs build their tables on the device (lut_mode FP64)");
+    if (p.lut_mode != TWISTY_LUT_FP64 && p.lut_mode != TWISTY_LUT_MULTI_DS)
+        fail(TWISTY_ERR_UNSUPPORTED, "batched runs build their tables on the device (lut_mode FP64) or take them "
+                                     "from the multi-ds set (lut_mode MULTI_DS)");
+    const bool multi = p.lut_mode == TWISTY_LUT_MULTI_DS;
+    if (multi) check_multi(ctx, p);
     if (n > 65535u) fail(TWISTY_ERR_INVALID_ARGUMENT, "at most 65535 experiments per batch");
     set_device(ctx);
     for (uint32_t e = 0; e < n; ++e) std::memset(&res[e], 0, sizeof(twisty_result));
@@ -1094,6 +1161,7 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
         uint32_t seg_off, chain_off;
         double log10_norm;
         LutMetaF meta;
+        uint32_t multi_index;
     };
     std::vector<ExpHost> eh(n);
     std::vector<LutBuildSpec> specs(n);
@@ -1118,6 +1186,12 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
         // maxBound = 10/eps per experiment (ExperimentRunner.cpp:169-171)
         const float max_k = (float)((2.0 / (double)h.ds) * (double)1.01f);
         h.meta = LutMetaF{0.0f, max_k, max_k / (float)(bins - 1), (int32_t)bins};
+        if (multi) {
+            if (x.eps != p.eps || x.scatter != p.scatter)
+                fail(TWISTY_ERR_LUT_INVALID, exp_msg(e, "lut_mode MULTI_DS needs the set's eps and scatter"));
+            h.multi_index = multi_closest(ctx, h.ds);
+            h.meta = ctx->multi.meta[h.multi_index];
+        }
         LutBuildSpec &ls = specs[e];
         ls = LutBuildSpec{};
         ls.mu = p.mu;
@@ -1196,8 +1270,16 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
     ck(cudaMemcpyAsync(B.specs.p, specs.data(), sizeof(LutBuildSpec) * n, cudaMemcpyHostToDevice, st), "upload specs");
     ck(cudaMemcpyAsync(B.steps.p, steps.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st), "upload");
     ck(cudaMemcpyAsync(B.nsegs.p, nsegs.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, st), "upload");
-    ck(launch_lut_build_batch(B.specs.as<LutBuildSpec>(), n, bins, B.lut64.as<double>(), st), "batch table build");
-    ck(launch_lut_finalize_batch(n, bins, B.lut64.as<double>(), B.lut32.as<float>(), nullptr, st), "batch table finalize");
+    if (multi) {
+        for (uint32_t e = 0; e < n; ++e)
+            ck(cudaMemcpyAsync(B.lut32.as<float>() + (size_t)e * bins, ctx->multi.dev.as<float>() + (size_t)eh[e].multi_index * bins,
+                               sizeof(float) * bins, cudaMemcpyDeviceToDevice, st),
+               "multi-ds table");
+    } else {
+        ck(launch_lut_build_batch(B.specs.as<LutBuildSpec>(), n, bins, B.lut64.as<double>(), st), "batch table build");
+        ck(launch_lut_finalize_batch(n, bins, B.lut64.as<double>(), B.lut32.as<float>(), nullptr, st),
+           "batch table finalize");
+    }
     ck(launch_comp_tables_batch(n, bins, B.lut32.as<float>(), B.steps.as<float>(), B.nsegs.as<uint32_t>(),
                                 B.fix.as<float2>(), B.lin.as<float2>(), B.lf.as<LogFixed>(), B.ok.as<int>(), st),
        "batch compensated tables");
@@ -1644,4 +1726,122 @@ twisty_status twisty_tuning_cache_load(const char *path)
     }
     for (const TuneEntry &e : got) tune_record(e);
     return TWISTY_OK;
+}
+
+// ------------------------------------------------------------ multi-arclength tables
+namespace {
+constexpr uint32_t kMultiMagic = 0x444D5754u;   // "TWMD"
+constexpr uint32_t kMultiVersion = 1;
+}  // namespace
+
+twisty_status twisty_multi_ds_tables(twisty_ctx *ctx, float min_ds, float max_ds, uint32_t n_ds, const char *cache_path)
+{
+    if (!ctx) return TWISTY_ERR_INVALID_ARGUMENT;
+    return guard(ctx, [&] {
+        const twisty_params &p = ctx->p;
+        if (n_ds < 2 || n_ds > 65535u || !(min_ds > 0.0f) || !(max_ds > min_ds))
+            fail(TWISTY_ERR_INVALID_ARGUMENT, "need 2 <= n_ds <= 65535 and 0 < min_ds < max_ds");
+        if (p.num_curvature_steps < 2 || p.num_steps_int < 4 || (p.num_steps_int & 1u) || !(p.eps > 0.0f))
+            fail(TWISTY_ERR_INVALID_CONFIG, "invalid weighting parameters");
+        set_device(ctx);
+        auto &M = ctx->multi;
+        M.ready = false;
+        M.n = n_ds;
+        M.bins = p.num_curvature_steps;
+        M.min_ds = min_ds;
+        M.max_ds = max_ds;
+        weighting_fingerprint(p, M.wp);
+        const uint32_t bins = M.bins;
+        // ds grid of the reference (:170-173)
+        const float step_ds = (max_ds - min_ds) / (float)(n_ds - 1);
+        M.ds.resize(n_ds);
+        M.meta.resize(n_ds);
+        for (uint32_t i = 0; i < n_ds; ++i) {
+            M.ds[i] = min_ds + (float)i * step_ds;
+            const float max_k = (float)((2.0 / (double)M.ds[i]) * (double)1.01f);
+            M.meta[i] = LutMetaF{0.0f, max_k, max_k / (float)(bins - 1), (int32_t)bins};
+        }
+        M.host.assign((size_t)n_ds * bins, 0.0f);
+        M.min_w.assign(n_ds, 0.0);
+        M.max_w.assign(n_ds, 0.0);
+        bool loaded = false;
+        if (cache_path) {
+            std::ifstream f(cache_path, std::ios::binary);
+            uint32_t hdr[4] = {0, 0, 0, 0};
+            float wp[9], rng[2];
+            if (f && f.read(reinterpret_cast<char *>(hdr), sizeof(hdr)) && f.read(reinterpret_cast<char *>(wp), sizeof(wp)) &&
+                f.read(reinterpret_cast<char *>(rng), sizeof(rng)) && hdr[0] == kMultiMagic && hdr[1] == kMultiVersion &&
+                hdr[2] == n_ds && hdr[3] == bins && std::memcmp(wp, M.wp, sizeof(wp)) == 0 && rng[0] == min_ds &&
+                rng[1] == max_ds) {
+                f.read(reinterpret_cast<char *>(M.min_w.data()), sizeof(double) * n_ds);
+                f.read(reinterpret_cast<char *>(M.max_w.data()), sizeof(double) * n_ds);
+                f.read(reinterpret_cast<char *>(M.host.data()), sizeof(float) * M.host.size());
+                loaded = (bool)f;
+            }
+        }
+        cudaStream_t st = ctx->stream;
+        ck(M.dev.ensure(sizeof(float) * M.host.size()), "alloc multi-ds tables");
+        if (loaded) {
+            ck(cudaMemcpyAsync(M.dev.p, M.host.data(), sizeof(float) * M.host.size(), cudaMemcpyHostToDevice, st), "upload");
+            ck(cudaStreamSynchronize(st), "upload");
+        } else {
+            std::vector<LutBuildSpec> specs(n_ds);
+            for (uint32_t i = 0; i < n_ds; ++i) {
+                LutBuildSpec &s = specs[i];
+                s = LutBuildSpec{};
+                s.mu = p.mu;
+                s.eps = p.eps;
+                s.scatter = p.scatter;
+                s.min_bound = p.min_bound;
+                s.max_bound = p.max_bound;
+                s.bias = p.bias;
+                s.num_steps_int = p.num_steps_int;
+                s.bins = bins;
+                s.ds = M.ds[i];
+                s.min_k = 0.0f;
+                s.step = M.meta[i].step;
+                s.step64 = ((2.0 / (double)M.ds[i]) * 1.01) / (double)(bins - 1);
+            }
+            DevBuf dspecs, d64, dmm;
+            struct Release {
+                DevBuf *b[3];
+                ~Release()
+                {
+                    for (DevBuf *x : b) x->release();
+                }
+            } rel{{&dspecs, &d64, &dmm}};
+            ck(dspecs.ensure(sizeof(LutBuildSpec) * n_ds), "alloc");
+            ck(d64.ensure(sizeof(double) * M.host.size()), "alloc");
+            ck(dmm.ensure(sizeof(double) * 3 * n_ds), "alloc");
+            ck(cudaMemcpyAsync(dspecs.p, specs.data(), sizeof(LutBuildSpec) * n_ds, cudaMemcpyHostToDevice, st), "upload");
+            ck(launch_lut_build_batch(dspecs.as<LutBuildSpec>(), n_ds, bins, d64.as<double>(), st), "multi-ds build");
+            ck(launch_lut_finalize_batch(n_ds, bins, d64.as<double>(), M.dev.as<float>(), dmm.as<double>(), st),
+               "multi-ds finalize");
+            std::vector<double> mm(3 * (size_t)n_ds);
+            ck(cudaMemcpyAsync(M.host.data(), M.dev.p, sizeof(float) * M.host.size(), cudaMemcpyDeviceToHost, st), "read");
+            ck(cudaMemcpyAsync(mm.data(), dmm.p, sizeof(double) * mm.size(), cudaMemcpyDeviceToHost, st), "read");
+            ck(cudaStreamSynchronize(st), "multi-ds tables");
+            for (uint32_t i = 0; i < n_ds; ++i) {
+                M.min_w[i] = mm[3 * i];
+                M.max_w[i] = mm[3 * i + 1];
+            }
+            if (cache_path) {
+                std::ofstream f(cache_path, std::ios::binary);
+                const uint32_t hdr[4] = {kMultiMagic, kMultiVersion, n_ds, bins};
+                const float rng[2] = {min_ds, max_ds};
+                f.write(reinterpret_cast<const char *>(hdr), sizeof(hdr));
+                f.write(reinterpret_cast<const char *>(M.wp), sizeof(M.wp));
+                f.write(reinterpret_cast<const char *>(rng), sizeof(rng));
+                f.write(reinterpret_cast<const char *>(M.min_w.data()), sizeof(double) * n_ds);
+                f.write(reinterpret_cast<const char *>(M.max_w.data()), sizeof(double) * n_ds);
+                f.write(reinterpret_cast<const char *>(M.host.data()), sizeof(float) * M.host.size());
+                if (!f) fail(TWISTY_ERR_IO, std::string("cannot write ") + cache_path);
+            }
+        }
+        for (size_t i = 0; i < M.host.size(); ++i)
+            if (!std::isfinite(M.host[i])) fail(TWISTY_ERR_LUT_INVALID, "multi-ds table has non-finite entries");
+        ++M.gen;
+        M.ready = true;
+        ctx->lut_ready = false;
+    });
 }
