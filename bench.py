@@ -158,6 +158,17 @@ def batch_experiments(T, n=None, seed=None):
     return out
 
 
+# Image workload: 64 x 64 receivers on the plane z = 10, x, y in [-4, 4], tangent (0, 0, 1),
+# source at the origin with tangent (0, 0, 1), N = 512, S = 1.3 x distance, sigma = 0.15,
+# mu_s = 20, 2^22 paths per pixel; the pixels share sigma and mu_s, so their tables come from
+# one multi-arclength set of 256 tables over the pixels' ds range.
+IMAGE = dict(nx=64, ny=64, half=4.0, z=10.0, N=512, sigma=0.15, scatter=20.0, paths=1 << 22, bins=4096,
+             num_steps_int=2000, n_ds=256, k_max=32, max_angle=0.05, burn_in=64, seed=1234)
+IMAGE_NAME = ("image: 64x64 receivers on z=10, x,y in [-4,4], tangent (0,0,1), N=512, S=1.3*distance, "
+              "sigma=0.15, mu_s=20, 2^22 paths per pixel, 256-table multi-arclength set, k~U{2..32}, "
+              "angle~U(-0.05,0.05), Philox seed 1234")
+
+
 def batch_params(T, device=0):
     return T.default_params(num_segments=16, mu=BATCH["mu"], eps=0.01, scatter=10.0, absorption=0.0,
                             num_steps_int=BATCH["num_steps_int"], num_curvature_steps=BATCH["bins"],
@@ -273,6 +284,67 @@ def run_reference_arm(args):
     return 0
 
 
+def run_image_workload(args, T, torch, device, ws, rank, pg):
+    """The image workload through the receiver-grid driver and twisty_run_batch, tables from a
+    multi-arclength set (twisty_multi_ds_tables)."""
+    from twisty_b200 import drivers
+    I = IMAGE
+    paths = args.paths or I["paths"]
+    eps = float(np.float32(I["sigma"]) * np.float32(I["sigma"]))
+    exps = drivers.image_plane_experiments(I["nx"], I["ny"], I["half"], I["z"], I["N"], I["scatter"], eps, paths)
+    ds = [e.bc.arclength / I["N"] for e in exps]
+    params = T.default_params(num_segments=I["N"], mu=1.0, eps=eps, scatter=I["scatter"], absorption=0.0,
+                              num_steps_int=I["num_steps_int"], num_curvature_steps=I["bins"],
+                              paths_to_skip=I["burn_in"], perturb_seed=I["seed"], bootstrap_seed=7,
+                              max_sub_chain=I["k_max"], max_angle=I["max_angle"], form=T.FORM_COMPENSATED,
+                              lut_mode=T.LUT_MULTI_DS, device=device, chain_offset=rank * 1_000_000)
+    ctx = T.Context(params)
+    t0 = time.perf_counter()
+    ctx.multi_ds_tables(min(ds), max(ds), I["n_ds"])
+    tables_ms = (time.perf_counter() - t0) * 1e3
+    ctx.run_batch(exps, iterations=max(1, args.warmup))
+    with ClockSampler(device) as clk:
+        res = ctx.run_batch(exps, iterations=args.steps)
+    launches = ctx.kernels_per_launch()
+    per_step = res[0].perturb_ms
+    if pg:
+        pg.barrier()
+    t0 = time.perf_counter()
+    ctx.run_batch(exps, iterations=1)
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+    if pg:
+        t = torch.tensor([per_step, e2e_ms], dtype=torch.float64, device=f"cuda:{device}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        per_step, e2e_ms = t.tolist()
+    ctx.close()
+    done = sum(r.total_paths * I["N"] for r in res)
+    value = done * ws / (per_step / 1e3)
+    peaks = load_peaks()
+    sm_max = peaks.get("sm_max_mhz", 1965.0)
+    peak_ti = SMS * LANES_PER_SM * sm_max * 1e6 / 1e12
+    achieved_ti = INSTR_PER_SEGMENT * done / (per_step / 1e3) / 1e12
+    if rank == 0:
+        import ctypes
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": per_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32 (f64 cross-chain)", "data": "synthetic",
+                "config": {"workload": IMAGE_NAME, "form": "compensated", "experiments": len(exps),
+                           "paths_per_pixel": paths, "path_segments_per_step": done, "multi_ds_tables_ms": tables_ms,
+                           "l2": "inputs larger than L2 per step (4096 chains' state per pixel batch, 256 tables)",
+                           "parallelism": f"independent chains x{ws}"},
+                "e2e": {"value": done * ws / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms,
+                        "h2d_bytes_per_step": ctypes.sizeof(T._abi.Experiment) * len(exps),
+                        "d2h_bytes_per_step": ctypes.sizeof(T._abi.Result) * len(exps)},
+                "roofline": {"bound": "fp32", "kernel": "batch_kernel", "achieved": achieved_ti, "peak": peak_ti,
+                             "unit": "Tinstr/s", "frac": achieved_ti / peak_ti, "traffic": None,
+                             "basis": f"{INSTR_PER_SEGMENT:g} FP32 instructions per path-segment"},
+                "cpu_baseline": None, "clocks": clk.summary(), "gpu_launches": launches * args.steps}
+        print(json.dumps(line))
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
 def run_batch_workload(args, T, torch, device, ws, rank, pg):
     """The batching workload through twisty_run_batch: every rank runs all experiments on its own
     chain range (chain_offset), and the per-experiment results combine across ranks."""
@@ -339,13 +411,14 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP32 drop-in")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--paths", type=int, default=0, help="paths per pass (default 2^26; smaller for profiling)")
-    ap.add_argument("--workload", default="precision", choices=["precision", "batch"],
-                    help="precision: one N=256 experiment (the headline); batch: 4096 uneven experiments")
+    ap.add_argument("--workload", default="precision", choices=["precision", "batch", "image"],
+                    help="precision: one N=256 experiment (the headline); batch: 4096 uneven experiments; "
+                         "image: 64x64 receiver grid at N=512 from a multi-arclength table set")
     ap.add_argument("--experiments", type=int, default=0, help="batch workload: number of experiments (default 4096)")
     args = ap.parse_args()
     if args.experiments:
         BATCH["n"] = args.experiments
-    if args.paths:
+    if args.paths and args.workload == "precision":
         W["paths"] = args.paths
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -364,6 +437,8 @@ def main():
         pg = dist
     if args.workload == "batch":
         return run_batch_workload(args, T, torch, device, ws, rank, pg)
+    if args.workload == "image":
+        return run_image_workload(args, T, torch, device, ws, rank, pg)
     form = {"compensated": T.FORM_COMPENSATED, "plain": T.FORM_PLAIN_FP32, "fp64": T.FORM_FP64}[args.form]
     bc = workload_bc(T)
 
