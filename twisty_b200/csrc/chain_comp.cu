@@ -469,24 +469,30 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
             }
             // chord x_right - x_left = sum of l_s t_s over the k segments left .. right-1
             constexpr int R = (kMaxSubChain + G - 1) / G;
-            float vx[R], vy[R], vz[R];
-            uint32_t va[R], vb[R];
+            // more than 4 rounds (8-lane groups) under the 64-register budget of 1024-thread
+            // CTAs (SPL < 16): the rotation pass reloads its tangents instead of keeping every
+            // round's in registers (measured: no spills, N <= 64 up to 27 % faster)
+            constexpr bool RELOAD = R > 4 && SPL < 16;
+            constexpr int RK = RELOAD ? 1 : R;
+            float vx[RK], vy[RK], vz[RK];
+            uint32_t va[RK], vb[RK];
             float cx = 0.f, cy = 0.f, cz = 0.f;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 if (r > 0 && (uint32_t)r >= rounds) break;
                 const uint32_t s = left + j + r * G;
-                va[r] = Lay::xy(gbase + s / SPL, s % SPL);
-                vb[r] = Lay::z(gbase + s / SPL, s % SPL);
+                const int ri = RELOAD ? 0 : r;
+                va[ri] = Lay::xy(gbase + s / SPL, s % SPL);
+                vb[ri] = Lay::z(gbase + s / SPL, s % SPL);
                 if (s < right) {
-                    const float2 a = st.xy[va[r]];
-                    vx[r] = a.x;
-                    vy[r] = a.y;
-                    vz[r] = st.z[vb[r]];
-                    const float l = st.l[vb[r]];
-                    cx = fmaf(l, vx[r], cx);
-                    cy = fmaf(l, vy[r], cy);
-                    cz = fmaf(l, vz[r], cz);
+                    const float2 a = st.xy[va[ri]];
+                    vx[ri] = a.x;
+                    vy[ri] = a.y;
+                    vz[ri] = st.z[vb[ri]];
+                    const float l = st.l[vb[ri]];
+                    cx = fmaf(l, vx[ri], cx);
+                    cy = fmaf(l, vy[ri], cy);
+                    cz = fmaf(l, vz[ri], cz);
                 }
             }
             if constexpr (G == 32) {
@@ -513,16 +519,27 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
             for (int r = 0; r < R; ++r) {
                 if (r > 0 && (uint32_t)r >= rounds) break;
                 const uint32_t s = left + j + r * G;
+                const int ri = RELOAD ? 0 : r;
+                if (RELOAD) {
+                    va[0] = Lay::xy(gbase + s / SPL, s % SPL);
+                    vb[0] = Lay::z(gbase + s / SPL, s % SPL);
+                }
                 if (s < right) {
-                    const float x = vx[r], y = vy[r], z = vz[r];
+                    if (RELOAD) {
+                        const float2 a = st.xy[va[0]];
+                        vx[0] = a.x;
+                        vy[0] = a.y;
+                        vz[0] = st.z[vb[0]];
+                    }
+                    const float x = vx[ri], y = vy[ri], z = vz[ri];
                     const float crx = ay * z - az * y, cry = az * x - ax * z, crz = ax * y - ay * x;
                     const float ad = (ax * x + ay * y + az * z) * omc;
                     const float nx = fmaf(ax, ad, fmaf(sth, crx, fmaf(-omc, x, x)));
                     const float ny = fmaf(ay, ad, fmaf(sth, cry, fmaf(-omc, y, y)));
                     const float nz = fmaf(az, ad, fmaf(sth, crz, fmaf(-omc, z, z)));
                     const float h = fmaf(-0.5f, fmaf(nx, nx, fmaf(ny, ny, nz * nz)), 1.5f);
-                    st.xy[va[r]] = make_float2(nx * h, ny * h);
-                    st.z[vb[r]] = nz * h;
+                    st.xy[va[ri]] = make_float2(nx * h, ny * h);
+                    st.z[vb[ri]] = nz * h;
                 }
             }
             __syncwarp();
