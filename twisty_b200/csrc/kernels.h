@@ -151,7 +151,11 @@ struct BatchShape {
     int group, spl, warps;
     int exact;               // tables are (L_i, L_{i+1}-L_i) with a log2 per segment
     int lut_smem;            // stage each item's table in shared memory (else read through L1)
+    int clamp;               // some table's curvature range can be left (else no clamping code)
 };
+// Whether curvatures of paths with this N/S can leave the table (it does not cover
+// [0, 2 N/S] from 0): such tables need the clamping kernel variants.
+bool comp_table_needs_clamp(float inv_ds, const LutMetaF &m);
 struct BatchExpHost {
     ChainSpec spec;
     LutMetaF meta;

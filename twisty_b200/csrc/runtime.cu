@@ -1303,7 +1303,8 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
     std::vector<Bucket> buckets;
     auto bucket_of = [&](const BatchShape &sh) -> Bucket & {
         for (Bucket &b : buckets)
-            if (b.shape.group == sh.group && b.shape.spl == sh.spl && b.shape.warps == sh.warps && b.shape.exact == sh.exact)
+            if (b.shape.group == sh.group && b.shape.spl == sh.spl && b.shape.warps == sh.warps && b.shape.exact == sh.exact &&
+                b.shape.clamp == sh.clamp && b.shape.lut_smem == sh.lut_smem)
                 return b;
         buckets.push_back(Bucket{});
         buckets.back().shape = sh;
@@ -1319,7 +1320,8 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
         b.tab = (exact ? B.lin.as<float2>() : B.fix.as<float2>()) + (size_t)e * bins;
         b.init_seg = B.init_seg.as<float>() + h.seg_off;
         b.out_offset = h.chain_off;
-        BatchShape sh{h.t.group, h.t.spl, h.t.warps_per_block, exact ? 1 : 0, 1};
+        BatchShape sh{h.t.group, h.t.spl, h.t.warps_per_block, exact ? 1 : 0, 1,
+                      (exact || comp_table_needs_clamp(h.spec.inv_ds, h.meta)) ? 1 : 0};
         if (batch_smem_bytes(sh, bins) > 227 * 1024) sh.lut_smem = 0;
         if (!batch_shape_supported(sh, h.N, h.spec.k_eff) || batch_smem_bytes(sh, bins) > 227 * 1024)
             fail(TWISTY_ERR_UNSUPPORTED, exp_msg(e, "no batched kernel shape fits"));
