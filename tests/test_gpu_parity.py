@@ -54,6 +54,26 @@ def test_fp64_table_matches_oracle_twin(oracle, name):
     assert np.max(np.abs(lut - ref) / ref) < 1.2e-7
 
 
+def test_batched_fp64_tables_match_oracle_twin(oracle, tmp_path):
+    """The batched builder (one launch for a set of tables, read back from the multi-ds cache
+    file) on a narrow-phase set (sigma = 0.05) whose high-curvature tail is replaced by the
+    smallest positive entry, and a broad one."""
+    for mu, eps, sc, nst, bins, lo, hi, n_ds in ((1.0, 0.0025, 5.0, 2000, 4096, 0.0195, 0.05, 3),
+                                                  (1.0, 0.09, 50.0, 2000, 2048, 0.1, 0.3, 3)):
+        p = T.default_params(num_segments=64, mu=mu, eps=eps, scatter=sc, num_steps_int=nst, num_curvature_steps=bins,
+                             lut_mode=T.LUT_MULTI_DS)
+        path = tmp_path / f"set_{eps}.twmd"
+        with T.Context(p) as ctx:
+            ctx.multi_ds_tables(lo, hi, n_ds, str(path))
+        raw = path.read_bytes()
+        tabs = np.frombuffer(raw, np.float32, offset=60 + 16 * n_ds).reshape(n_ds, bins)
+        step = (F32(hi) - F32(lo)) / F32(n_ds - 1)
+        for i in range(n_ds):
+            ds = F32(lo) + F32(i) * step
+            ref, _ = oracle.lut_f64(oracle.wparams(mu, eps, sc, 0.0, nst, bins), float(ds))
+            assert np.max(np.abs(tabs[i] - ref) / ref) < 1.2e-7, (eps, i)
+
+
 # ------------------------------------------------------------------------ weighting
 @pytest.mark.parametrize("name", sorted(LUT_SETS))
 def test_plain_weigher_matches_reference(name):

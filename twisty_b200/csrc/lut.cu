@@ -2,11 +2,13 @@
 //
 // The reference builds its table with an OpenMP loop over bins, each bin a composite
 // Simpson quadrature of IntegrandRT whose terms are sorted then summed
-// (Twisty/PathWeightUtils.cpp:281-433). Here one CTA integrates one bin: every thread
-// takes a strided share of the nodes and keeps a Neumaier-compensated FP64 sum, and the
-// CTA combines the partial sums pairwise. The compensated sum replaces the sort (it is
-// at least as accurate), so the float table matches the reference's to within one float
-// ulp rather than bit for bit.
+// (Twisty/PathWeightUtils.cpp:281-433). The faithful form and the derivative tables use one
+// CTA per bin: every thread takes a strided share of the nodes and keeps a
+// Neumaier-compensated FP64 sum, and the CTA combines the partial sums pairwise. The plain
+// FP64 form (single tables and batches) uses lut_build_fast_kernel: one thread per bin over
+// node weights shared by all bins (the integrand factors into a bin-independent weight times
+// sin(kds p)). The compensated sums replace the sort (they are at least as accurate), so the
+// float table matches the reference's to within one float ulp rather than bit for bit.
 //
 // The node set keeps the reference's rule exactly: weights h/3 * {1, 4, 2, ..., 4, 2, 1}
 // with the odd loop ending at node n-3 and the even loop at n-4 (nodes n-2 and n-1 are
@@ -176,13 +178,91 @@ __global__ void __launch_bounds__(kLutThreads) lut_build_kernel(LutBuildSpec s, 
     build_bin(s, blockIdx.x, out64, d_mus, d_eps, red);
 }
 
-// Tables of many experiments: blockIdx.y selects the experiment, its table at out64 + y*bins.
-__global__ void __launch_bounds__(kLutThreads) lut_build_batch_kernel(const LutBuildSpec *__restrict__ specs,
-                                                                       uint32_t bins, double *out64)
+// The FP64 form without derivatives factors: node j contributes w_j sin(kds p_j) / kds with
+// w_j = c_j (h/3) p_j exp(bds phase(p_j) - reg^2 p_j^2 / 2) the same for every bin. A CTA
+// of kFastThreads threads covers that many consecutive bins of one table: it stages w_j for a
+// chunk of nodes in shared memory and each thread sweeps its bin over the chunk, stepping
+// (sin, cos)(kds j h) by the rotation through kds h and restarting from sincos every kRun
+// nodes, so the phase drift stays at the level of the direct argument's own rounding
+// (kds j h carries a relative error of one ulp either way). Runs are summed plainly and
+// folded into a Neumaier total; node n (p = maxBound exactly) is added with a direct sin;
+// bin 0 (kds = 0) takes the limit sin(kds p)/kds -> p. Against the per-node quadrature
+// (lut_build_kernel) it replaces two exp and one sin per node and bin by five FMAs.
+constexpr int kFastThreads = 128;
+constexpr uint32_t kFastChunk = 1024;
+constexpr uint32_t kRun = 64;
+
+__device__ __forceinline__ void build_fast(const LutBuildSpec &s, uint32_t bin0, double *out64, double *sw)
 {
-    __shared__ double red[kLutThreads / 32];
+    const uint32_t n = s.num_steps_int;
+    const double m = (double)s.eps, reg = (double)s.mu;
+    const double ds = (double)s.ds;
+    const double bds = (double)s.scatter * ds;
+    const double maxb = 10.0 / m;
+    const double h = maxb / (double)n;
+    const double weight = h / 3.0;
+    const double np_d = sqrt((CUDART_PI * m) * 0.5) / (1.0 - exp(-2.0 / m));
+    const uint32_t bin = bin0 + threadIdx.x;
+    const double kds = (double)bin * s.step64 * ds;
+    const bool zero_k = !(kds > 0.0);
+    double st, ct;
+    sincos(kds * h, &st, &ct);
+    Neumaier acc;
+    for (uint32_t c0 = 0; c0 < n; c0 += kFastChunk) {
+        const uint32_t cn = min(kFastChunk, n - c0);
+        __syncthreads();   // the previous chunk is consumed
+        for (uint32_t i = threadIdx.x; i < cn; i += blockDim.x) {
+            const uint32_t j = c0 + i;
+            const double c = (j == 0) ? 1.0 : (j >= n - 2) ? 0.0 : ((j & 1u) ? 4.0 : 2.0);
+            const double p = (double)j * h;
+            const double ph = np_d * exp(-m * p * p * 0.5);
+            sw[i] = (p * exp(bds * ph - reg * reg * p * p * 0.5)) * weight * c;
+        }
+        __syncthreads();
+        if (zero_k) {
+            double run = 0.0;
+            for (uint32_t i = 0; i < cn; ++i) run = fma(sw[i], (double)(c0 + i) * h, run);
+            acc.add(run);
+        } else {
+            for (uint32_t r0 = 0; r0 < cn; r0 += kRun) {
+                double sn, cs;
+                sincos(kds * ((double)(c0 + r0) * h), &sn, &cs);
+                const uint32_t rn = min(kRun, cn - r0);
+                double run = 0.0;
+#pragma unroll 8
+                for (uint32_t i = 0; i < rn; ++i) {
+                    run = fma(sw[r0 + i], sn, run);
+                    const double t = fma(sn, ct, cs * st);
+                    cs = fma(cs, ct, -(sn * st));
+                    sn = t;
+                }
+                acc.add(run);
+            }
+        }
+    }
+    const double ph = np_d * exp(-m * maxb * maxb * 0.5);
+    const double wn = (maxb * exp(bds * ph - reg * reg * maxb * maxb * 0.5)) * weight;
+    acc.add(zero_k ? wn * maxb : wn * sin(kds * maxb));
+    if (bin < s.bins) {
+        const double total = zero_k ? acc.value() : acc.value() / kds;
+        out64[bin] = (total / (2.0 * CUDART_PI * CUDART_PI)) * (double)s.bias;
+    }
+}
+
+__global__ void __launch_bounds__(kFastThreads) lut_build_fast_kernel(LutBuildSpec s, double *out64)
+{
+    __shared__ double sw[kFastChunk];
+    build_fast(s, blockIdx.x * kFastThreads, out64, sw);
+}
+
+// Tables of many experiments (FP64 form, no derivatives): blockIdx.y selects the
+// experiment, its table at out64 + y*bins.
+__global__ void __launch_bounds__(kFastThreads) lut_build_batch_kernel(const LutBuildSpec *__restrict__ specs,
+                                                                        uint32_t bins, double *out64)
+{
+    __shared__ double sw[kFastChunk];
     const LutBuildSpec s = specs[blockIdx.y];
-    build_bin(s, blockIdx.x, out64 + (size_t)blockIdx.y * bins, nullptr, nullptr, red);
+    build_fast(s, blockIdx.x * kFastThreads, out64 + (size_t)blockIdx.y * bins, sw);
 }
 
 // Replace non-positive entries by the smallest non-negative one and emit the float copy
@@ -337,7 +417,8 @@ cudaError_t launch_lut_build_batch(const LutBuildSpec *d_specs, uint32_t n, uint
 {
     if (n == 0) return cudaSuccess;
     if (bins < 2 || n > 65535u) return cudaErrorInvalidValue;
-    lut_build_batch_kernel<<<dim3(bins, n), kLutThreads, 0, st>>>(d_specs, bins, out64);
+    lut_build_batch_kernel<<<dim3((bins + kFastThreads - 1) / kFastThreads, n), kFastThreads, 0, st>>>(d_specs, bins,
+                                                                                                      out64);
     return cudaGetLastError();
 }
 
@@ -361,7 +442,10 @@ cudaError_t launch_comp_tables_batch(uint32_t n, uint32_t bins, const float *lut
 cudaError_t launch_lut_build(const LutBuildSpec &s, double *out64, double *d_mus, double *d_eps, cudaStream_t st)
 {
     if (s.bins < 2 || s.num_steps_int < 4 || (s.num_steps_int & 1u)) return cudaErrorInvalidValue;
-    lut_build_kernel<<<s.bins, kLutThreads, 0, st>>>(s, out64, d_mus, d_eps);
+    if (!s.faithful && !s.derivatives)
+        lut_build_fast_kernel<<<(s.bins + kFastThreads - 1) / kFastThreads, kFastThreads, 0, st>>>(s, out64);
+    else
+        lut_build_kernel<<<s.bins, kLutThreads, 0, st>>>(s, out64, d_mus, d_eps);
     return cudaGetLastError();
 }
 
