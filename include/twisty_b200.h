@@ -147,7 +147,22 @@ typedef struct twisty_result {
     double setup_ms;             /* setupExperimentMs: table, normaliser, initial curve */
     double perturb_ms;           /* perturbExperimentMs: the chain kernel, device time */
     double weighting_ms;         /* weightingExperimentMs: final reduction */
+    /* Compensated form only (no reference counterpart): which table the pass weighed with,
+       TWISTY_TABLE_FIXED_NARROW / _FIXED_WIDE (fixed-point log tables, 32- or 64-bit path
+       totals) or TWISTY_TABLE_EXACT_BLEND (linear table, a log per segment); other forms
+       report TWISTY_TABLE_NONE. steep_bins counts the fixed-point table's bins whose secant
+       would err by more than 1e-7 per segment: paths crossing one are re-weighed through the
+       linear table. */
+    uint32_t table_form;
+    uint32_t steep_bins;
 } twisty_result;
+
+enum {
+    TWISTY_TABLE_FIXED_NARROW = 0,
+    TWISTY_TABLE_FIXED_WIDE = 1,
+    TWISTY_TABLE_EXACT_BLEND = 2,
+    TWISTY_TABLE_NONE = 3
+};
 
 /* Table metadata (BaseWeightLookupTable accessors, Twisty/PathWeightUtils.h:129-141). */
 typedef struct twisty_lut_info {

@@ -22,13 +22,14 @@ import numpy as np
 
 from . import _abi
 from ._abi import (FORM_COMPENSATED, FORM_FP64, FORM_PLAIN_FP32, LUT_EXTERNAL, LUT_FAITHFUL, LUT_MULTI_DS,
-                   LUT_FP64)
+                   LUT_FP64, TABLE_EXACT_BLEND, TABLE_FIXED_NARROW, TABLE_FIXED_WIDE, TABLE_NONE)
 
 __all__ = [
     "TwistyError", "Context", "ExperimentParameters", "BoundaryConditions", "ExperimentResults",
     "ParseExperimentParamsFromConfig", "FullExperimentRunnerOptimalPerturb",
     "FullExperimentRunnerOptimalPerturbOptimized_GPU", "FORM_PLAIN_FP32", "FORM_COMPENSATED",
-    "FORM_FP64", "LUT_FAITHFUL", "LUT_FP64", "LUT_EXTERNAL", "default_params", "make_bc",
+    "FORM_FP64", "LUT_FAITHFUL", "LUT_FP64", "LUT_EXTERNAL", "TABLE_FIXED_NARROW", "TABLE_FIXED_WIDE",
+    "TABLE_EXACT_BLEND", "TABLE_NONE", "default_params", "make_bc",
 ]
 
 

@@ -32,6 +32,10 @@ LUT_FAITHFUL = 0
 LUT_FP64 = 1
 LUT_EXTERNAL = 2
 LUT_MULTI_DS = 3
+TABLE_FIXED_NARROW = 0
+TABLE_FIXED_WIDE = 1
+TABLE_EXACT_BLEND = 2
+TABLE_NONE = 3
 
 
 class Vec3(C.Structure):
@@ -94,6 +98,8 @@ class Result(C.Structure):
         ("setup_ms", C.c_double),
         ("perturb_ms", C.c_double),
         ("weighting_ms", C.c_double),
+        ("table_form", C.c_uint32),
+        ("steep_bins", C.c_uint32),
     ]
 
 

@@ -15,13 +15,14 @@ struct BatchExp {
     ChainSpec spec;
     CompConsts kc;
     const float2 *tab;
+    const float2 *lin;       // linear table (the fallback of steep bins in the fixed-point form)
     const float *init_seg;
     double log10_abs;
     uint32_t out_offset;
     uint32_t pad;
 };
 
-template <int G, int SPL, bool EXACT, bool LUT_SMEM, bool CLAMP, int MAXT>
+template <int G, int SPL, bool EXACT, bool LUT_SMEM, bool CLAMP, bool STEEP, int MAXT>
 __global__ void __launch_bounds__(MAXT, 1) batch_kernel(const BatchExp *__restrict__ exps,
                                                         const uint2 *__restrict__ items, uint32_t n_items,
                                                         uint32_t *__restrict__ counter, ChainOut *__restrict__ out,
@@ -53,55 +54,63 @@ __global__ void __launch_bounds__(MAXT, 1) batch_kernel(const BatchExp *__restri
         __syncthreads();
         ModeArgs ma{};
         ma.log10_abs = e.log10_abs;
+        ma.lin = e.lin;
         const uint32_t chain = it.y + warp * CPW + q;
-        chain_body<G, SPL, EXACT, CLAMP, false, kModeForward>(e.spec, e.kc, e.init_seg, tab, st, q * G, j, chain,
-                                                             chain < e.spec.n_chains, out + e.out_offset, ma);
+        chain_body<G, SPL, EXACT, CLAMP, false, kModeForward, false, STEEP>(e.spec, e.kc, e.init_seg, tab, st, q * G, j,
+                                                                            chain, chain < e.spec.n_chains,
+                                                                            out + e.out_offset, ma);
         __syncthreads();
     }
 }
 
-template <int G, int SPL, bool EXACT, bool LS, bool CL>
+template <int G, int SPL, bool EXACT, bool LS, bool CL, bool SP>
 cudaError_t batch_t(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items, uint32_t *counter,
                     ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st)
 {
     constexpr int MAXT = (SPL >= 16 || G == 8) ? 512 : 1024;
     if (s.warps * 32 > MAXT) return cudaErrorInvalidConfiguration;
-    auto kern = batch_kernel<G, SPL, EXACT, LS, CL, MAXT>;
+    auto kern = batch_kernel<G, SPL, EXACT, LS, CL, SP, MAXT>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     kern<<<grid, s.warps * 32, smem, st>>>(exps, items, n_items, counter, out, bins);
     return cudaGetLastError();
 }
 
-template <int G, int SPL, bool EXACT, bool LS, bool CL>
+template <int G, int SPL, bool EXACT, bool LS, bool CL, bool SP>
 int batch_occ_t(const BatchShape &s, size_t smem)
 {
     constexpr int MAXT = (SPL >= 16 || G == 8) ? 512 : 1024;
-    auto kern = batch_kernel<G, SPL, EXACT, LS, CL, MAXT>;
+    auto kern = batch_kernel<G, SPL, EXACT, LS, CL, SP, MAXT>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, s.warps * 32, smem) != cudaSuccess) return 0;
     return nb;
 }
 
-// Instantiated: fixed-point tables with or without clamping, exact tables with clamping,
-// each with the table in shared memory or read through L1.
+// Instantiated: exact tables with clamping (table in shared memory or read through L1);
+// fixed-point tables with or without clamping, in shared memory with the steep-bin fallback
+// or read through L1 without it.
 template <int G, int SPL>
 int batch_occ_g(const BatchShape &s, size_t smem)
 {
-    if (s.exact) return s.lut_smem ? batch_occ_t<G, SPL, true, true, true>(s, smem) : batch_occ_t<G, SPL, true, false, true>(s, smem);
-    if (s.clamp) return s.lut_smem ? batch_occ_t<G, SPL, false, true, true>(s, smem) : batch_occ_t<G, SPL, false, false, true>(s, smem);
-    return s.lut_smem ? batch_occ_t<G, SPL, false, true, false>(s, smem) : batch_occ_t<G, SPL, false, false, false>(s, smem);
+    if (s.exact) return s.lut_smem ? batch_occ_t<G, SPL, true, true, true, false>(s, smem)
+                                   : batch_occ_t<G, SPL, true, false, true, false>(s, smem);
+    if (s.lut_smem != s.steep) return 0;
+    if (s.steep) return s.clamp ? batch_occ_t<G, SPL, false, true, true, true>(s, smem)
+                                : batch_occ_t<G, SPL, false, true, false, true>(s, smem);
+    return s.clamp ? batch_occ_t<G, SPL, false, false, true, false>(s, smem)
+                   : batch_occ_t<G, SPL, false, false, false, false>(s, smem);
 }
 
 template <int G, int SPL>
 cudaError_t batch_g(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items, uint32_t *counter,
                     ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st)
 {
-#define TWISTY_BT(E, LS, CL) batch_t<G, SPL, E, LS, CL>(s, exps, items, n_items, counter, out, bins, grid, smem, st)
-    if (s.exact) return s.lut_smem ? TWISTY_BT(true, true, true) : TWISTY_BT(true, false, true);
-    if (s.clamp) return s.lut_smem ? TWISTY_BT(false, true, true) : TWISTY_BT(false, false, true);
-    return s.lut_smem ? TWISTY_BT(false, true, false) : TWISTY_BT(false, false, false);
+#define TWISTY_BT(E, LS, CL, SP) batch_t<G, SPL, E, LS, CL, SP>(s, exps, items, n_items, counter, out, bins, grid, smem, st)
+    if (s.exact) return s.lut_smem ? TWISTY_BT(true, true, true, false) : TWISTY_BT(true, false, true, false);
+    if (s.lut_smem != s.steep) return cudaErrorInvalidValue;
+    if (s.steep) return s.clamp ? TWISTY_BT(false, true, true, true) : TWISTY_BT(false, true, false, true);
+    return s.clamp ? TWISTY_BT(false, false, true, false) : TWISTY_BT(false, false, false, false);
 #undef TWISTY_BT
 }
 
@@ -118,6 +127,7 @@ void batch_pack_experiments(const BatchExpHost *in, uint32_t n, void *dst)
         e.spec = in[i].spec;
         e.kc = make_consts(in[i].spec.inv_ds, in[i].meta, in[i].spec.n_segments, in[i].lf);
         e.tab = in[i].tab;
+        e.lin = in[i].lin;
         e.init_seg = in[i].init_seg;
         e.log10_abs = log10(in[i].spec.absorption_factor);
         e.out_offset = in[i].out_offset;

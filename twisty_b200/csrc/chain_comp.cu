@@ -6,7 +6,7 @@
 namespace twisty {
 namespace {
 
-template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MAXT, int MODE, bool INCR>
+template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MAXT, int MODE, bool INCR, bool STEEP>
 __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompConsts kc,
                                                              const float *__restrict__ init_seg,
                                                              const float2 *__restrict__ tab_g,
@@ -31,8 +31,8 @@ __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompCo
     unsigned char *wb = s_state + (size_t)warp * Lay::WARP_BYTES;
     const Planes pl{reinterpret_cast<float2 *>(wb), reinterpret_cast<float *>(wb + Lay::XY_BYTES),
                     reinterpret_cast<float *>(wb + Lay::XY_BYTES + Lay::Z_BYTES)};
-    const double cl = chain_body<G, SPL, EXACT, CLAMP, SHIFT, MODE, INCR>(c, kc, init_seg, s_tab, pl, q * G, j, chain,
-                                                                          chain < c.n_chains, out, ma);
+    const double cl = chain_body<G, SPL, EXACT, CLAMP, SHIFT, MODE, INCR, STEEP>(c, kc, init_seg, s_tab, pl, q * G, j,
+                                                                                 chain, chain < c.n_chains, out, ma);
     if (j == 0) s_res[warp * CPW + q] = cl;
     __syncthreads();
     // Per-CTA log-sum-exp of the chains, rescaled by the block maximum (FP64).
@@ -54,6 +54,7 @@ __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompCo
 template <int SPL, bool EXACT>
 __global__ void __launch_bounds__(256) weigh_comp_kernel(const float *__restrict__ pos, uint64_t n_paths, uint32_t N,
                                                           CompConsts kc, const float2 *__restrict__ tab,
+                                                          const float2 *__restrict__ lin,
                                                           double log10_absorption, double *__restrict__ log10w,
                                                           uint8_t *__restrict__ valid, int32_t *__restrict__ bins)
 {
@@ -78,7 +79,11 @@ __global__ void __launch_bounds__(256) weigh_comp_kernel(const float *__restrict
         if (brow) brow[i] = b;
     };
     uint32_t clamped = 0;
-    const double w = path_log10<32, SPL, EXACT, true>(j, N, tab, kc, tan, ShflNext<32>{}, sink, clamped);
+    double w = path_log10<32, SPL, EXACT, true>(j, N, tab, kc, tan, ShflNext<32>{}, sink, clamped);
+    if (!EXACT && isnan(w)) {
+        // a steep bin (NaN slope) or a NaN curvature: the exact blend through the linear table
+        w = path_log10<32, SPL, true, true>(j, N, lin, kc, tan, ShflNext<32>{}, sink, clamped);
+    }
     if (j == 0) {
         const bool ok = !isnan(w);
         log10w[p] = ok ? w + (double)(N - 1) * log10_absorption : 0.0;
@@ -87,13 +92,13 @@ __global__ void __launch_bounds__(256) weigh_comp_kernel(const float *__restrict
 }
 
 // ------------------------------------------------------------------------------ launchers
-template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MODE, bool INCR = false>
+template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MODE, bool INCR = false, bool STEEP = false>
 cudaError_t launch_t(const ChainSpec &c, const CompConsts &kc, int warps, const float *init_seg, const float2 *tab,
                      ChainOut *out, double2 *partials, const ModeArgs &ma, size_t smem, uint32_t blocks, cudaStream_t st)
 {
     constexpr int MAXT = (SPL >= 16) ? 512 : 1024;
     if (warps * 32 > MAXT) return cudaErrorInvalidConfiguration;
-    auto kern = comp_chain_kernel<G, SPL, EXACT, CLAMP, SHIFT, MAXT, MODE, INCR>;
+    auto kern = comp_chain_kernel<G, SPL, EXACT, CLAMP, SHIFT, MAXT, MODE, INCR, STEEP>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     kern<<<blocks, warps * 32, smem, st>>>(c, kc, init_seg, tab, out, partials, ma);
@@ -101,23 +106,32 @@ cudaError_t launch_t(const ChainSpec &c, const CompConsts &kc, int warps, const 
 }
 
 // Instantiated variants: forward (fixed/exact x clamp/no clamp, plus an exact+clamp+shift
-// variant for receiver-shifted evaluation), export (fixed/exact with clamp), adjoint (exact).
+// variant for receiver-shifted evaluation), export (fixed/exact with clamp), adjoint (exact);
+// the fixed-point forward, incremental and export variants again with the steep-bin fallback.
 template <int G, int SPL>
-cudaError_t launch_g(int mode, bool exact, bool clamp, bool shift, const ChainSpec &c, const CompConsts &kc,
-                     const CompTuning &t, const float *init_seg, const float2 *tab, ChainOut *out, double2 *partials,
-                     const ModeArgs &ma, size_t smem, uint32_t blocks, cudaStream_t st)
+cudaError_t launch_g(int mode, bool exact, bool clamp, bool shift, bool steep, const ChainSpec &c,
+                     const CompConsts &kc, const CompTuning &t, const float *init_seg, const float2 *tab,
+                     ChainOut *out, double2 *partials, const ModeArgs &ma, size_t smem, uint32_t blocks,
+                     cudaStream_t st)
 {
     const int w = t.warps_per_block;
 #define TWISTY_L(E, CL, SH, MO) launch_t<G, SPL, E, CL, SH, MO>(c, kc, w, init_seg, tab, out, partials, ma, smem, blocks, st)
+#define TWISTY_S(CL, MO, IN) \
+    launch_t<G, SPL, false, CL, false, MO, IN, true>(c, kc, w, init_seg, tab, out, partials, ma, smem, blocks, st)
     if (mode == kModeAdjoint) return TWISTY_L(true, true, false, kModeAdjoint);
-    if (mode == kModeExport) return exact ? TWISTY_L(true, true, false, kModeExport) : TWISTY_L(false, true, false, kModeExport);
+    if (mode == kModeExport) {
+        if (exact) return TWISTY_L(true, true, false, kModeExport);
+        return steep ? TWISTY_S(true, kModeExport, false) : TWISTY_L(false, true, false, kModeExport);
+    }
     if (shift) return TWISTY_L(true, true, true, kModeForward);
     if (exact) return clamp ? TWISTY_L(true, true, false, kModeForward) : TWISTY_L(true, false, false, kModeForward);
-    if (clamp) return TWISTY_L(false, true, false, kModeForward);
+    if (clamp) return steep ? TWISTY_S(true, kModeForward, false) : TWISTY_L(false, true, false, kModeForward);
     if (c.incr_resync > 1)
-        return launch_t<G, SPL, false, false, false, kModeForward, true>(c, kc, w, init_seg, tab, out, partials, ma, smem,
-                                                                         blocks, st);
-    return TWISTY_L(false, false, false, kModeForward);
+        return steep ? TWISTY_S(false, kModeForward, true)
+                     : launch_t<G, SPL, false, false, false, kModeForward, true>(c, kc, w, init_seg, tab, out, partials,
+                                                                                  ma, smem, blocks, st);
+    return steep ? TWISTY_S(false, kModeForward, false) : TWISTY_L(false, false, false, kModeForward);
+#undef TWISTY_S
 #undef TWISTY_L
 }
 
@@ -136,9 +150,13 @@ cudaError_t launch_mode(int mode, const ChainSpec &c, const CompTuning &t, const
     const uint32_t blocks = comp_blocks(c, t);
     const float2 *tab = exact ? lintab : fixtab;
     const bool clamp = table_needs_clamp(kc);
+    const bool steep = !exact && lf.steep > 0;
+    ModeArgs mb = ma;
+    mb.lin = lintab;
 #define TWISTY_CASE(GG, SS) \
     if (t.group == GG && t.spl == SS) \
-        return launch_g<GG, SS>(mode, exact, clamp, shift, c, kc, t, init_seg, tab, out, block_partials, ma, smem, blocks, st);
+        return launch_g<GG, SS>(mode, exact, clamp, shift, steep, c, kc, t, init_seg, tab, out, block_partials, mb, smem, \
+                                blocks, st);
     TWISTY_CASE(8, 2)
     TWISTY_CASE(8, 4)
     TWISTY_CASE(8, 8)
@@ -282,10 +300,12 @@ cudaError_t launch_weigh_comp(const float *pos, uint64_t n_paths, uint32_t n_seg
     if (n_segments <= 32u * SS) {                                                                              \
         if (exact)                                                                                             \
             weigh_comp_kernel<SS, true><<<(unsigned)blocks, 256, 0, st>>>(pos, n_paths, n_segments, kc, tab,  \
-                                                                          log10_absorption, log10w, valid, bins); \
+                                                                          lintab, log10_absorption, log10w, valid, \
+                                                                          bins);                                  \
         else                                                                                                   \
             weigh_comp_kernel<SS, false><<<(unsigned)blocks, 256, 0, st>>>(pos, n_paths, n_segments, kc, tab, \
-                                                                           log10_absorption, log10w, valid, bins); \
+                                                                           lintab, log10_absorption, log10w,     \
+                                                                           valid, bins);                          \
         return cudaGetLastError();                                                                             \
     }
     TWISTY_W(1)

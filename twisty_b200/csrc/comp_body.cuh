@@ -218,7 +218,8 @@ __device__ __forceinline__ double path_log10(uint32_t j, uint32_t N, const float
             kahan_add(ks, kc, valid ? term : 0.0f);
         } else {
             isum += valid ? __float_as_uint(e.x) : 0u;
-            csum = fmaf(valid ? frac : 0.0f, e.y, csum);
+            const float c2 = fmaf(frac, e.y, csum);
+            csum = valid ? c2 : csum;
         }
     });
     if (EXACT) {
@@ -248,7 +249,9 @@ __device__ __forceinline__ unsigned long long path_fixed(uint32_t j, uint32_t gb
         const float r = bin_of<CLAMP>(qq, k, valid, clamped, L);
         const float2 e = tab[L];
         isum += valid ? __float_as_uint(e.x) : 0u;
-        csum = fmaf(valid ? r - (float)L : 0.0f, e.y, csum);
+        // a padding slot leaves the sum alone even where the slope is NaN (a steep bin)
+        const float c2 = fmaf(r - (float)L, e.y, csum);
+        csum = valid ? c2 : csum;
     };
     if (N == (uint32_t)(G * SPL))
         for_curvatures<G, SPL, true>(j, N, tan, next, seg);
@@ -290,6 +293,9 @@ enum { kModeForward = 0, kModeExport = 1, kModeAdjoint = 2 };
 
 struct ModeArgs {
     double log10_abs;    // log10 of the per-segment absorption factor
+    // linear table (L_i, L_{i+1} - L_i) of the fixed-point table's curve: paths that cross a
+    // steep bin (NaN slope) are re-weighed through it
+    const float2 *lin;
     // export
     float *exp_pos;      // [chains][steps][N+1][3]
     double *exp_w;       // [chains][steps] log10 weights (absorption included, normaliser not)
@@ -343,11 +349,32 @@ __device__ __forceinline__ void stage_table(float4 *smem4, const float2 *__restr
     if ((bins & 1) && threadIdx.x == 0) reinterpret_cast<float2 *>(smem4)[bins - 1] = tab_g[bins - 1];
 }
 
+// Exact-blend weight of the group's current path through the linear table, for paths of a
+// fixed-point table that cross a steep bin. Not inlined: it runs rarely, and inlined its
+// registers would count against the hot loop's.
+template <int G, int SPL, bool CLAMP>
+__device__ __noinline__ double steep_fallback(Planes st, uint32_t gbase, uint32_t j, uint32_t N,
+                                              const float2 *__restrict__ lin, CompConsts kc)
+{
+    using Lay = Layout<G, SPL>;
+    const uint32_t own = gbase + j;
+    auto tan = [&](int m, float &x, float &y, float &z) {
+        const float2 a = st.xy[Lay::xy(own, m)];
+        x = a.x;
+        y = a.y;
+        z = st.z[Lay::z(own, m)];
+    };
+    uint32_t unused = 0;
+    return path_log10<G, SPL, true, CLAMP>(j, N, lin, kc, tan, ShflNext<G>{}, [](uint32_t, int32_t) {}, unused);
+}
+
 // One Markov chain run by the G lanes of one group on its own records st (tangent, length;
 // warp-local slots): initial state from init_seg (segment vectors), burn_in + steps
 // proposals, a full recompute of every weighted path, and the chain's running log-sum-exp.
 // Writes out[chain] (when out is set and the chain is real) and returns the chain's log10 sum.
-template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MODE, bool INCR = false>
+// STEEP: the fixed-point table has steep bins (NaN slopes); paths crossing one are re-weighed
+// through ma.lin. Without it a NaN slope cannot occur and a NaN total means a NaN curvature.
+template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MODE, bool INCR = false, bool STEEP = false>
 __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConsts &kc,
                                              const float *__restrict__ init_seg, const float2 *s_tab, Planes st,
                                              uint32_t gbase, uint32_t j, uint32_t chain, bool real_chain,
@@ -417,9 +444,9 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
         uint32_t unused = 0;
         const float r = bin_of<CLAMP>(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), kc, false, unused, L);
         const float2 e = s_tab[L];
-        const float frac = r - (float)L;
-        nan |= isnan(frac);
-        return __float_as_uint(e.x) + (uint32_t)__float2int_rn(frac * e.y * kc.fscale);
+        const float cor = (r - (float)L) * e.y;
+        nan |= isnan(cor);   // a NaN curvature or a steep bin's NaN slope
+        return __float_as_uint(e.x) + (uint32_t)__float2int_rn(cor * kc.fscale);
     };
 
     const uint32_t own = gbase + j;
@@ -551,21 +578,40 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
             const bool active = wstep < steps_c;
 
             if (FIX) {
-                bool bad;
-                unsigned long long tot;
-                if (INCR && incr_now) {
-                    // the two end curvatures after the rotation; the interior ones keep their terms
-                    float a1x, a1y, a1z, b0x, b0y, b0z;
-                    tan_at(left, a1x, a1y, a1z);
-                    tan_at(right - 1, b0x, b0y, b0z);
-                    const uint32_t t_new =
-                          term(e0x, e0y, e0z, a1x, a1y, a1z, inc_bad) + term(b0x, b0y, b0z, e3x, e3y, e3z, inc_bad);
-                    inc_tot += (unsigned long long)(long long)(int32_t)(t_new - t_old);
+                bool bad = false;
+                unsigned long long tot = 0;
+                bool need_full = true;
+                if constexpr (INCR) {
+                    if (incr_now) {
+                        // the two end curvatures after the rotation; the interior ones keep their terms
+                        float a1x, a1y, a1z, b0x, b0y, b0z;
+                        tan_at(left, a1x, a1y, a1z);
+                        tan_at(right - 1, b0x, b0y, b0z);
+                        const uint32_t t_new =
+                              term(e0x, e0y, e0z, a1x, a1y, a1z, inc_bad) + term(b0x, b0y, b0z, e3x, e3y, e3z, inc_bad);
+                        inc_tot += (unsigned long long)(long long)(int32_t)(t_new - t_old);
+                        need_full = inc_bad;
+                    }
+                }
+                // one decision per warp: the full recompute shuffles across the whole warp, and
+                // every chain of the warp then stays on the same resync schedule
+                if (INCR && !__any_sync(FULL, need_full)) {
                     tot = inc_tot;
-                    bad = inc_bad;
                     ++inc_since_full;
                 } else {
                     tot = path_fixed<G, SPL, CLAMP>(j, gbase, N, s_tab, kc, tan_smem, next_smem, bad, clamped);
+                    // a NaN slope marks a steep bin, where the secant would err by more than
+                    // 1e-7: weigh such paths (rare) with the exact blend through the linear
+                    // table; only a NaN curvature leaves a path invalid
+                    if constexpr (STEEP) {
+                        if (__any_sync(FULL, bad)) {
+                            const double wx = steep_fallback<G, SPL, CLAMP>(st, gbase, j, N, ma.lin, kc);
+                            if (bad && !isnan(wx)) {
+                                bad = false;
+                                tot = (unsigned long long)llrint(fmax(0.0, (wx - kc.lw_offset) * (double)kc.fscale));
+                            }
+                        }
+                    }
                     inc_tot = tot;
                     inc_bad = bad;
                     inc_since_full = 0;

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cctype>
 #include <cmath>
+#include <limits>
 #include <cstdlib>
 #include <cstring>
 #include <random>
@@ -888,7 +889,8 @@ double norm_k4_log10(float z, float ds)
 }
 
 bool compensated_tables(const float *lut, uint32_t bins, float step, uint32_t n_segments, std::vector<float> &lin,
-                        std::vector<float> &fix, double &c0, double &inv_scale, int &wide, double &secant_err)
+                        std::vector<float> &fix, double &c0, double &inv_scale, int &wide, double &secant_err,
+                        uint32_t &steep)
 {
     wide = 0;
     lin.assign(2 * (size_t)bins, 0.0f);
@@ -896,8 +898,10 @@ bool compensated_tables(const float *lut, uint32_t bins, float step, uint32_t n_
     c0 = 0.0;
     inv_scale = 0.0;
     secant_err = 0.0;
+    steep = 0;
     bool positive = true;
     std::vector<double> lg(bins);
+    std::vector<unsigned char> is_steep(bins, 0);
     double lo = INFINITY, hi = -INFINITY;
     const double st = (double)step;
     for (uint32_t i = 0; i < bins; ++i) {
@@ -913,7 +917,13 @@ bool compensated_tables(const float *lut, uint32_t bins, float step, uint32_t n_
         hi = std::max(hi, lg[i]);
         if (i + 1 < bins) {
             const double r = (double)b / (double)a - 1.0;
-            secant_err = std::max(secant_err, (st * r) * (st * r) / (8.0 * 2.302585092994046));
+            const double e = (st * r) * (st * r) / (8.0 * 2.302585092994046);
+            if (e > kSecantBound) {
+                is_steep[i] = 1;
+                ++steep;
+            } else {
+                secant_err = std::max(secant_err, e);
+            }
         }
     }
     if (!positive) {
@@ -932,7 +942,7 @@ bool compensated_tables(const float *lut, uint32_t bins, float step, uint32_t n_
         s = 30;
         while (s > 0 && range * std::ldexp(1.0, s) + 65.0 > cap) --s;
     }
-    if (secant_err > 1e-7 || s < 22) {
+    if (s < 22 || steep > bins / kSteepFraction) {
         wide = 0;
         return false;
     }
@@ -944,7 +954,7 @@ bool compensated_tables(const float *lut, uint32_t bins, float step, uint32_t n_
         std::memcpy(&fix[2 * i], &u, 4);
         double delta = 0.0;
         if (i + 1 < bins) delta = std::log10(1.0 + st * ((double)lut[i + 1] / (double)lut[i] - 1.0));
-        fix[2 * i + 1] = (float)delta;
+        fix[2 * i + 1] = is_steep[i] ? std::numeric_limits<float>::quiet_NaN() : (float)delta;
     }
     return true;
 }

@@ -70,11 +70,17 @@ bool lut_faithful_host(float mu, float eps, float scatter, float min_bound, floa
 //    that a path total and the difference of two totals are exact in 32 bits (narrow);
 //    when that leaves fewer than 22 fraction bits, 32 * max entry < 2^32 (wide = 1: exact
 //    32-bit lane sums of up to 32 entries, 64-bit path totals).
-// secant_err = the worst per-segment error of the secant, (step a)^2 / (8 ln 10) with
-// a = L_{i+1}/L_i - 1. Returns false (fix unusable, the exact blend is needed) when an
-// entry is not positive, secant_err > 1e-7, or fewer than 22 fraction bits fit either way.
+// The secant's worst per-segment error in bin i is (step a)^2 / (8 ln 10) with
+// a = L_{i+1}/L_i - 1. Bins where it exceeds kSecantBound are steep: their slope is stored
+// as NaN, so a path crossing one is flagged and re-weighed through lin by the kernels;
+// steep = their count, secant_err = the worst error over the other bins. Returns false (fix
+// unusable, the exact blend is needed) when an entry is not positive, more than
+// bins / kSteepFraction bins are steep, or fewer than 22 fraction bits fit either way.
+constexpr double kSecantBound = 1e-7;
+constexpr uint32_t kSteepFraction = 16;
 bool compensated_tables(const float *lut, uint32_t bins, float step, uint32_t n_segments, std::vector<float> &lin,
-                        std::vector<float> &fix, double &c0, double &inv_scale, int &wide, double &secant_err);
+                        std::vector<float> &fix, double &c0, double &inv_scale, int &wide, double &secant_err,
+                        uint32_t &steep);
 
 // K4 (Twisty/PathWeightUtils.cpp:643-651) and the z of Norm (:729-732), float math.
 double norm_k4_log10(float z, float ds);

@@ -115,7 +115,7 @@ struct LogFixed {
     double c0;
     double inv_scale;
     int32_t wide;
-    int32_t pad;
+    int32_t steep;           // bins whose secant slope is NaN (paths crossing them are re-weighed exactly)
 };
 struct CompTuning {
     int group;               // lanes per chain (4, 8, 16, 32)
@@ -152,6 +152,9 @@ struct BatchShape {
     int exact;               // tables are (L_i, L_{i+1}-L_i) with a log2 per segment
     int lut_smem;            // stage each item's table in shared memory (else read through L1)
     int clamp;               // some table's curvature range can be left (else no clamping code)
+    int steep;               // fixed-point kernel with the steep-bin fallback (paths crossing a
+                             // NaN-slope bin re-weighed through the linear table); fixed-point
+                             // kernels have it exactly when lut_smem is set
 };
 // Whether curvatures of paths with this N/S can leave the table (it does not cover
 // [0, 2 N/S] from 0): such tables need the clamping kernel variants.
@@ -161,6 +164,7 @@ struct BatchExpHost {
     LutMetaF meta;
     LogFixed lf;
     const float2 *tab;       // device table of meta.bins entries in the shape's form
+    const float2 *lin;       // device linear table of the same curve (steep-bin fallback)
     const float *init_seg;   // device initial segment vectors
     uint32_t out_offset;
 };

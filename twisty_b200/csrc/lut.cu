@@ -23,6 +23,10 @@ namespace twisty {
 namespace {
 
 constexpr int kLutThreads = 256;
+// bins whose secant (fixed-point form) errs by more than this per segment are steep; a table
+// with more than bins / kSteepFractionDev of them takes the exact blend (same rule on the host)
+constexpr double kSecantBoundDev = 1e-7;
+constexpr uint32_t kSteepFractionDev = 16;
 
 struct Integrand {
     double kds, bds, reg, m;   // reg = config mu, m = config eps (phase parameter)
@@ -326,22 +330,24 @@ __global__ void __launch_bounds__(1024) lut_finalize_kernel(uint32_t bins, doubl
 // compensated_tables (same rules): lin = (L_i, L_{i+1} - L_i); fix = (round((log10 L_i - c0)
 // 2^s) as uint32, log10(1 + step (L_{i+1}/L_i - 1))) with c0 = min log10 L - 64 2^-s and the
 // largest s <= 30 keeping (N+1) (range 2^s + 65) below 2^31, else the wide form with
-// 32 (range 2^s + 65) below 2^32. ok[x] = 1 when the fixed form is usable: every entry
-// positive, secant error <= 1e-7 per segment, s >= 22.
+// 32 (range 2^s + 65) below 2^32. Bins whose secant error exceeds 1e-7 per segment are
+// steep: slope NaN (paths crossing them are re-weighed through lin), counted in lf[x].steep.
+// ok[x] = 1 when the fixed form is usable: every entry positive, at most bins/16 steep bins,
+// s >= 22.
 __global__ void __launch_bounds__(1024) comp_tables_kernel(uint32_t bins, const float *__restrict__ lut32,
                                                            const float *__restrict__ steps,
                                                            const uint32_t *__restrict__ nsegs, float2 *fix,
                                                            float2 *lin, LogFixed *lf, int *ok)
 {
     __shared__ double s_lo[32], s_hi[32], s_err[32];
-    __shared__ int s_bad[32];
+    __shared__ int s_bad[32], s_steep[32];
     const uint32_t x = blockIdx.x;
     const float *L = lut32 + (size_t)x * bins;
     fix += (size_t)x * bins;
     lin += (size_t)x * bins;
     const double st = (double)steps[x];
     double lo = DBL_MAX, hi = -DBL_MAX, err = 0.0;
-    int bad = 0;
+    int bad = 0, steep = 0;
     for (uint32_t i = threadIdx.x; i < bins; i += blockDim.x) {
         const float a = L[i], b = L[i + 1 < bins ? i + 1 : i];
         lin[i] = make_float2(a, b - a);
@@ -354,7 +360,9 @@ __global__ void __launch_bounds__(1024) comp_tables_kernel(uint32_t bins, const 
         hi = fmax(hi, lg);
         if (i + 1 < bins) {
             const double r = (double)b / (double)a - 1.0;
-            err = fmax(err, (st * r) * (st * r) / (8.0 * 2.302585092994046));
+            const double e = (st * r) * (st * r) / (8.0 * 2.302585092994046);
+            if (e > kSecantBoundDev) ++steep;
+            else err = fmax(err, e);
         }
     }
     for (int o = 16; o > 0; o >>= 1) {
@@ -362,28 +370,32 @@ __global__ void __launch_bounds__(1024) comp_tables_kernel(uint32_t bins, const 
         hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
         err = fmax(err, __shfl_xor_sync(0xffffffffu, err, o));
         bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+        steep += __shfl_xor_sync(0xffffffffu, steep, o);
     }
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
-    if (l == 0) { s_lo[w] = lo; s_hi[w] = hi; s_err[w] = err; s_bad[w] = bad; }
+    if (l == 0) { s_lo[w] = lo; s_hi[w] = hi; s_err[w] = err; s_bad[w] = bad; s_steep[w] = steep; }
     __syncthreads();
     if (w == 0) {
         lo = l < nw ? s_lo[l] : DBL_MAX;
         hi = l < nw ? s_hi[l] : -DBL_MAX;
         err = l < nw ? s_err[l] : 0.0;
         bad = l < nw ? s_bad[l] : 0;
+        steep = l < nw ? s_steep[l] : 0;
         for (int o = 16; o > 0; o >>= 1) {
             lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
             hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
             err = fmax(err, __shfl_xor_sync(0xffffffffu, err, o));
             bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+            steep += __shfl_xor_sync(0xffffffffu, steep, o);
         }
-        if (l == 0) { s_lo[0] = lo; s_hi[0] = hi; s_err[0] = err; s_bad[0] = bad; }
+        if (l == 0) { s_lo[0] = lo; s_hi[0] = hi; s_err[0] = err; s_bad[0] = bad; s_steep[0] = steep; }
     }
     __syncthreads();
     lo = s_lo[0];
     hi = s_hi[0];
     err = s_err[0];
     bad = s_bad[0];
+    steep = s_steep[0];
     double cap = floor(2147483647.0 / (double)(nsegs[x] + 1));
     int s = 30;
     while (s > 0 && (hi - lo) * ldexp(1.0, s) + 65.0 > cap) --s;
@@ -394,19 +406,23 @@ __global__ void __launch_bounds__(1024) comp_tables_kernel(uint32_t bins, const 
         s = 30;
         while (s > 0 && (hi - lo) * ldexp(1.0, s) + 65.0 > cap) --s;
     }
-    const bool usable = !bad && err <= 1e-7 && s >= 22;
+    const bool usable = !bad && (uint32_t)steep <= bins / kSteepFractionDev && s >= 22;
     const double inv_scale = ldexp(1.0, -s);
     if (threadIdx.x == 0) {
-        lf[x] = usable ? LogFixed{lo - 64.0 * inv_scale, inv_scale, wide, 0} : LogFixed{0.0, 0.0, 0, 0};
+        lf[x] = usable ? LogFixed{lo - 64.0 * inv_scale, inv_scale, wide, steep} : LogFixed{0.0, 0.0, 0, steep};
         ok[x] = usable ? 1 : 0;
     }
     if (!usable) return;
     for (uint32_t i = threadIdx.x; i < bins; i += blockDim.x) {
         const double e = 64.0 + rint((log10((double)L[i]) - lo) * ldexp(1.0, s));
         const uint32_t u = (uint32_t)fmin(e, cap - 1.0);
-        double delta = 0.0;
-        if (i + 1 < bins) delta = log10(1.0 + st * ((double)L[i + 1] / (double)L[i] - 1.0));
-        fix[i] = make_float2(__uint_as_float(u), (float)delta);
+        float delta = 0.0f;
+        if (i + 1 < bins) {
+            const double r = (double)L[i + 1] / (double)L[i] - 1.0;
+            delta = ((st * r) * (st * r) / (8.0 * 2.302585092994046) > kSecantBoundDev) ? __int_as_float(0x7fffffff)
+                                                                                       : (float)log10(1.0 + st * r);
+        }
+        fix[i] = make_float2(__uint_as_float(u), delta);
     }
 }
 

@@ -343,14 +343,16 @@ void build_tables(twisty_ctx *ctx, float ds, bool derivatives)
     }
     for (uint32_t i = 0; i < bins; ++i)
         if (!std::isfinite(host32[i])) fail(TWISTY_ERR_LUT_INVALID, "weight table has non-finite entries");
-    // compensated-form tables, the fixed-point one scaled for paths of this N. The
-    // fixed-point secant form is used only when its worst-case error is below 1e-7 per
-    // segment; otherwise the exact blend.
+    // compensated-form tables, the fixed-point one scaled for paths of this N. Bins where the
+    // fixed-point secant would err by more than 1e-7 per segment carry a NaN slope (paths
+    // crossing them are re-weighed through the linear table); a table with too many of
+    // them, or too wide a range, takes the exact blend.
     std::vector<float> lin, fix;
     double c0 = 0.0, inv_scale = 0.0, err = 0.0;
     int wide = 0;
-    const bool fixed_ok =
-          compensated_tables(host32.data(), bins, ctx->meta.step, p.num_segments, lin, fix, c0, inv_scale, wide, err);
+    uint32_t steep = 0;
+    const bool fixed_ok = compensated_tables(host32.data(), bins, ctx->meta.step, p.num_segments, lin, fix, c0,
+                                             inv_scale, wide, err, steep);
     ck(cudaMemcpyAsync(ctx->lintab.p, lin.data(), sizeof(float) * lin.size(), cudaMemcpyHostToDevice, st), "upload linear table");
     if (fixed_ok)
         ck(cudaMemcpyAsync(ctx->fixtab.p, fix.data(), sizeof(float) * fix.size(), cudaMemcpyHostToDevice, st),
@@ -358,7 +360,7 @@ void build_tables(twisty_ctx *ctx, float ds, bool derivatives)
     ck(cudaStreamSynchronize(st), "tables");
     ctx->secant_err = err;
     ctx->exact_blend = fixed_ok ? 0 : 1;
-    ctx->lf = fixed_ok ? LogFixed{c0, inv_scale, wide, 0} : LogFixed{0.0, 0.0, 0, 0};
+    ctx->lf = fixed_ok ? LogFixed{c0, inv_scale, wide, (int32_t)steep} : LogFixed{0.0, 0.0, 0, (int32_t)steep};
     std::memcpy(ctx->lut_key, key, sizeof(key));
     ctx->lut_ready = true;
 }
@@ -570,6 +572,12 @@ void collect(twisty_ctx *ctx, twisty_result *res)
     res->setup_ms = ctx->setup_ms;
     res->perturb_ms = a;
     res->weighting_ms = b;
+    res->table_form = TWISTY_TABLE_NONE;
+    if (ctx->p.form == TWISTY_FORM_COMPENSATED) {
+        const bool exact = ctx->tuning.exact_blend || ctx->lf.inv_scale == 0.0 || ctx->spec.has_eval_shift;
+        res->table_form = exact ? TWISTY_TABLE_EXACT_BLEND : ctx->lf.wide ? TWISTY_TABLE_FIXED_WIDE : TWISTY_TABLE_FIXED_NARROW;
+        res->steep_bins = exact ? 0u : (uint32_t)ctx->lf.steep;
+    }
 }
 
 twisty_status guard(twisty_ctx *ctx, const std::function<void()> &f)
@@ -1304,7 +1312,7 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
     auto bucket_of = [&](const BatchShape &sh) -> Bucket & {
         for (Bucket &b : buckets)
             if (b.shape.group == sh.group && b.shape.spl == sh.spl && b.shape.warps == sh.warps && b.shape.exact == sh.exact &&
-                b.shape.clamp == sh.clamp && b.shape.lut_smem == sh.lut_smem)
+                b.shape.clamp == sh.clamp && b.shape.lut_smem == sh.lut_smem && b.shape.steep == sh.steep)
                 return b;
         buckets.push_back(Bucket{});
         buckets.back().shape = sh;
@@ -1312,16 +1320,25 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
     };
     for (uint32_t e = 0; e < n; ++e) {
         ExpHost &h = eh[e];
-        const bool exact = okv[e] == 0;
+        // Fixed-point tables staged in shared memory all take the kernel with the steep-bin
+        // fallback (whether or not this table has steep bins: one bucket per shape balances
+        // better than two, measured 5 % faster on the batching workload); a table that does
+        // not fit in shared memory takes the plain fixed-point kernel, or the exact blend
+        // when it has steep bins.
+        const bool smem_fits = batch_smem_bytes(BatchShape{h.t.group, h.t.spl, h.t.warps_per_block, 0, 1, 0, 1}, bins) <=
+                               227 * 1024;
+        const bool exact = okv[e] == 0 || (lf[e].steep > 0 && !smem_fits);
+        const bool steep = !exact && smem_fits;
         BatchExpHost &b = bh[e];
         b.spec = h.spec;
         b.meta = h.meta;
         b.lf = exact ? LogFixed{0.0, 0.0, 0, 0} : lf[e];
         b.tab = (exact ? B.lin.as<float2>() : B.fix.as<float2>()) + (size_t)e * bins;
+        b.lin = B.lin.as<float2>() + (size_t)e * bins;
         b.init_seg = B.init_seg.as<float>() + h.seg_off;
         b.out_offset = h.chain_off;
         BatchShape sh{h.t.group, h.t.spl, h.t.warps_per_block, exact ? 1 : 0, 1,
-                      (exact || comp_table_needs_clamp(h.spec.inv_ds, h.meta)) ? 1 : 0};
+                      (exact || comp_table_needs_clamp(h.spec.inv_ds, h.meta)) ? 1 : 0, steep ? 1 : 0};
         if (batch_smem_bytes(sh, bins) > 227 * 1024) sh.lut_smem = 0;
         if (!batch_shape_supported(sh, h.N, h.spec.k_eff) || batch_smem_bytes(sh, bins) > 227 * 1024)
             fail(TWISTY_ERR_UNSUPPORTED, exp_msg(e, "no batched kernel shape fits"));
@@ -1418,6 +1435,9 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
         r.num_chains = eh[e].spec.n_chains;
         r.steps_per_chain = eh[e].spec.steps;
         r.setup_ms = setup_ms;
+        const bool fixed = bh[e].lf.inv_scale != 0.0;
+        r.table_form = fixed ? (lf[e].wide ? TWISTY_TABLE_FIXED_WIDE : TWISTY_TABLE_FIXED_NARROW) : TWISTY_TABLE_EXACT_BLEND;
+        r.steep_bins = fixed ? (uint32_t)lf[e].steep : 0u;
         r.perturb_ms = sum_ms / iters;
         r.weighting_ms = 0.0;
         r.total_ms = total_ms;
