@@ -67,7 +67,7 @@ template <int G, int SPL, bool EXACT, bool LS, bool CL, bool SP>
 cudaError_t batch_t(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items, uint32_t *counter,
                     ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st)
 {
-    constexpr int MAXT = (SPL >= 16 || G == 8) ? 512 : 1024;
+    constexpr int MAXT = (SPL >= 12 || G == 8) ? 512 : 1024;
     if (s.warps * 32 > MAXT) return cudaErrorInvalidConfiguration;
     auto kern = batch_kernel<G, SPL, EXACT, LS, CL, SP, MAXT>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -79,7 +79,7 @@ cudaError_t batch_t(const BatchShape &s, const BatchExp *exps, const uint2 *item
 template <int G, int SPL, bool EXACT, bool LS, bool CL, bool SP>
 int batch_occ_t(const BatchShape &s, size_t smem)
 {
-    constexpr int MAXT = (SPL >= 16 || G == 8) ? 512 : 1024;
+    constexpr int MAXT = (SPL >= 12 || G == 8) ? 512 : 1024;
     auto kern = batch_kernel<G, SPL, EXACT, LS, CL, SP, MAXT>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
     int nb = 0;
@@ -138,7 +138,7 @@ void batch_pack_experiments(const BatchExpHost *in, uint32_t n, void *dst)
 bool batch_shape_supported(const BatchShape &s, uint32_t n_max, uint32_t k_eff)
 {
     CompTuning t{s.group, s.spl, s.warps, s.exact};
-    const int maxt = (s.spl >= 16 || s.group == 8) ? 512 : 1024;
+    const int maxt = (s.spl >= 12 || s.group == 8) ? 512 : 1024;
     return comp_tuning_supported(t, n_max, k_eff) && s.warps * 32 <= maxt;
 }
 
@@ -158,13 +158,17 @@ int batch_blocks_per_sm(const BatchShape &s, int bins)
     TWISTY_O(8, 2)
     TWISTY_O(8, 4)
     TWISTY_O(8, 8)
+    TWISTY_O(8, 12)
     TWISTY_O(8, 16)
     TWISTY_O(16, 4)
     TWISTY_O(16, 8)
+    TWISTY_O(16, 12)
     TWISTY_O(16, 16)
     TWISTY_O(32, 4)
     TWISTY_O(32, 8)
+    TWISTY_O(32, 12)
     TWISTY_O(32, 16)
+    TWISTY_O(32, 24)
     TWISTY_O(32, 32)
 #undef TWISTY_O
     return 0;
@@ -180,13 +184,17 @@ cudaError_t launch_batch(const BatchShape &s, const void *d_exps, const uint2 *d
     TWISTY_B(8, 2)
     TWISTY_B(8, 4)
     TWISTY_B(8, 8)
+    TWISTY_B(8, 12)
     TWISTY_B(8, 16)
     TWISTY_B(16, 4)
     TWISTY_B(16, 8)
+    TWISTY_B(16, 12)
     TWISTY_B(16, 16)
     TWISTY_B(32, 4)
     TWISTY_B(32, 8)
+    TWISTY_B(32, 12)
     TWISTY_B(32, 16)
+    TWISTY_B(32, 24)
     TWISTY_B(32, 32)
 #undef TWISTY_B
     return cudaErrorInvalidValue;
