@@ -211,9 +211,18 @@ __device__ __forceinline__ void build_fast(const LutBuildSpec &s, uint32_t bin0,
     const bool zero_k = !(kds > 0.0);
     double st, ct;
     sincos(kds * h, &st, &ct);
+    // Past p_cut the weight is exactly zero in FP64 (bds phase(p) <= bds np_d, so the exponent
+    // is below -750 and exp underflows to 0): those nodes add nothing and are not visited.
+    // With the regulariser of the usual configurations most of [0, 10/eps] lies there.
+    uint32_t n_eff = n;
+    if (reg > 0.0) {
+        const double p_cut = sqrt(2.0 * (bds * np_d + 750.0)) / reg;
+        const double j_cut = ceil(p_cut / h) + 2.0;
+        if (j_cut < (double)n) n_eff = (uint32_t)j_cut;
+    }
     Neumaier acc;
-    for (uint32_t c0 = 0; c0 < n; c0 += kFastChunk) {
-        const uint32_t cn = min(kFastChunk, n - c0);
+    for (uint32_t c0 = 0; c0 < n_eff; c0 += kFastChunk) {
+        const uint32_t cn = min(kFastChunk, n_eff - c0);
         __syncthreads();   // the previous chunk is consumed
         for (uint32_t i = threadIdx.x; i < cn; i += blockDim.x) {
             const uint32_t j = c0 + i;

@@ -20,6 +20,8 @@
 #include <mutex>
 #include <new>
 #include <sstream>
+#include <thread>
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -79,6 +81,18 @@ uint64_t seed_of(uint32_t s)
 
 }  // namespace
 
+// Device buffers of batched runs, kept by the context so that repeated batches of the same
+// size allocate nothing (DevBuf::ensure only grows).
+struct BatchBufs {
+    DevBuf specs, lut64, lut32, fix, lin, steps, nsegs, lf, ok, init_seg, exps, items, counters, chain_out, ranges, red;
+    void release()
+    {
+        DevBuf *all[] = {&specs, &lut64, &lut32, &fix, &lin, &steps, &nsegs, &lf, &ok, &init_seg, &exps, &items,
+                         &counters, &chain_out, &ranges, &red};
+        for (DevBuf *b : all) b->release();
+    }
+};
+
 struct twisty_ctx {
     twisty_params p{};
     int device = 0;
@@ -125,6 +139,7 @@ struct twisty_ctx {
     DevBuf init_pos, init_seg, state, chain_out, partials, reduce_out, norm_scratch;
     uint32_t kernels_per_launch = 0;
     bool launched = false;
+    BatchBufs batch;
 };
 
 namespace {
@@ -815,6 +830,7 @@ void twisty_destroy(twisty_ctx *ctx)
                       &ctx->init_pos, &ctx->init_seg, &ctx->state, &ctx->chain_out, &ctx->partials, &ctx->reduce_out,
                       &ctx->norm_scratch, &ctx->multi.dev};
     for (DevBuf *b : bufs) b->release();
+    ctx->batch.release();
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1094,17 +1110,6 @@ float twisty_min_arclength(const twisty_bc *bc, uint32_t n) { return bc ? twisty
 
 namespace {
 
-// Buffers of one batched pass, released however the pass ends.
-struct BatchBufs {
-    DevBuf specs, lut64, lut32, fix, lin, steps, nsegs, lf, ok, init_seg, exps, items, counters, chain_out, ranges, red;
-    ~BatchBufs()
-    {
-        DevBuf *all[] = {&specs, &lut64, &lut32, &fix, &lin, &steps, &nsegs, &lf, &ok, &init_seg, &exps, &items,
-                         &counters, &chain_out, &ranges, &red};
-        for (DevBuf *b : all) b->release();
-    }
-};
-
 // Streams, events and the graph of one batched pass.
 struct BatchGraph {
     std::vector<cudaStream_t> streams;
@@ -1173,9 +1178,10 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
     };
     std::vector<ExpHost> eh(n);
     std::vector<LutBuildSpec> specs(n);
-    std::vector<float> steps(n), segs;
+    std::vector<float> steps(n);
     std::vector<uint32_t> nsegs(n);
     uint32_t total_chains = 0;
+    uint32_t n_seg_floats = 0;
     for (uint32_t e = 0; e < n; ++e) {
         const twisty_experiment &x = ex[e];
         ExpHost &h = eh[e];
@@ -1216,15 +1222,9 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
         ls.step64 = ((2.0 / (double)h.ds) * 1.01) / (double)(bins - 1);
         steps[e] = h.meta.step;
         nsegs[e] = N;
-        // initial curve
-        std::vector<float> pos;
-        std::string err;
-        if (!bootstrap_curve(x.bc, N, p.bootstrap_seed + e, p.bootstrap_kind, pos, err))
-            fail(TWISTY_ERR_INFEASIBLE_GEOMETRY, exp_msg(e, err));
-        h.seg_off = (uint32_t)segs.size();
-        for (uint32_t i = 0; i < N; ++i)
-            for (int k = 0; k < 3; ++k) segs.push_back(pos[3 * (i + 1) + k] - pos[3 * i + k]);
-        h.log10_norm = normalizer_log10(ctx, N, h.ds, x.bc);
+        // the initial curve's segment vectors go to segs[seg_off .. seg_off + 3N) (below)
+        h.seg_off = n_seg_floats;
+        n_seg_floats += 3 * N;
         // kernel shape and chain layout: whole CTAs of chains, ~2048 steps per chain
         h.t = comp_default_tuning(N);
         tune_lookup(ctx->device_name, N, bins, h.t);
@@ -1264,8 +1264,9 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
         total_chains += c.n_chains;
     }
 
-    BatchBufs B;
-    // ---- tables, all experiments at once
+    BatchBufs &B = ctx->batch;
+    // ---- tables, all experiments at once (launched before the host builds the curves)
+    ck(B.init_seg.ensure(sizeof(float) * std::max<uint32_t>(1, n_seg_floats)), "alloc batch curves");
     ck(B.specs.ensure(sizeof(LutBuildSpec) * n), "alloc batch");
     ck(B.lut64.ensure(sizeof(double) * (size_t)bins * n), "alloc batch tables");
     ck(B.lut32.ensure(sizeof(float) * (size_t)bins * n), "alloc batch tables");
@@ -1291,12 +1292,46 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
     ck(launch_comp_tables_batch(n, bins, B.lut32.as<float>(), B.steps.as<float>(), B.nsegs.as<uint32_t>(),
                                 B.fix.as<float2>(), B.lin.as<float2>(), B.lf.as<LogFixed>(), B.ok.as<int>(), st),
        "batch compensated tables");
+    // ---- initial curves on host threads while the device builds the tables
+    std::vector<float> segs(n_seg_floats);
+    {
+        std::atomic<uint32_t> next{0};
+        std::atomic<bool> failed{false};
+        std::mutex err_mu;
+        uint32_t err_exp = n;
+        std::string err_msg;
+        auto work = [&] {
+            std::vector<float> pos;
+            std::string err;
+            for (;;) {
+                const uint32_t e = next.fetch_add(1);
+                if (e >= n || failed.load()) return;
+                const uint32_t N = eh[e].N;
+                if (!bootstrap_curve(ex[e].bc, N, p.bootstrap_seed + e, p.bootstrap_kind, pos, err)) {
+                    std::lock_guard<std::mutex> lk(err_mu);
+                    if (e < err_exp) { err_exp = e; err_msg = err; }
+                    failed.store(true);
+                    return;
+                }
+                float *dst = segs.data() + eh[e].seg_off;
+                for (uint32_t i = 0; i < N; ++i)
+                    for (int k = 0; k < 3; ++k) dst[3 * i + k] = pos[3 * (i + 1) + k] - pos[3 * i + k];
+            }
+        };
+        const uint32_t hw = std::max(1u, std::thread::hardware_concurrency());
+        const uint32_t nt = std::min<uint32_t>(std::min<uint32_t>(hw, 32u), std::max<uint32_t>(1, n / 16));
+        std::vector<std::thread> pool;
+        for (uint32_t t = 1; t < nt; ++t) pool.emplace_back(work);
+        work();
+        for (std::thread &t : pool) t.join();
+        if (failed.load()) fail(TWISTY_ERR_INFEASIBLE_GEOMETRY, exp_msg(err_exp, err_msg));
+    }
+    for (uint32_t e = 0; e < n; ++e) eh[e].log10_norm = normalizer_log10(ctx, eh[e].N, eh[e].ds, ex[e].bc);
     std::vector<LogFixed> lf(n);
     std::vector<int> okv(n);
+    ck(cudaMemcpyAsync(B.init_seg.p, segs.data(), sizeof(float) * segs.size(), cudaMemcpyHostToDevice, st), "upload curves");
     ck(cudaMemcpyAsync(lf.data(), B.lf.p, sizeof(LogFixed) * n, cudaMemcpyDeviceToHost, st), "read tables");
     ck(cudaMemcpyAsync(okv.data(), B.ok.p, sizeof(int) * n, cudaMemcpyDeviceToHost, st), "read tables");
-    ck(B.init_seg.ensure(sizeof(float) * segs.size()), "alloc batch curves");
-    ck(cudaMemcpyAsync(B.init_seg.p, segs.data(), sizeof(float) * segs.size(), cudaMemcpyHostToDevice, st), "upload curves");
     ck(cudaStreamSynchronize(st), "batch tables");
 
     // ---- experiments packed for the device, buckets by shape and table form
