@@ -162,6 +162,7 @@ cudaError_t launch_mode(int mode, const ChainSpec &c, const CompTuning &t, const
     TWISTY_CASE(8, 8)
     TWISTY_CASE(8, 12)
     TWISTY_CASE(8, 16)
+    TWISTY_CASE(8, 32)
     TWISTY_CASE(16, 4)
     TWISTY_CASE(16, 8)
     TWISTY_CASE(16, 12)
@@ -227,7 +228,8 @@ CompTuning comp_default_tuning(uint32_t n)
 
 bool comp_tuning_supported(const CompTuning &t, uint32_t n, uint32_t k_eff)
 {
-    const bool shape = (t.group == 8 && (t.spl == 2 || t.spl == 4 || t.spl == 8 || t.spl == 12 || t.spl == 16)) ||
+    const bool shape = (t.group == 8 && (t.spl == 2 || t.spl == 4 || t.spl == 8 || t.spl == 12 || t.spl == 16 ||
+                                         t.spl == 32)) ||
                        (t.group == 16 && (t.spl == 4 || t.spl == 8 || t.spl == 12 || t.spl == 16)) ||
                        (t.group == 32 && (t.spl == 4 || t.spl == 8 || t.spl == 12 || t.spl == 16 || t.spl == 24 ||
                                           t.spl == 32));

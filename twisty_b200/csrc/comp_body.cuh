@@ -138,9 +138,11 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float x)
 
 // Fractional bin index of |t_{i+1}-t_i|^2 and its bin. CLAMP handles tables whose curvature
 // range a path can leave; tables spanning [0, 2.02 N/S] (the reference's) cannot be left by
-// unit tangents (|t_{i+1}-t_i| <= 2). r >= 0 or NaN after this (NaN converts to bin 0 and
-// propagates through the interpolation fraction); the bound on the bin also keeps a
-// non-finite tangent, which only a degenerate zero-length chord can produce, in the table.
+// unit tangents (|t_{i+1}-t_i| <= 2). r >= 0 or NaN after the clamp. Returns the fraction
+// r - L within bin L. floor(r) comes without conversion instructions (which share the MUFU
+// pipe with the square root): r + 2^23 rounded toward -infinity carries floor(r) in its low
+// mantissa bits for 0 <= r < 2^23. NaN and infinity, which only a degenerate zero-length
+// chord can produce, land past the last bin, are bounded to it and get a NaN fraction.
 template <bool CLAMP>
 __device__ __forceinline__ float bin_of(float qq, const CompConsts &k, bool valid, uint32_t &clamped, int32_t &L)
 {
@@ -152,8 +154,9 @@ __device__ __forceinline__ float bin_of(float qq, const CompConsts &k, bool vali
             r = k.rmax;
         }
     }
-    L = min((int32_t)r, k.bins - 1);
-    return r;
+    const float fl = __fadd_rd(r, 8388608.0f);
+    L = (int32_t)min(__float_as_uint(fl) - 0x4B000000u, (uint32_t)k.bins - 1u);
+    return r - (fl - 8388608.0f);
 }
 
 // Walk the curvatures this lane owns: seg(i, qq, valid) for curvature i = base+m-1 (between
@@ -209,9 +212,8 @@ __device__ __forceinline__ double path_log10(uint32_t j, uint32_t N, const float
     float csum = 0.f, ks = 0.f, kc = 0.f;
     for_curvatures<G, SPL, false>(j, N, tan, next, [&](uint32_t i, float qq, bool valid) {
         int32_t L;
-        const float r = bin_of<CLAMP>(qq, k, valid, clamped, L);
-        if (valid) bin_sink(i, isnan(r) ? -1 : L);
-        const float frac = r - (float)L;
+        const float frac = bin_of<CLAMP>(qq, k, valid, clamped, L);
+        if (valid) bin_sink(i, isnan(frac) ? -1 : L);
         const float2 e = tab[L];
         if (EXACT) {
             const float term = __log2f(fmaf(frac * k.step, e.y, e.x)) * kLog10_2;
@@ -246,11 +248,11 @@ __device__ __forceinline__ unsigned long long path_fixed(uint32_t j, uint32_t gb
     float csum = 0.f;
     auto seg = [&](uint32_t, float qq, bool valid) {
         int32_t L;
-        const float r = bin_of<CLAMP>(qq, k, valid, clamped, L);
+        const float frac = bin_of<CLAMP>(qq, k, valid, clamped, L);
         const float2 e = tab[L];
         isum += valid ? __float_as_uint(e.x) : 0u;
         // a padding slot leaves the sum alone even where the slope is NaN (a steep bin)
-        const float c2 = fmaf(r - (float)L, e.y, csum);
+        const float c2 = fmaf(frac, e.y, csum);
         csum = valid ? c2 : csum;
     };
     if (N == (uint32_t)(G * SPL))
@@ -442,9 +444,9 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
         const float dx = bx - ax, dy = by - ay, dz = bz - az;
         int32_t L;
         uint32_t unused = 0;
-        const float r = bin_of<CLAMP>(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), kc, false, unused, L);
+        const float frac = bin_of<CLAMP>(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), kc, false, unused, L);
         const float2 e = s_tab[L];
-        const float cor = (r - (float)L) * e.y;
+        const float cor = frac * e.y;
         nan |= isnan(cor);   // a NaN curvature or a steep bin's NaN slope
         return __float_as_uint(e.x) + (uint32_t)__float2int_rn(cor * kc.fscale);
     };
