@@ -421,8 +421,8 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
     const uint32_t steps_c = real_chain ? ((chain == c.n_chains - 1) ? c.last_steps : c.steps) : 0;
     const uint32_t total = c.burn_in + c.steps;
     const uint32_t gchain = c.chain0 + (real_chain ? chain : 0);
-    // rotation rounds actually needed: sub-chains have at most k_eff segments
-    const uint32_t rounds = (c.k_eff + G - 1) / G;
+    // rotation rounds: sub-chains have at most k_eff segments (a step takes the warp's longest)
+    const uint32_t max_rounds = (c.k_eff + G - 1) / G;
     float lse_m = 0.f, lse_s = 0.f, lse_c = 0.f;  // exact form: running max (float) and Kahan sum
     unsigned long long lse_t = 0;                   // fixed form: running max as a path total
     uint32_t valid = 0, failed = 0, clamped = 0;
@@ -482,6 +482,11 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
             const float sn = __shfl_sync(FULL, psn, jj, G);
             const float cs = __shfl_sync(FULL, pcs, jj, G);
             const uint32_t right = left + k;
+            // rounds this step needs: the longest sub-chain among the warp's chains
+            uint32_t kmax = k;
+#pragma unroll
+            for (int o = G; o < 32; o <<= 1) kmax = max(kmax, __shfl_xor_sync(FULL, kmax, o));
+            const uint32_t rounds = min((kmax + G - 1) / G, max_rounds);
             // incremental form: the two end curvatures before the rotation (kappa_{left-1} and
             // kappa_{right-1}; left >= 1 and right <= N-1, so all four tangents exist)
             bool incr_now = false;
