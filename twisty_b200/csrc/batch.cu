@@ -67,7 +67,7 @@ template <int G, int SPL, bool EXACT, bool LS, bool CL, bool SP>
 cudaError_t batch_t(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items, uint32_t *counter,
                     ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st)
 {
-    constexpr int MAXT = (SPL >= 12 || G == 8) ? 512 : 1024;
+    constexpr int MAXT = (SPL >= 12 || G <= 8) ? 512 : 1024;
     if (s.warps * 32 > MAXT) return cudaErrorInvalidConfiguration;
     auto kern = batch_kernel<G, SPL, EXACT, LS, CL, SP, MAXT>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -79,7 +79,7 @@ cudaError_t batch_t(const BatchShape &s, const BatchExp *exps, const uint2 *item
 template <int G, int SPL, bool EXACT, bool LS, bool CL, bool SP>
 int batch_occ_t(const BatchShape &s, size_t smem)
 {
-    constexpr int MAXT = (SPL >= 12 || G == 8) ? 512 : 1024;
+    constexpr int MAXT = (SPL >= 12 || G <= 8) ? 512 : 1024;
     auto kern = batch_kernel<G, SPL, EXACT, LS, CL, SP, MAXT>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
     int nb = 0;
@@ -138,7 +138,7 @@ void batch_pack_experiments(const BatchExpHost *in, uint32_t n, void *dst)
 bool batch_shape_supported(const BatchShape &s, uint32_t n_max, uint32_t k_eff)
 {
     CompTuning t{s.group, s.spl, s.warps, s.exact};
-    const int maxt = (s.spl >= 12 || s.group == 8) ? 512 : 1024;
+    const int maxt = (s.spl >= 12 || s.group <= 8) ? 512 : 1024;
     return comp_tuning_supported(t, n_max, k_eff) && s.warps * 32 <= maxt;
 }
 
@@ -155,6 +155,8 @@ int batch_blocks_per_sm(const BatchShape &s, int bins)
     const size_t smem = batch_smem_bytes(s, (uint32_t)bins);
 #define TWISTY_O(GG, SS) \
     if (s.group == GG && s.spl == SS) return batch_occ_g<GG, SS>(s, smem);
+    TWISTY_O(4, 4)
+    TWISTY_O(4, 8)
     TWISTY_O(8, 2)
     TWISTY_O(8, 4)
     TWISTY_O(8, 8)
@@ -181,6 +183,8 @@ cudaError_t launch_batch(const BatchShape &s, const void *d_exps, const uint2 *d
     const size_t smem = batch_smem_bytes(s, (uint32_t)bins);
 #define TWISTY_B(GG, SS) \
     if (s.group == GG && s.spl == SS) return batch_g<GG, SS>(s, exps, d_items, n_items, d_counter, out, bins, grid, smem, st);
+    TWISTY_B(4, 4)
+    TWISTY_B(4, 8)
     TWISTY_B(8, 2)
     TWISTY_B(8, 4)
     TWISTY_B(8, 8)

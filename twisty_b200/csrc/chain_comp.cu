@@ -157,6 +157,8 @@ cudaError_t launch_mode(int mode, const ChainSpec &c, const CompTuning &t, const
     if (t.group == GG && t.spl == SS) \
         return launch_g<GG, SS>(mode, exact, clamp, shift, steep, c, kc, t, init_seg, tab, out, block_partials, mb, smem, \
                                 blocks, st);
+    TWISTY_CASE(4, 4)
+    TWISTY_CASE(4, 8)
     TWISTY_CASE(8, 2)
     TWISTY_CASE(8, 4)
     TWISTY_CASE(8, 8)
@@ -208,12 +210,15 @@ bool comp_table_needs_clamp(float inv_ds, const LutMetaF &m)
 // per lane keep 16 independent table loads in flight per lane, which outweighs the halved
 // warp count above N = 64. The 12- and 24-segment shapes cover the N between powers of two
 // with less padding (measured: N = 192, 384, 768 18-27 % faster than the next power of two).
+// Up to N = 32, 4-lane groups put 8 chains in a warp, which share the per-step work of the
+// proposal broadcast, the group reductions and the log-sum-exp (N = 16: +23 %, 32: +12 %
+// over 8 lanes).
 CompTuning comp_default_tuning(uint32_t n)
 {
     CompTuning t;
     t.exact_blend = 0;
-    if (n <= 16) { t.group = 8; t.spl = 2; t.warps_per_block = 32; }
-    else if (n <= 32) { t.group = 8; t.spl = 4; t.warps_per_block = 32; }
+    if (n <= 16) { t.group = 4; t.spl = 4; t.warps_per_block = 32; }
+    else if (n <= 32) { t.group = 4; t.spl = 8; t.warps_per_block = 32; }
     else if (n <= 64) { t.group = 8; t.spl = 8; t.warps_per_block = 32; }
     else if (n <= 96) { t.group = 8; t.spl = 12; t.warps_per_block = 16; }
     else if (n <= 128) { t.group = 8; t.spl = 16; t.warps_per_block = 16; }
@@ -228,7 +233,8 @@ CompTuning comp_default_tuning(uint32_t n)
 
 bool comp_tuning_supported(const CompTuning &t, uint32_t n, uint32_t k_eff)
 {
-    const bool shape = (t.group == 8 && (t.spl == 2 || t.spl == 4 || t.spl == 8 || t.spl == 12 || t.spl == 16 ||
+    const bool shape = (t.group == 4 && (t.spl == 4 || t.spl == 8)) ||
+                       (t.group == 8 && (t.spl == 2 || t.spl == 4 || t.spl == 8 || t.spl == 12 || t.spl == 16 ||
                                          t.spl == 32)) ||
                        (t.group == 16 && (t.spl == 4 || t.spl == 8 || t.spl == 12 || t.spl == 16)) ||
                        (t.group == 32 && (t.spl == 4 || t.spl == 8 || t.spl == 12 || t.spl == 16 || t.spl == 24 ||

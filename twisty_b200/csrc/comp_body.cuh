@@ -508,7 +508,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
             // more than 4 rounds (8-lane groups) under the 64-register budget of 1024-thread
             // CTAs (SPL < 16): the rotation pass reloads its tangents instead of keeping every
             // round's in registers (measured: no spills, N <= 64 up to 27 % faster)
-            constexpr bool RELOAD = R > 4 && SPL < 16;
+            constexpr bool RELOAD = R > 4 && (SPL < 16 || G < 8);
             constexpr int RK = RELOAD ? 1 : R;
             float vx[RK], vy[RK], vz[RK];
             uint32_t va[RK], vb[RK];

@@ -1243,7 +1243,7 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
         c.absorption_factor = (double)std::exp(-p.absorption * h.ds);
         if (!comp_tuning_supported(h.t, N, c.k_eff))
             fail(TWISTY_ERR_UNSUPPORTED, exp_msg(e, "no compensated kernel shape for this N / max_sub_chain"));
-        const int maxt = (h.t.spl >= 12 || h.t.group == 8) ? 512 : 1024;
+        const int maxt = (h.t.spl >= 12 || h.t.group <= 8) ? 512 : 1024;
         h.t.warps_per_block = std::min(h.t.warps_per_block, maxt / 32);
         const uint64_t cpb = (uint64_t)h.t.warps_per_block * (32u / (uint32_t)h.t.group);
         uint64_t chains = p.num_chains;
@@ -1647,7 +1647,7 @@ twisty_status twisty_autotune(twisty_ctx *ctx, const twisty_bc *bc, uint64_t tri
         };
         std::vector<Cand> cands;
         const CompTuning def = comp_default_tuning(N);
-        for (int g : {8, 16, 32})
+        for (int g : {4, 8, 16, 32})
             for (int spl : {2, 4, 8, 12, 16, 24, 32})
                 for (int w = 4; w <= 32; w += 4) {
                     CompTuning t{g, spl, w, 0};
