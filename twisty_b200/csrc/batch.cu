@@ -1,120 +1,9 @@
-// batch.cu -- the batched persistent form: many experiments per launch (comp_body.cuh holds
-// the chain body).
-#include "comp_body.cuh"
+// batch.cu -- the host side of the batched persistent form: experiment packing, shape and
+// occupancy queries, and the launch, which dispatches to the kernel variants instantiated in
+// batch_shapes_{a,b}.cu (batch_launch.cuh holds the kernel; comp_body.cuh the chain body).
+#include "batch_launch.cuh"
 
 namespace twisty {
-namespace {
-
-// ---------------------------------------------------------------------------------------
-// Batched persistent form: many experiments (uneven N, S, mu_s, eps) per launch. Work items
-// are (experiment, first chain of a CTA's worth of chains), sorted by cost; persistent CTAs
-// pull items from a device counter (atomicAdd), stage that experiment's table in shared
-// memory (or read it through L1), and run their chains with chain_body.
-// ---------------------------------------------------------------------------------------
-struct BatchExp {
-    ChainSpec spec;
-    CompConsts kc;
-    const float2 *tab;
-    const float2 *lin;       // linear table (the fallback of steep bins in the fixed-point form)
-    const float *init_seg;
-    double log10_abs;
-    uint32_t out_offset;
-    uint32_t pad;
-};
-
-template <int G, int SPL, bool EXACT, bool LUT_SMEM, bool CLAMP, bool STEEP, int MAXT>
-__global__ void __launch_bounds__(MAXT, 1) batch_kernel(const BatchExp *__restrict__ exps,
-                                                        const uint2 *__restrict__ items, uint32_t n_items,
-                                                        uint32_t *__restrict__ counter, ChainOut *__restrict__ out,
-                                                        int bins)
-{
-    extern __shared__ float4 smem4[];
-    __shared__ uint32_t s_item;
-    const int tab_f4 = LUT_SMEM ? (bins + 1) / 2 : 0;
-    unsigned char *s_state = reinterpret_cast<unsigned char *>(smem4 + tab_f4);
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t q = lane / G, j = lane % G;
-    constexpr int CPW = 32 / G;
-    using Lay = Layout<G, SPL>;
-    unsigned char *wb = s_state + (size_t)warp * Lay::WARP_BYTES;
-    const Planes st{reinterpret_cast<float2 *>(wb), reinterpret_cast<float *>(wb + Lay::XY_BYTES),
-                    reinterpret_cast<float *>(wb + Lay::XY_BYTES + Lay::Z_BYTES)};
-    for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1u);
-        __syncthreads();
-        const uint32_t item = s_item;
-        if (item >= n_items) break;
-        const uint2 it = items[item];
-        const BatchExp &e = exps[it.x];
-        const float2 *tab = e.tab;
-        if (LUT_SMEM) {
-            stage_table(smem4, e.tab, bins);
-            tab = reinterpret_cast<const float2 *>(smem4);
-        }
-        __syncthreads();
-        ModeArgs ma{};
-        ma.log10_abs = e.log10_abs;
-        ma.lin = e.lin;
-        const uint32_t chain = it.y + warp * CPW + q;
-        chain_body<G, SPL, EXACT, CLAMP, false, kModeForward, false, STEEP>(e.spec, e.kc, e.init_seg, tab, st, q * G, j,
-                                                                            chain, chain < e.spec.n_chains,
-                                                                            out + e.out_offset, ma);
-        __syncthreads();
-    }
-}
-
-template <int G, int SPL, bool EXACT, bool LS, bool CL, bool SP>
-cudaError_t batch_t(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items, uint32_t *counter,
-                    ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st)
-{
-    constexpr int MAXT = (SPL >= 12 || G <= 8) ? 512 : 1024;
-    if (s.warps * 32 > MAXT) return cudaErrorInvalidConfiguration;
-    auto kern = batch_kernel<G, SPL, EXACT, LS, CL, SP, MAXT>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    kern<<<grid, s.warps * 32, smem, st>>>(exps, items, n_items, counter, out, bins);
-    return cudaGetLastError();
-}
-
-template <int G, int SPL, bool EXACT, bool LS, bool CL, bool SP>
-int batch_occ_t(const BatchShape &s, size_t smem)
-{
-    constexpr int MAXT = (SPL >= 12 || G <= 8) ? 512 : 1024;
-    auto kern = batch_kernel<G, SPL, EXACT, LS, CL, SP, MAXT>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
-    int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, s.warps * 32, smem) != cudaSuccess) return 0;
-    return nb;
-}
-
-// Instantiated: exact tables with clamping (table in shared memory or read through L1);
-// fixed-point tables with or without clamping, in shared memory with the steep-bin fallback
-// or read through L1 without it.
-template <int G, int SPL>
-int batch_occ_g(const BatchShape &s, size_t smem)
-{
-    if (s.exact) return s.lut_smem ? batch_occ_t<G, SPL, true, true, true, false>(s, smem)
-                                   : batch_occ_t<G, SPL, true, false, true, false>(s, smem);
-    if (s.lut_smem != s.steep) return 0;
-    if (s.steep) return s.clamp ? batch_occ_t<G, SPL, false, true, true, true>(s, smem)
-                                : batch_occ_t<G, SPL, false, true, false, true>(s, smem);
-    return s.clamp ? batch_occ_t<G, SPL, false, false, true, false>(s, smem)
-                   : batch_occ_t<G, SPL, false, false, false, false>(s, smem);
-}
-
-template <int G, int SPL>
-cudaError_t batch_g(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items, uint32_t *counter,
-                    ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st)
-{
-#define TWISTY_BT(E, LS, CL, SP) batch_t<G, SPL, E, LS, CL, SP>(s, exps, items, n_items, counter, out, bins, grid, smem, st)
-    if (s.exact) return s.lut_smem ? TWISTY_BT(true, true, true, false) : TWISTY_BT(true, false, true, false);
-    if (s.lut_smem != s.steep) return cudaErrorInvalidValue;
-    if (s.steep) return s.clamp ? TWISTY_BT(false, true, true, true) : TWISTY_BT(false, true, false, true);
-    return s.clamp ? TWISTY_BT(false, false, true, false) : TWISTY_BT(false, false, false, false);
-#undef TWISTY_BT
-}
-
-}  // namespace
 
 // ------------------------------------------------------------------------- batched form
 size_t batch_exp_bytes() { return sizeof(BatchExp); }
@@ -153,26 +42,8 @@ int batch_chains_per_block(const BatchShape &s) { return s.warps * (32 / s.group
 int batch_blocks_per_sm(const BatchShape &s, int bins)
 {
     const size_t smem = batch_smem_bytes(s, (uint32_t)bins);
-#define TWISTY_O(GG, SS) \
-    if (s.group == GG && s.spl == SS) return batch_occ_g<GG, SS>(s, smem);
-    TWISTY_O(4, 4)
-    TWISTY_O(4, 8)
-    TWISTY_O(8, 2)
-    TWISTY_O(8, 4)
-    TWISTY_O(8, 8)
-    TWISTY_O(8, 12)
-    TWISTY_O(8, 16)
-    TWISTY_O(16, 4)
-    TWISTY_O(16, 8)
-    TWISTY_O(16, 12)
-    TWISTY_O(16, 16)
-    TWISTY_O(32, 4)
-    TWISTY_O(32, 8)
-    TWISTY_O(32, 12)
-    TWISTY_O(32, 16)
-    TWISTY_O(32, 24)
-    TWISTY_O(32, 32)
-#undef TWISTY_O
+    int occ = 0;
+    if (batch_shapes_a_occ(s, smem, occ) || batch_shapes_b_occ(s, smem, occ)) return occ;
     return 0;
 }
 
@@ -181,26 +52,10 @@ cudaError_t launch_batch(const BatchShape &s, const void *d_exps, const uint2 *d
 {
     const BatchExp *exps = static_cast<const BatchExp *>(d_exps);
     const size_t smem = batch_smem_bytes(s, (uint32_t)bins);
-#define TWISTY_B(GG, SS) \
-    if (s.group == GG && s.spl == SS) return batch_g<GG, SS>(s, exps, d_items, n_items, d_counter, out, bins, grid, smem, st);
-    TWISTY_B(4, 4)
-    TWISTY_B(4, 8)
-    TWISTY_B(8, 2)
-    TWISTY_B(8, 4)
-    TWISTY_B(8, 8)
-    TWISTY_B(8, 12)
-    TWISTY_B(8, 16)
-    TWISTY_B(16, 4)
-    TWISTY_B(16, 8)
-    TWISTY_B(16, 12)
-    TWISTY_B(16, 16)
-    TWISTY_B(32, 4)
-    TWISTY_B(32, 8)
-    TWISTY_B(32, 12)
-    TWISTY_B(32, 16)
-    TWISTY_B(32, 24)
-    TWISTY_B(32, 32)
-#undef TWISTY_B
+    cudaError_t e = cudaSuccess;
+    if (batch_shapes_a_launch(s, exps, d_items, n_items, d_counter, out, bins, grid, smem, st, e) ||
+        batch_shapes_b_launch(s, exps, d_items, n_items, d_counter, out, bins, grid, smem, st, e))
+        return e;
     return cudaErrorInvalidValue;
 }
 

@@ -1,53 +1,10 @@
-// chain_comp.cu -- single-run kernels of the compensated form (comp_body.cuh holds the chain
-// body): the chain kernel in its forward, export, adjoint and incremental variants, the
-// compensated weigher of given paths, their launchers and the kernel-shape table.
-#include "comp_body.cuh"
+// chain_comp.cu -- single-run entry points of the compensated form: the weigher of given
+// paths, the launchers and the kernel-shape table. The chain kernel (comp_launch.cuh, body in
+// comp_body.cuh) is instantiated per shape in comp_shapes_{a..e}.cu, compiled in parallel.
+#include "comp_launch.cuh"
 
 namespace twisty {
 namespace {
-
-template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MAXT, int MODE, bool INCR, bool STEEP>
-__global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompConsts kc,
-                                                             const float *__restrict__ init_seg,
-                                                             const float2 *__restrict__ tab_g,
-                                                             ChainOut *__restrict__ out,
-                                                             double2 *__restrict__ block_partials, ModeArgs ma)
-{
-    extern __shared__ float4 smem4[];
-    const int bins = kc.bins;
-    const float2 *s_tab = reinterpret_cast<const float2 *>(smem4);
-    const int tab_f4 = (bins + 1) / 2;  // float2 entries, padded to float4
-    unsigned char *s_state = reinterpret_cast<unsigned char *>(smem4 + tab_f4);
-    const int warps = blockDim.x >> 5;
-    using Lay = Layout<G, SPL>;
-    double *s_res = reinterpret_cast<double *>(s_state + (size_t)warps * Lay::WARP_BYTES);
-    stage_table(smem4, tab_g, bins);
-    __syncthreads();
-
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t q = lane / G, j = lane % G;
-    constexpr int CPW = 32 / G;
-    const uint32_t chain = (blockIdx.x * warps + warp) * CPW + q;
-    unsigned char *wb = s_state + (size_t)warp * Lay::WARP_BYTES;
-    const Planes pl{reinterpret_cast<float2 *>(wb), reinterpret_cast<float *>(wb + Lay::XY_BYTES),
-                    reinterpret_cast<float *>(wb + Lay::XY_BYTES + Lay::Z_BYTES)};
-    const double cl = chain_body<G, SPL, EXACT, CLAMP, SHIFT, MODE, INCR, STEEP>(c, kc, init_seg, s_tab, pl, q * G, j,
-                                                                                 chain, chain < c.n_chains, out, ma);
-    if (j == 0) s_res[warp * CPW + q] = cl;
-    __syncthreads();
-    // Per-CTA log-sum-exp of the chains, rescaled by the block maximum (FP64).
-    if (warp == 0 && block_partials) {
-        const int nres = warps * CPW;
-        double mx = -INFINITY;
-        for (int i = lane; i < nres; i += 32) mx = fmax(mx, s_res[i]);
-        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(FULL, mx, o));
-        double sum = 0.0;
-        if (mx > -INFINITY)
-            for (int i = lane; i < nres; i += 32) sum += (s_res[i] > -INFINITY) ? exp10(s_res[i] - mx) : 0.0;
-        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(FULL, sum, o);
-        if (lane == 0) block_partials[blockIdx.x] = make_double2(mx, sum);
-    }
-}
 
 // Compensated weigher of given paths: one group of 32 lanes per path; tangents from the
 // positions, normalised here.
@@ -91,51 +48,6 @@ __global__ void __launch_bounds__(256) weigh_comp_kernel(const float *__restrict
     }
 }
 
-// ------------------------------------------------------------------------------ launchers
-template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MODE, bool INCR = false, bool STEEP = false>
-cudaError_t launch_t(const ChainSpec &c, const CompConsts &kc, int warps, const float *init_seg, const float2 *tab,
-                     ChainOut *out, double2 *partials, const ModeArgs &ma, size_t smem, uint32_t blocks, cudaStream_t st)
-{
-    constexpr int MAXT = (SPL >= 12) ? 512 : 1024;
-    if (warps * 32 > MAXT) return cudaErrorInvalidConfiguration;
-    auto kern = comp_chain_kernel<G, SPL, EXACT, CLAMP, SHIFT, MAXT, MODE, INCR, STEEP>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    kern<<<blocks, warps * 32, smem, st>>>(c, kc, init_seg, tab, out, partials, ma);
-    return cudaGetLastError();
-}
-
-// Instantiated variants: forward (fixed/exact x clamp/no clamp, plus an exact+clamp+shift
-// variant for receiver-shifted evaluation), export (fixed/exact with clamp), adjoint (exact);
-// the fixed-point forward, incremental and export variants again with the steep-bin fallback.
-template <int G, int SPL>
-cudaError_t launch_g(int mode, bool exact, bool clamp, bool shift, bool steep, const ChainSpec &c,
-                     const CompConsts &kc, const CompTuning &t, const float *init_seg, const float2 *tab,
-                     ChainOut *out, double2 *partials, const ModeArgs &ma, size_t smem, uint32_t blocks,
-                     cudaStream_t st)
-{
-    const int w = t.warps_per_block;
-#define TWISTY_L(E, CL, SH, MO) launch_t<G, SPL, E, CL, SH, MO>(c, kc, w, init_seg, tab, out, partials, ma, smem, blocks, st)
-#define TWISTY_S(CL, MO, IN) \
-    launch_t<G, SPL, false, CL, false, MO, IN, true>(c, kc, w, init_seg, tab, out, partials, ma, smem, blocks, st)
-    if (mode == kModeAdjoint) return TWISTY_L(true, true, false, kModeAdjoint);
-    if (mode == kModeExport) {
-        if (exact) return TWISTY_L(true, true, false, kModeExport);
-        return steep ? TWISTY_S(true, kModeExport, false) : TWISTY_L(false, true, false, kModeExport);
-    }
-    if (shift) return TWISTY_L(true, true, true, kModeForward);
-    if (exact) return clamp ? TWISTY_L(true, true, false, kModeForward) : TWISTY_L(true, false, false, kModeForward);
-    if (clamp) return steep ? TWISTY_S(true, kModeForward, false) : TWISTY_L(false, true, false, kModeForward);
-    if (c.incr_resync > 1)
-        return steep ? TWISTY_S(false, kModeForward, true)
-                     : launch_t<G, SPL, false, false, false, kModeForward, true>(c, kc, w, init_seg, tab, out, partials,
-                                                                                  ma, smem, blocks, st);
-    return steep ? TWISTY_S(false, kModeForward, false) : TWISTY_L(false, false, false, kModeForward);
-#undef TWISTY_S
-#undef TWISTY_L
-}
-
-
 cudaError_t launch_mode(int mode, const ChainSpec &c, const CompTuning &t, const float *init_seg, const float2 *fixtab,
                         const float2 *lintab, LutMetaF m, ChainOut *out, double2 *block_partials, const ModeArgs &ma,
                         const LogFixed &lf, cudaStream_t st)
@@ -153,29 +65,11 @@ cudaError_t launch_mode(int mode, const ChainSpec &c, const CompTuning &t, const
     const bool steep = !exact && lf.steep > 0;
     ModeArgs mb = ma;
     mb.lin = lintab;
-#define TWISTY_CASE(GG, SS) \
-    if (t.group == GG && t.spl == SS) \
-        return launch_g<GG, SS>(mode, exact, clamp, shift, steep, c, kc, t, init_seg, tab, out, block_partials, mb, smem, \
-                                blocks, st);
-    TWISTY_CASE(4, 4)
-    TWISTY_CASE(4, 8)
-    TWISTY_CASE(8, 2)
-    TWISTY_CASE(8, 4)
-    TWISTY_CASE(8, 8)
-    TWISTY_CASE(8, 12)
-    TWISTY_CASE(8, 16)
-    TWISTY_CASE(8, 32)
-    TWISTY_CASE(16, 4)
-    TWISTY_CASE(16, 8)
-    TWISTY_CASE(16, 12)
-    TWISTY_CASE(16, 16)
-    TWISTY_CASE(32, 4)
-    TWISTY_CASE(32, 8)
-    TWISTY_CASE(32, 12)
-    TWISTY_CASE(32, 16)
-    TWISTY_CASE(32, 24)
-    TWISTY_CASE(32, 32)
-#undef TWISTY_CASE
+    const CompLaunch a{mode, exact, clamp, shift, steep, c, kc, t, init_seg, tab, out, block_partials, mb, smem, blocks, st};
+    cudaError_t e = cudaSuccess;
+    if (launch_comp_shapes_a(a, e) || launch_comp_shapes_b(a, e) || launch_comp_shapes_c(a, e) ||
+        launch_comp_shapes_d(a, e) || launch_comp_shapes_e(a, e))
+        return e;
     return cudaErrorInvalidValue;
 }
 

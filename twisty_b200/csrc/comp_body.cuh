@@ -57,14 +57,8 @@
 #include <cfloat>
 
 namespace twisty {
-namespace {
 
-constexpr uint32_t FULL = 0xffffffffu;
-constexpr int kMaxSubChain = 64;  // largest k the rotation rounds cover
-constexpr float kLog2_10 = 3.32192809488736234787f;
-constexpr float kLog10_2 = 0.30102999566398119521f;
-constexpr float kInvLn10 = 0.43429448190325182765f;
-
+// Shared by the translation units that instantiate the chain kernels (plain structs).
 struct CompConsts {
     float kscale;        // (N/S) / step : |t_{i+1}-t_i| -> fractional bin index
     float roff;          // -min_k / step
@@ -78,6 +72,32 @@ struct CompConsts {
     double lw_offset;    // (N-1) c0 of the fixed-point table
     double inv_scale;    // 2^-s of the fixed-point table
 };
+
+struct ModeArgs {
+    double log10_abs;    // log10 of the per-segment absorption factor
+    // linear table (L_i, L_{i+1} - L_i) of the fixed-point table's curve: paths that cross a
+    // steep bin (NaN slope) are re-weighed through it
+    const float2 *lin;
+    // export
+    float *exp_pos;      // [chains][steps][N+1][3]
+    double *exp_w;       // [chains][steps] log10 weights (absorption included, normaliser not)
+    float x0[3];
+    // adjoint
+    const float *lut;    // float table
+    const float *dmu;    // d table / d mu_s
+    const float *deps;   // d table / d eps
+    float ref_log10;     // log10 of the forward sum of path weights (normaliser and absorption excluded)
+    double *grad;        // [chains][6]: d/dmu_s, d/deps, d/dx, d/dy, d/dz (log10 units), sum of weights
+};
+
+namespace {
+
+constexpr uint32_t FULL = 0xffffffffu;
+constexpr int kMaxSubChain = 64;  // largest k the rotation rounds cover
+constexpr float kLog2_10 = 3.32192809488736234787f;
+constexpr float kLog10_2 = 0.30102999566398119521f;
+constexpr float kInvLn10 = 0.43429448190325182765f;
+
 
 __device__ __forceinline__ float sqrt_approx(float x)
 {
@@ -293,22 +313,6 @@ struct Planes {
 
 enum { kModeForward = 0, kModeExport = 1, kModeAdjoint = 2 };
 
-struct ModeArgs {
-    double log10_abs;    // log10 of the per-segment absorption factor
-    // linear table (L_i, L_{i+1} - L_i) of the fixed-point table's curve: paths that cross a
-    // steep bin (NaN slope) are re-weighed through it
-    const float2 *lin;
-    // export
-    float *exp_pos;      // [chains][steps][N+1][3]
-    double *exp_w;       // [chains][steps] log10 weights (absorption included, normaliser not)
-    float x0[3];
-    // adjoint
-    const float *lut;    // float table
-    const float *dmu;    // d table / d mu_s
-    const float *deps;   // d table / d eps
-    float ref_log10;     // log10 of the forward sum of path weights (normaliser and absorption excluded)
-    double *grad;        // [chains][6]: d/dmu_s, d/deps, d/dx, d/dy, d/dz (log10 units), sum of weights
-};
 
 // Receiver-position gradient of one path's log10 weight, computed by one lane from the last
 // three segments: moving the receiver moves points N-1 and N together, so only the segment
