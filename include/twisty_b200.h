@@ -129,6 +129,11 @@ typedef struct twisty_params {
        curvatures a rotation changes and recomputes it in full every R-th weighted step
        (an algorithmic shortcut, reported separately; fixed-point tables without clamping) */
     uint32_t incremental_resync;
+    /* where the compensated form keeps the weight table (no reference counterpart): 0 = chosen
+       from its size (shared memory when it fits beside a full CTA of chain state, else read
+       through L1), 1 = shared memory (fewer warps per CTA for large tables), 2 = through L1.
+       Path export, the adjoint, receiver-shifted and incremental runs always stage it. */
+    uint32_t comp_table_memory;
 } twisty_params;
 
 /* ExperimentRunner::ExperimentResults (Twisty/ExperimentRunner.h:73-82). */

@@ -80,6 +80,7 @@ class Params(C.Structure):
         ("comp_spl", C.c_uint32),
         ("comp_warps", C.c_uint32),
         ("incremental_resync", C.c_uint32),
+        ("comp_table_memory", C.c_uint32),
     ]
 
 

@@ -145,7 +145,7 @@ uint32_t comp_default_chains(uint32_t n, int sm_count)
 
 size_t comp_smem_bytes(const CompTuning &t, uint32_t bins)
 {
-    const size_t tab = (size_t)((bins + 1) / 2) * sizeof(float4);
+    const size_t tab = t.lut_global ? 0 : (size_t)((bins + 1) / 2) * sizeof(float4);
     const size_t state = (size_t)t.warps_per_block * warp_state_bytes(t.group, t.spl);
     const size_t res = (size_t)t.warps_per_block * (32 / t.group) * sizeof(double);
     return tab + state + res;

@@ -32,7 +32,9 @@ bool launch_comp_shapes_e(const CompLaunch &a, cudaError_t &e);   // 32 x {16, 2
 
 namespace {
 
-template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MAXT, int MODE, bool INCR, bool STEEP>
+// LUTG: the table is gathered from global memory through L1 (tables too large to stage next to
+// the chain state); otherwise each CTA stages it in shared memory first.
+template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MAXT, int MODE, bool INCR, bool STEEP, bool LUTG>
 __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompConsts kc,
                                                              const float *__restrict__ init_seg,
                                                              const float2 *__restrict__ tab_g,
@@ -41,13 +43,13 @@ __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompCo
 {
     extern __shared__ float4 smem4[];
     const int bins = kc.bins;
-    const float2 *s_tab = reinterpret_cast<const float2 *>(smem4);
-    const int tab_f4 = (bins + 1) / 2;  // float2 entries, padded to float4
+    const float2 *s_tab = LUTG ? tab_g : reinterpret_cast<const float2 *>(smem4);
+    const int tab_f4 = LUTG ? 0 : (bins + 1) / 2;  // float2 entries, padded to float4
     unsigned char *s_state = reinterpret_cast<unsigned char *>(smem4 + tab_f4);
     const int warps = blockDim.x >> 5;
     using Lay = Layout<G, SPL>;
     double *s_res = reinterpret_cast<double *>(s_state + (size_t)warps * Lay::WARP_BYTES);
-    stage_table(smem4, tab_g, bins);
+    if (!LUTG) stage_table(smem4, tab_g, bins);
     __syncthreads();
 
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -76,13 +78,14 @@ __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompCo
 }
 
 // ------------------------------------------------------------------------------ launchers
-template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MODE, bool INCR = false, bool STEEP = false>
+template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MODE, bool INCR = false, bool STEEP = false,
+          bool LUTG = false>
 cudaError_t launch_t(const ChainSpec &c, const CompConsts &kc, int warps, const float *init_seg, const float2 *tab,
                      ChainOut *out, double2 *partials, const ModeArgs &ma, size_t smem, uint32_t blocks, cudaStream_t st)
 {
     constexpr int MAXT = (SPL >= 12) ? 512 : 1024;
     if (warps * 32 > MAXT) return cudaErrorInvalidConfiguration;
-    auto kern = comp_chain_kernel<G, SPL, EXACT, CLAMP, SHIFT, MAXT, MODE, INCR, STEEP>;
+    auto kern = comp_chain_kernel<G, SPL, EXACT, CLAMP, SHIFT, MAXT, MODE, INCR, STEEP, LUTG>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     kern<<<blocks, warps * 32, smem, st>>>(c, kc, init_seg, tab, out, partials, ma);
@@ -91,7 +94,8 @@ cudaError_t launch_t(const ChainSpec &c, const CompConsts &kc, int warps, const 
 
 // Instantiated variants: forward (fixed/exact x clamp/no clamp, plus an exact+clamp+shift
 // variant for receiver-shifted evaluation), export (fixed/exact with clamp), adjoint (exact);
-// the fixed-point forward, incremental and export variants again with the steep-bin fallback.
+// the fixed-point forward, incremental and export variants again with the steep-bin fallback;
+// with the table in global memory (lut_global), the forward variants only.
 template <int G, int SPL>
 cudaError_t launch_g(int mode, bool exact, bool clamp, bool shift, bool steep, const ChainSpec &c,
                      const CompConsts &kc, const CompTuning &t, const float *init_seg, const float2 *tab,
@@ -99,6 +103,16 @@ cudaError_t launch_g(int mode, bool exact, bool clamp, bool shift, bool steep, c
                      cudaStream_t st)
 {
     const int w = t.warps_per_block;
+    if (t.lut_global) {
+        // table through L1: forward passes (fixed point with or without steep bins, exact blend)
+        if (mode != kModeForward || shift || c.incr_resync > 1) return cudaErrorInvalidConfiguration;
+#define TWISTY_G(E, CL, SP) \
+    launch_t<G, SPL, E, CL, false, kModeForward, false, SP, true>(c, kc, w, init_seg, tab, out, partials, ma, smem, blocks, st)
+        if (exact) return clamp ? TWISTY_G(true, true, false) : TWISTY_G(true, false, false);
+        if (steep) return clamp ? TWISTY_G(false, true, true) : TWISTY_G(false, false, true);
+        return clamp ? TWISTY_G(false, true, false) : TWISTY_G(false, false, false);
+#undef TWISTY_G
+    }
 #define TWISTY_L(E, CL, SH, MO) launch_t<G, SPL, E, CL, SH, MO>(c, kc, w, init_seg, tab, out, partials, ma, smem, blocks, st)
 #define TWISTY_S(CL, MO, IN) \
     launch_t<G, SPL, false, CL, false, MO, IN, true>(c, kc, w, init_seg, tab, out, partials, ma, smem, blocks, st)

@@ -388,7 +388,7 @@ bool params_from_node(const Node &root, twisty_params &p, twisty_bc *bc, std::st
     p.min_bound = 0.0f;
     p.max_bound = 10.0f / p.eps;  // ExperimentRunner.cpp:169-171
     // Optional B200 block: experimentParams.b200 { form, lutMode, maxSubChain, maxAngle, numChains, device,
-    // compGroup, compSpl, compWarps, incrementalResync }
+    // compGroup, compSpl, compWarps, incrementalResync, compTableMemory }
     if (const Node *b = ep->get("b200")) {
         if (b->kind != Node::Object) {
             err = "experimentParams.b200 must be a mapping";
@@ -405,6 +405,8 @@ bool params_from_node(const Node &root, twisty_params &p, twisty_bc *bc, std::st
         if (b->get("compWarps") && num(b, "compWarps", "b200.compWarps", v, err)) p.comp_warps = (uint32_t)v;
         if (b->get("incrementalResync") && num(b, "incrementalResync", "b200.incrementalResync", v, err))
             p.incremental_resync = (uint32_t)v;
+        if (b->get("compTableMemory") && num(b, "compTableMemory", "b200.compTableMemory", v, err))
+            p.comp_table_memory = (uint32_t)v;
         if (!err.empty()) return false;
     }
     if (bc) {

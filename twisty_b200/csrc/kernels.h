@@ -122,6 +122,8 @@ struct CompTuning {
     int spl;                 // segments per lane
     int warps_per_block;
     int exact_blend;         // 1: interpolate the linear table and take log2 (MUFU)
+    int lut_global = 0;      // 1: gather the table through L1 instead of staging it in shared memory
+                             // (forward passes only; the chain state keeps the shared memory)
 };
 CompTuning comp_default_tuning(uint32_t n_segments);
 bool comp_tuning_supported(const CompTuning &t, uint32_t n_segments, uint32_t k_eff);

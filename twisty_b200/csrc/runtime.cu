@@ -162,6 +162,7 @@ void validate(const twisty_params &p)
     if (p.max_sub_chain < 2) fail(TWISTY_ERR_INVALID_CONFIG, "max_sub_chain must be at least 2");
     if (!(p.max_angle >= 0.0f) || p.max_angle > 3.1415927f) fail(TWISTY_ERR_INVALID_CONFIG, "max_angle must be in [0, pi]");
     if (p.bootstrap_kind < 0 || p.bootstrap_kind > 2) fail(TWISTY_ERR_INVALID_CONFIG, "bootstrap_kind must be 0, 1 or 2");
+    if (p.comp_table_memory > 2) fail(TWISTY_ERR_INVALID_CONFIG, "comp_table_memory must be 0, 1 or 2");
 }
 
 void validate_bc(const twisty_bc *bc)
@@ -420,6 +421,26 @@ void layout(twisty_ctx *ctx, uint64_t paths, uint32_t requested, uint32_t max_st
     c.last_steps = (uint32_t)(paths - (C - 1) * L);
 }
 
+constexpr size_t kSmemCap = 227 * 1024;
+
+// Fewer warps per CTA until the table (when staged) and the chain state fit in shared memory;
+// fails when even 4 warps do not fit.
+void fit_table_smem(CompTuning &t, uint32_t bins, bool may_shrink)
+{
+    while (may_shrink && t.warps_per_block > 4 && comp_smem_bytes(t, bins) > kSmemCap) t.warps_per_block -= 4;
+    if (comp_smem_bytes(t, bins) > kSmemCap)
+        fail(TWISTY_ERR_UNSUPPORTED, "weight table too large to stage in shared memory");
+}
+
+// The context's shape for the passes that stage the table (export, adjoint).
+CompTuning staged_tuning(const twisty_ctx *ctx)
+{
+    CompTuning t = ctx->tuning;
+    t.lut_global = 0;
+    fit_table_smem(t, ctx->p.num_curvature_steps, true);
+    return t;
+}
+
 void prepare(twisty_ctx *ctx, const twisty_bc *bcp)
 {
     const double t0 = now_ms();
@@ -483,13 +504,27 @@ void prepare(twisty_ctx *ctx, const twisty_bc *bcp)
         if (p.comp_warps) ctx->tuning.warps_per_block = (int)p.comp_warps;
         ctx->tuning.exact_blend = ctx->exact_blend;
         if (!comp_tuning_supported(ctx->tuning, N, c.k_eff)) fail(TWISTY_ERR_UNSUPPORTED, "no compensated kernel shape for this N / max_sub_chain");
-        // a large table leaves less shared memory for chain state: fewer warps per CTA
-        const size_t smem_cap = 227 * 1024;
-        while (!p.comp_warps && ctx->tuning.warps_per_block > 4 &&
-               comp_smem_bytes(ctx->tuning, p.num_curvature_steps) > smem_cap)
-            ctx->tuning.warps_per_block -= 4;
-        if (comp_smem_bytes(ctx->tuning, p.num_curvature_steps) > smem_cap)
-            fail(TWISTY_ERR_UNSUPPORTED, "weight table too large to stage in shared memory");
+        // A table too large to stage beside the chain state costs warps per CTA; when staging it
+        // would leave fewer than 2/3 of the shape's warps, forward passes of the full recompute
+        // read it through L1 instead (measured on B200 with 10000- and 20000-bin tables: L1
+        // 4-23 % below a staged table at full occupancy, 12-53 % above one at 1/4 to 1/2 of
+        // the warps). comp_table_memory 1 / 2 force the choice.
+        ctx->tuning.lut_global = 0;
+        const bool can_global = c.incr_resync <= 1 && !c.has_eval_shift;
+        bool few_warps = false;
+        if (p.comp_table_memory == 0 && can_global) {
+            CompTuning staged = ctx->tuning;
+            while (!p.comp_warps && staged.warps_per_block > 4 && comp_smem_bytes(staged, p.num_curvature_steps) > kSmemCap)
+                staged.warps_per_block -= 4;
+            few_warps = comp_smem_bytes(staged, p.num_curvature_steps) > kSmemCap ||
+                        3 * staged.warps_per_block < 2 * ctx->tuning.warps_per_block;
+        }
+        if (p.comp_table_memory == 2 || few_warps) {
+            if (!can_global)
+                fail(TWISTY_ERR_UNSUPPORTED, "comp_table_memory 2 serves plain forward passes (no incremental or shifted runs)");
+            ctx->tuning.lut_global = 1;
+        }
+        fit_table_smem(ctx->tuning, p.num_curvature_steps, p.comp_warps == 0);
         if (!requested)
             requested = (uint32_t)ctx->sm_count * (uint32_t)ctx->tuning.warps_per_block * (32u / (uint32_t)ctx->tuning.group);
     } else {
@@ -1524,7 +1559,7 @@ twisty_status twisty_export_paths(twisty_ctx *ctx, const twisty_bc *bc, const ch
                 } else if (ctx->p.form == TWISTY_FORM_COMPENSATED) {
                     if (ce.has_eval_shift) fail(TWISTY_ERR_UNSUPPORTED, "eval_end_shift applies to forward passes of the compensated form only");
                     const float x0[3] = {bc->start_pos.x, bc->start_pos.y, bc->start_pos.z};
-                    ck(launch_comp_export(ce, ctx->tuning, ctx->init_seg.as<float>(), ctx->fixtab.as<float2>(),
+                    ck(launch_comp_export(ce, staged_tuning(ctx), ctx->init_seg.as<float>(), ctx->fixtab.as<float2>(),
                                           ctx->lintab.as<float2>(), ctx->meta, x0, dpos.as<float>(), dw.as<double>(),
                                           dout.as<ChainOut>(), ctx->stream, ctx->lf),
                        "export replay");
@@ -1593,7 +1628,7 @@ twisty_status twisty_adjoint(twisty_ctx *ctx, const twisty_bc *bc, const twisty_
             ck(dout.ensure(sizeof(double) * 6), "alloc");
             ck(cudaMemcpyAsync(dtab.p, f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice, ctx->stream), "upload");
             const double ref = fwd->log10_weight - fwd->log10_normalizer - (double)(N - 1) * std::log10(c.absorption_factor);
-            CompTuning t = ctx->tuning;
+            CompTuning t = staged_tuning(ctx);
             t.exact_blend = 1;
             ck(launch_comp_adjoint(c, t, ctx->init_seg.as<float>(), ctx->lintab.as<float2>(), ctx->meta,
                                    ctx->lut32.as<float>(), dtab.as<float>(), dtab.as<float>() + bins, (float)ref,
