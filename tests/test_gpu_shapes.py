@@ -2,8 +2,9 @@
 Needs a B200.
 
 The default shape depends on N (4, 8, 16 or 32 lanes per chain x 2..32 segments per lane), so
-a sweep of N, powers of two and the N just past them (only the group's last slots padded, or
-most of them), covers every shape and both the full and the padded curvature loops. Small
+a sweep of N, powers of two, 2^k + 2 (the reference's own configurations) and the N just
+past them (only the group's last slots padded, or most of them), covers every shape and both
+the full and the padded curvature loops. Small
 rotation angles keep the FP32 and FP64 trajectories together, so the two estimates of
 log10(experimentWeight) agree to ~1e-7 of its magnitude (the per-segment rounding of the
 FP32 trajectory adds up along the path: at N = 384, |log10 w| = 430, that is 5e-5) on the
@@ -15,8 +16,8 @@ import twisty_b200 as T
 
 pytestmark = pytest.mark.gpu
 
-NS = [4, 5, 6, 7, 8, 12, 16, 17, 31, 32, 33, 48, 64, 65, 96, 100, 128, 129, 192, 200, 256, 257, 384, 400, 512,
-      513, 768, 800, 1000, 1024]
+NS = [4, 5, 6, 7, 8, 9, 10, 12, 16, 17, 18, 20, 31, 32, 33, 34, 36, 48, 64, 65, 66, 72, 96, 100, 128, 129, 130,
+      136, 192, 200, 256, 257, 258, 272, 384, 400, 512, 513, 514, 544, 768, 800, 1000, 1024]
 
 
 def _params(N, form, **kw):

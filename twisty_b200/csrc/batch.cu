@@ -34,7 +34,7 @@ bool batch_shape_supported(const BatchShape &s, uint32_t n_max, uint32_t k_eff)
 size_t batch_smem_bytes(const BatchShape &s, uint32_t bins)
 {
     return (s.lut_smem ? (size_t)((bins + 1) / 2) * sizeof(float4) : 0) +
-           (size_t)s.warps * warp_state_bytes(s.group, s.spl);
+           (size_t)s.warps * warp_state_bytes(s.group, s.spl) + cta_len_bytes(s.group, s.spl);
 }
 
 int batch_chains_per_block(const BatchShape &s) { return s.warps * (32 / s.group); }

@@ -27,10 +27,10 @@ struct BatchExp {
 // the occupancy (sets occ).
 bool batch_shapes_a_launch(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items,
                            uint32_t *counter, ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st,
-                           cudaError_t &e);   // 4 x {4, 8}, 8 x {2, 4, 8, 12, 16}, 16 x {4, 8, 12, 16}
+                           cudaError_t &e);   // 4 x {2..9}, 8 x {2..17}, 16 x {4, 8, 12, 16, 17}
 bool batch_shapes_b_launch(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items,
                            uint32_t *counter, ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st,
-                           cudaError_t &e);   // 32 x {4, 8, 12, 16, 24, 32}
+                           cudaError_t &e);   // 32 x {4, 8, 12, 16, 17, 24, 32}
 bool batch_shapes_a_occ(const BatchShape &s, size_t smem, int &occ);
 bool batch_shapes_b_occ(const BatchShape &s, size_t smem, int &occ);
 
@@ -51,8 +51,8 @@ __global__ void __launch_bounds__(MAXT, 1) batch_kernel(const BatchExp *__restri
     constexpr int CPW = 32 / G;
     using Lay = Layout<G, SPL>;
     unsigned char *wb = s_state + (size_t)warp * Lay::WARP_BYTES;
-    const Planes st{reinterpret_cast<float2 *>(wb), reinterpret_cast<float *>(wb + Lay::XY_BYTES),
-                    reinterpret_cast<float *>(wb + Lay::XY_BYTES + Lay::Z_BYTES)};
+    float *s_len = reinterpret_cast<float *>(s_state + (size_t)(blockDim.x >> 5) * Lay::WARP_BYTES);
+    const Planes st{reinterpret_cast<float2 *>(wb), reinterpret_cast<float *>(wb + Lay::XY_BYTES), s_len};
     for (;;) {
         if (threadIdx.x == 0) s_item = atomicAdd(counter, 1u);
         __syncthreads();
@@ -70,7 +70,8 @@ __global__ void __launch_bounds__(MAXT, 1) batch_kernel(const BatchExp *__restri
         ma.log10_abs = e.log10_abs;
         ma.lin = e.lin;
         const uint32_t chain = it.y + warp * CPW + q;
-        chain_body<G, SPL, EXACT, CLAMP, false, kModeForward, false, STEEP>(e.spec, e.kc, e.init_seg, tab, st, q * G, j,
+        chain_body<G, SPL, EXACT, CLAMP, false, kModeForward, false, STEEP, !LUT_SMEM>(e.spec, e.kc, e.init_seg, tab, st,
+                                                                                       q * G, j,
                                                                             chain, chain < e.spec.n_chains,
                                                                             out + e.out_offset, ma);
         __syncthreads();

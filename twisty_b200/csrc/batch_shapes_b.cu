@@ -1,4 +1,4 @@
-// batch_shapes_b.cu -- batched kernel variants for the shapes 32 x 4, 32 x 8, 32 x 12, 32 x 16, 32 x 24, 32 x 32
+// batch_shapes_b.cu -- batched kernel variants for the shapes 32 x 4, 32 x 8, 32 x 12, 32 x 16, 32 x 17, 32 x 24, 32 x 32
 // (lanes per chain x segments per lane).
 #include "batch_launch.cuh"
 
@@ -11,6 +11,7 @@ bool batch_shapes_b_launch(const BatchShape &s, const BatchExp *exps, const uint
     TWISTY_BATCH_SHAPE_LAUNCH(32, 4)
     TWISTY_BATCH_SHAPE_LAUNCH(32, 8)
     TWISTY_BATCH_SHAPE_LAUNCH(32, 12)
+    TWISTY_BATCH_SHAPE_LAUNCH(32, 17)
     TWISTY_BATCH_SHAPE_LAUNCH(32, 16)
     TWISTY_BATCH_SHAPE_LAUNCH(32, 24)
     TWISTY_BATCH_SHAPE_LAUNCH(32, 32)
@@ -22,6 +23,7 @@ bool batch_shapes_b_occ(const BatchShape &s, size_t smem, int &occ)
     TWISTY_BATCH_SHAPE_OCC(32, 4)
     TWISTY_BATCH_SHAPE_OCC(32, 8)
     TWISTY_BATCH_SHAPE_OCC(32, 12)
+    TWISTY_BATCH_SHAPE_OCC(32, 17)
     TWISTY_BATCH_SHAPE_OCC(32, 16)
     TWISTY_BATCH_SHAPE_OCC(32, 24)
     TWISTY_BATCH_SHAPE_OCC(32, 32)

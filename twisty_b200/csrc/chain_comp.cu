@@ -36,10 +36,10 @@ __global__ void __launch_bounds__(256) weigh_comp_kernel(const float *__restrict
         if (brow) brow[i] = b;
     };
     uint32_t clamped = 0;
-    double w = path_log10<32, SPL, EXACT, true>(j, N, tab, kc, tan, ShflNext<32>{}, sink, clamped);
+    double w = path_log10<32, SPL, EXACT, true, true>(j, N, tab, kc, tan, ShflNext<32>{}, sink, clamped);
     if (!EXACT && isnan(w)) {
         // a steep bin (NaN slope) or a NaN curvature: the exact blend through the linear table
-        w = path_log10<32, SPL, true, true>(j, N, lin, kc, tan, ShflNext<32>{}, sink, clamped);
+        w = path_log10<32, SPL, true, true, true>(j, N, lin, kc, tan, ShflNext<32>{}, sink, clamped);
     }
     if (j == 0) {
         const bool ok = !isnan(w);
@@ -106,20 +106,30 @@ bool comp_table_needs_clamp(float inv_ds, const LutMetaF &m)
 // with less padding (measured: N = 192, 384, 768 18-27 % faster than the next power of two).
 // Up to N = 32, 4-lane groups put 8 chains in a warp, which share the per-step work of the
 // proposal broadcast, the group reductions and the log-sum-exp (N = 16: +23 %, 32: +12 %
-// over 8 lanes).
+// over 8 lanes). The shapes with one segment per lane more than a power of two (3, 5, 9, 17)
+// serve N = 2^k + 2, the N of the reference's own configurations (10, 18, 34, 66, 130, 258,
+// 514), which would otherwise pad to the next power of two.
 CompTuning comp_default_tuning(uint32_t n)
 {
     CompTuning t;
     t.exact_blend = 0;
-    if (n <= 16) { t.group = 4; t.spl = 4; t.warps_per_block = 32; }
+    if (n <= 8) { t.group = 4; t.spl = 2; t.warps_per_block = 32; }
+    else if (n <= 12) { t.group = 4; t.spl = 3; t.warps_per_block = 32; }
+    else if (n <= 16) { t.group = 4; t.spl = 4; t.warps_per_block = 32; }
+    else if (n <= 20) { t.group = 4; t.spl = 5; t.warps_per_block = 32; }
     else if (n <= 32) { t.group = 4; t.spl = 8; t.warps_per_block = 32; }
+    else if (n <= 36) { t.group = 4; t.spl = 9; t.warps_per_block = 32; }
     else if (n <= 64) { t.group = 8; t.spl = 8; t.warps_per_block = 32; }
+    else if (n <= 72) { t.group = 8; t.spl = 9; t.warps_per_block = 32; }
     else if (n <= 96) { t.group = 8; t.spl = 12; t.warps_per_block = 16; }
     else if (n <= 128) { t.group = 8; t.spl = 16; t.warps_per_block = 16; }
+    else if (n <= 136) { t.group = 8; t.spl = 17; t.warps_per_block = 16; }
     else if (n <= 192) { t.group = 16; t.spl = 12; t.warps_per_block = 16; }
     else if (n <= 256) { t.group = 16; t.spl = 16; t.warps_per_block = 16; }
+    else if (n <= 272) { t.group = 16; t.spl = 17; t.warps_per_block = 16; }
     else if (n <= 384) { t.group = 32; t.spl = 12; t.warps_per_block = 16; }
     else if (n <= 512) { t.group = 32; t.spl = 16; t.warps_per_block = 16; }
+    else if (n <= 544) { t.group = 32; t.spl = 17; t.warps_per_block = 16; }
     else if (n <= 768) { t.group = 32; t.spl = 24; t.warps_per_block = 12; }
     else { t.group = 32; t.spl = 32; t.warps_per_block = 8; }
     return t;
@@ -127,12 +137,11 @@ CompTuning comp_default_tuning(uint32_t n)
 
 bool comp_tuning_supported(const CompTuning &t, uint32_t n, uint32_t k_eff)
 {
-    const bool shape = (t.group == 4 && (t.spl == 4 || t.spl == 8)) ||
-                       (t.group == 8 && (t.spl == 2 || t.spl == 4 || t.spl == 8 || t.spl == 12 || t.spl == 16 ||
-                                         t.spl == 32)) ||
-                       (t.group == 16 && (t.spl == 4 || t.spl == 8 || t.spl == 12 || t.spl == 16)) ||
-                       (t.group == 32 && (t.spl == 4 || t.spl == 8 || t.spl == 12 || t.spl == 16 || t.spl == 24 ||
-                                          t.spl == 32));
+    const int s = t.spl;
+    const bool shape = (t.group == 4 && (s == 2 || s == 3 || s == 4 || s == 5 || s == 8 || s == 9)) ||
+                       (t.group == 8 && (s == 2 || s == 4 || s == 8 || s == 9 || s == 12 || s == 16 || s == 17 || s == 32)) ||
+                       (t.group == 16 && (s == 4 || s == 8 || s == 12 || s == 16 || s == 17)) ||
+                       (t.group == 32 && (s == 4 || s == 8 || s == 12 || s == 16 || s == 17 || s == 24 || s == 32));
     return shape && (uint32_t)(t.group * t.spl) >= n && n >= 4 && k_eff <= (uint32_t)kMaxSubChain &&
            t.warps_per_block >= 1 && t.warps_per_block * 32 <= ((t.spl >= 12) ? 512 : 1024);
 }
@@ -146,7 +155,7 @@ uint32_t comp_default_chains(uint32_t n, int sm_count)
 size_t comp_smem_bytes(const CompTuning &t, uint32_t bins)
 {
     const size_t tab = t.lut_global ? 0 : (size_t)((bins + 1) / 2) * sizeof(float4);
-    const size_t state = (size_t)t.warps_per_block * warp_state_bytes(t.group, t.spl);
+    const size_t state = (size_t)t.warps_per_block * warp_state_bytes(t.group, t.spl) + cta_len_bytes(t.group, t.spl);
     const size_t res = (size_t)t.warps_per_block * (32 / t.group) * sizeof(double);
     return tab + state + res;
 }

@@ -54,6 +54,7 @@
 #include "kernels.h"
 #include "device_common.cuh"
 
+#include <algorithm>
 #include <cfloat>
 
 namespace twisty {
@@ -220,10 +221,25 @@ struct ShflNext {
     }
 };
 
+// Table entry L. GLOBAL: the table is in global memory, read through L1 by an unconditional
+// non-coherent load, so that the compiler cannot turn the padded slots' loads into predicated
+// ones (measured: with plain loads the padded curvature loop ran 15 % slower through L1).
+template <bool GLOBAL>
+__device__ __forceinline__ float2 tab_load(const float2 *__restrict__ tab, int32_t L)
+{
+    if constexpr (GLOBAL) {
+        float2 e;
+        asm("ld.global.nc.v2.f32 {%0, %1}, [%2];" : "=f"(e.x), "=f"(e.y) : "l"(tab + L));
+        return e;
+    } else {
+        return tab[L];
+    }
+}
+
 // Generic full recompute of one path's log10 weight (absorption excluded), for the exact
 // table or, with 64-bit lane sums, for the fixed-point table at any lane width. bin_sink(i,
 // bin) receives every curvature's bin (-1 for NaN).
-template <int G, int SPL, bool EXACT, bool CLAMP, class TanFn, class NextFn, class BinFn>
+template <int G, int SPL, bool EXACT, bool CLAMP, bool GLOBAL = false, class TanFn, class NextFn, class BinFn>
 __device__ __forceinline__ double path_log10(uint32_t j, uint32_t N, const float2 *__restrict__ tab,
                                              const CompConsts &k, TanFn tan, NextFn next, BinFn bin_sink,
                                              uint32_t &clamped)
@@ -234,7 +250,7 @@ __device__ __forceinline__ double path_log10(uint32_t j, uint32_t N, const float
         int32_t L;
         const float frac = bin_of<CLAMP>(qq, k, valid, clamped, L);
         if (valid) bin_sink(i, isnan(frac) ? -1 : L);
-        const float2 e = tab[L];
+        const float2 e = tab_load<GLOBAL>(tab, L);
         if (EXACT) {
             const float term = __log2f(fmaf(frac * k.step, e.y, e.x)) * kLog10_2;
             kahan_add(ks, kc, valid ? term : 0.0f);
@@ -259,7 +275,7 @@ __device__ __forceinline__ double path_log10(uint32_t j, uint32_t N, const float
 // value lies in [0, 2^32) by the table's scale); the group total is added in 32 bits for a
 // narrow table, in 64 bits for a wide one (both exact). *bad is set when any curvature of
 // the path is NaN.
-template <int G, int SPL, bool CLAMP, class TanFn, class NextFn>
+template <int G, int SPL, bool CLAMP, bool GLOBAL, class TanFn, class NextFn>
 __device__ __forceinline__ unsigned long long path_fixed(uint32_t j, uint32_t gbase, uint32_t N, const float2 *__restrict__ tab,
                                                const CompConsts &k, TanFn tan, NextFn next, bool &bad,
                                                uint32_t &clamped)
@@ -269,7 +285,7 @@ __device__ __forceinline__ unsigned long long path_fixed(uint32_t j, uint32_t gb
     auto seg = [&](uint32_t, float qq, bool valid) {
         int32_t L;
         const float frac = bin_of<CLAMP>(qq, k, valid, clamped, L);
-        const float2 e = tab[L];
+        const float2 e = tab_load<GLOBAL>(tab, L);
         isum += valid ? __float_as_uint(e.x) : 0u;
         // a padding slot leaves the sum alone even where the slope is NaN (a steep bin)
         const float c2 = fmaf(frac, e.y, csum);
@@ -293,22 +309,29 @@ struct Layout {
     static constexpr int PZ = 32 + ((G / SPL) > 1 ? (G / SPL) : 1);     // float plane pitch
     static constexpr int XY_BYTES = SPL * PXY * 8;
     static constexpr int Z_BYTES = SPL * PZ * 4;
-    static constexpr int WARP_BYTES = XY_BYTES + 2 * Z_BYTES;           // xy, z, l planes
+    // xy, z planes; rounded to 16 bytes so that every warp's float2 plane (and what follows the
+    // last warp) stays aligned when SPL * PZ is odd
+    static constexpr int WARP_BYTES = (XY_BYTES + Z_BYTES + 15) / 16 * 16;
     __device__ __forceinline__ static uint32_t xy(uint32_t col, uint32_t m) { return m * (uint32_t)PXY + col; }
     __device__ __forceinline__ static uint32_t z(uint32_t col, uint32_t m) { return m * (uint32_t)PZ + col; }
 };
 
 constexpr size_t warp_state_bytes(int G, int SPL)
 {
-    return (size_t)SPL * (32 + ((16 / SPL) > 1 ? (16 / SPL) : 1)) * 8 +
-           2 * (size_t)SPL * (32 + ((G / SPL) > 1 ? (G / SPL) : 1)) * 4;
+    return ((size_t)SPL * (32 + ((16 / SPL) > 1 ? (16 / SPL) : 1)) * 8 +
+            (size_t)SPL * (32 + ((G / SPL) > 1 ? (G / SPL) : 1)) * 4 + 15) / 16 * 16;
 }
 
-// The planes of one warp's chains.
+// The segment lengths, one array per CTA: rotations never change a length, and every chain of
+// a CTA starts from the same initial curve, so all its chains share them (G * SPL floats,
+// padding segments 1).
+__host__ __device__ constexpr size_t cta_len_bytes(int G, int SPL) { return ((size_t)G * SPL * 4 + 15) / 16 * 16; }
+
+// The planes of one warp's chains (tangents) and the CTA's segment lengths.
 struct Planes {
     float2 *xy;
     float *z;
-    float *l;
+    float *l;    // CTA-wide, by segment index
 };
 
 enum { kModeForward = 0, kModeExport = 1, kModeAdjoint = 2 };
@@ -371,7 +394,7 @@ __device__ __noinline__ double steep_fallback(Planes st, uint32_t gbase, uint32_
         z = st.z[Lay::z(own, m)];
     };
     uint32_t unused = 0;
-    return path_log10<G, SPL, true, CLAMP>(j, N, lin, kc, tan, ShflNext<G>{}, [](uint32_t, int32_t) {}, unused);
+    return path_log10<G, SPL, true, CLAMP, true>(j, N, lin, kc, tan, ShflNext<G>{}, [](uint32_t, int32_t) {}, unused);
 }
 
 // One Markov chain run by the G lanes of one group on its own records st (tangent, length;
@@ -380,7 +403,8 @@ __device__ __noinline__ double steep_fallback(Planes st, uint32_t gbase, uint32_
 // Writes out[chain] (when out is set and the chain is real) and returns the chain's log10 sum.
 // STEEP: the fixed-point table has steep bins (NaN slopes); paths crossing one are re-weighed
 // through ma.lin. Without it a NaN slope cannot occur and a NaN total means a NaN curvature.
-template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MODE, bool INCR = false, bool STEEP = false>
+template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MODE, bool INCR = false, bool STEEP = false,
+          bool TAB_GLOBAL = false>
 __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConsts &kc,
                                              const float *__restrict__ init_seg, const float2 *s_tab, Planes st,
                                              uint32_t gbase, uint32_t j, uint32_t chain, bool real_chain,
@@ -392,7 +416,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
     // segment record (tangent, length) of segment index s = owner*SPL + m
     auto load_rec = [&](uint32_t owner, uint32_t m) {
         const float2 a = st.xy[Lay::xy(gbase + owner, m)];
-        return make_float4(a.x, a.y, st.z[Lay::z(gbase + owner, m)], st.l[Lay::z(gbase + owner, m)]);
+        return make_float4(a.x, a.y, st.z[Lay::z(gbase + owner, m)], st.l[owner * SPL + m]);
     };
 
     float max_len = 0.f;
@@ -414,7 +438,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
         }
         st.xy[Lay::xy(gbase + j, m)] = make_float2(x, y);
         st.z[Lay::z(gbase + j, m)] = z;
-        st.l[Lay::z(gbase + j, m)] = len;
+        st.l[s] = len;   // every chain of the CTA writes the same value
     }
 #pragma unroll
     for (int o = 1; o < G; o <<= 1) max_len = fmaxf(max_len, __shfl_xor_sync(FULL, max_len, o));
@@ -464,7 +488,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
         y = a.y;
         z = st.z[Lay::z(own, m)];
         if (SHIFT && j * SPL + m == N - 2) {
-            const float l = st.l[Lay::z(own, m)];
+            const float l = st.l[j * SPL + m];
             x = fmaf(l, x, c.eval_shift[0]);
             y = fmaf(l, y, c.eval_shift[1]);
             z = fmaf(l, z, c.eval_shift[2]);
@@ -529,7 +553,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                     vx[ri] = a.x;
                     vy[ri] = a.y;
                     vz[ri] = st.z[vb[ri]];
-                    const float l = st.l[vb[ri]];
+                    const float l = st.l[s];
                     cx = fmaf(l, vx[ri], cx);
                     cy = fmaf(l, vy[ri], cy);
                     cz = fmaf(l, vz[ri], cz);
@@ -610,7 +634,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                     tot = inc_tot;
                     ++inc_since_full;
                 } else {
-                    tot = path_fixed<G, SPL, CLAMP>(j, gbase, N, s_tab, kc, tan_smem, next_smem, bad, clamped);
+                    tot = path_fixed<G, SPL, CLAMP, TAB_GLOBAL>(j, gbase, N, s_tab, kc, tan_smem, next_smem, bad, clamped);
                     // a NaN slope marks a steep bin, where the secant would err by more than
                     // 1e-7: weigh such paths (rare) with the exact blend through the linear
                     // table; only a NaN curvature leaves a path invalid
@@ -741,7 +765,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                     if (j == 0) acc[5] += wt;
                 }
             } else {
-                w = path_log10<G, SPL, true, CLAMP>(j, N, s_tab, kc, tan_smem, next_smem, no_bins, clamped);
+                w = path_log10<G, SPL, true, CLAMP, TAB_GLOBAL>(j, N, s_tab, kc, tan_smem, next_smem, no_bins, clamped);
             }
             if (MODE == kModeExport) {
                 double px = 0.0, py = 0.0, pz = 0.0;

@@ -24,10 +24,10 @@ struct CompLaunch {
 };
 
 // Each returns false when the launch's shape is not among its own, else launches and sets e.
-bool launch_comp_shapes_a(const CompLaunch &a, cudaError_t &e);   // 4 x {4, 8}, 8 x {2, 4}
-bool launch_comp_shapes_b(const CompLaunch &a, cudaError_t &e);   // 8 x {8, 12, 16, 32}
-bool launch_comp_shapes_c(const CompLaunch &a, cudaError_t &e);   // 16 x {4, 8, 12, 16}
-bool launch_comp_shapes_d(const CompLaunch &a, cudaError_t &e);   // 32 x {4, 8, 12}
+bool launch_comp_shapes_a(const CompLaunch &a, cudaError_t &e);   // 4 x {2, 3, 4, 5, 8, 9}, 8 x {2, 4}
+bool launch_comp_shapes_b(const CompLaunch &a, cudaError_t &e);   // 8 x {8, 9, 12, 16, 17, 32}
+bool launch_comp_shapes_c(const CompLaunch &a, cudaError_t &e);   // 16 x {4, 8, 12, 16, 17}
+bool launch_comp_shapes_d(const CompLaunch &a, cudaError_t &e);   // 32 x {4, 8, 12, 17}
 bool launch_comp_shapes_e(const CompLaunch &a, cudaError_t &e);   // 32 x {16, 24, 32}
 
 namespace {
@@ -48,7 +48,8 @@ __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompCo
     unsigned char *s_state = reinterpret_cast<unsigned char *>(smem4 + tab_f4);
     const int warps = blockDim.x >> 5;
     using Lay = Layout<G, SPL>;
-    double *s_res = reinterpret_cast<double *>(s_state + (size_t)warps * Lay::WARP_BYTES);
+    float *s_len = reinterpret_cast<float *>(s_state + (size_t)warps * Lay::WARP_BYTES);
+    double *s_res = reinterpret_cast<double *>(s_state + (size_t)warps * Lay::WARP_BYTES + cta_len_bytes(G, SPL));
     if (!LUTG) stage_table(smem4, tab_g, bins);
     __syncthreads();
 
@@ -57,10 +58,10 @@ __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompCo
     constexpr int CPW = 32 / G;
     const uint32_t chain = (blockIdx.x * warps + warp) * CPW + q;
     unsigned char *wb = s_state + (size_t)warp * Lay::WARP_BYTES;
-    const Planes pl{reinterpret_cast<float2 *>(wb), reinterpret_cast<float *>(wb + Lay::XY_BYTES),
-                    reinterpret_cast<float *>(wb + Lay::XY_BYTES + Lay::Z_BYTES)};
-    const double cl = chain_body<G, SPL, EXACT, CLAMP, SHIFT, MODE, INCR, STEEP>(c, kc, init_seg, s_tab, pl, q * G, j,
-                                                                                 chain, chain < c.n_chains, out, ma);
+    const Planes pl{reinterpret_cast<float2 *>(wb), reinterpret_cast<float *>(wb + Lay::XY_BYTES), s_len};
+    const double cl = chain_body<G, SPL, EXACT, CLAMP, SHIFT, MODE, INCR, STEEP, LUTG>(c, kc, init_seg, s_tab, pl, q * G,
+                                                                                       j, chain, chain < c.n_chains, out,
+                                                                                       ma);
     if (j == 0) s_res[warp * CPW + q] = cl;
     __syncthreads();
     // Per-CTA log-sum-exp of the chains, rescaled by the block maximum (FP64).
@@ -88,6 +89,14 @@ cudaError_t launch_t(const ChainSpec &c, const CompConsts &kc, int warps, const 
     auto kern = comp_chain_kernel<G, SPL, EXACT, CLAMP, SHIFT, MAXT, MODE, INCR, STEEP, LUTG>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    if (LUTG) {
+        // the table is gathered through L1: ask for no more shared memory than the one CTA per SM
+        // needs (plus the 1 KB the system reserves per CTA), leaving the rest of the SM's 256 KB
+        // of L1/shared storage to L1
+        const int pct = (int)std::min<size_t>(100, ((smem + 1024) * 100 + 228 * 1024 - 1) / (228 * 1024));
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+        if (e != cudaSuccess) return e;
+    }
     kern<<<blocks, warps * 32, smem, st>>>(c, kc, init_seg, tab, out, partials, ma);
     return cudaGetLastError();
 }
