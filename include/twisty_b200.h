@@ -119,7 +119,7 @@ typedef struct twisty_params {
                                     only; 2 the arc (any N >= 4) */
     twisty_vec3 eval_end_shift;  /* weights evaluated with the receiver moved by this vector,
                                     the chain itself unchanged (finite-difference checks) */
-    /* compensated-form kernel shape; 0 = chosen from N. comp_group lanes per chain (4, 8, 16,
+    /* compensated-form kernel shape; 0 = chosen from N. comp_group lanes per chain (1, 4, 8, 16,
        32) x comp_spl segments per lane (>= N in total), comp_warps warps per CTA. */
     uint32_t comp_group;
     uint32_t comp_spl;

@@ -27,7 +27,7 @@ struct BatchExp {
 // the occupancy (sets occ).
 bool batch_shapes_a_launch(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items,
                            uint32_t *counter, ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st,
-                           cudaError_t &e);   // 4 x {2..9}, 8 x {2..17}, 16 x {4, 8, 12, 16, 17}
+                           cudaError_t &e);   // 1 x {8, 12}, 4 x {2..9}, 8 x {2..17}, 16 x {4, 8, 12, 16, 17}
 bool batch_shapes_b_launch(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items,
                            uint32_t *counter, ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st,
                            cudaError_t &e);   // 32 x {4, 8, 12, 16, 17, 24, 32}

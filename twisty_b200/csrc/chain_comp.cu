@@ -106,15 +106,17 @@ bool comp_table_needs_clamp(float inv_ds, const LutMetaF &m)
 // with less padding (measured: N = 192, 384, 768 18-27 % faster than the next power of two).
 // Up to N = 32, 4-lane groups put 8 chains in a warp, which share the per-step work of the
 // proposal broadcast, the group reductions and the log-sum-exp (N = 16: +23 %, 32: +12 %
-// over 8 lanes). The shapes with one segment per lane more than a power of two (3, 5, 9, 17)
+// over 8 lanes); up to N = 12 one lane carries a whole chain, 32 chains per warp, with no group
+// reductions at all (N = 5: +76 %, 8: +54 %, 10: +9 % over 4 lanes). The shapes with one
+// segment per lane more than a power of two (3, 5, 9, 17)
 // serve N = 2^k + 2, the N of the reference's own configurations (10, 18, 34, 66, 130, 258,
 // 514), which would otherwise pad to the next power of two.
 CompTuning comp_default_tuning(uint32_t n)
 {
     CompTuning t;
     t.exact_blend = 0;
-    if (n <= 8) { t.group = 4; t.spl = 2; t.warps_per_block = 32; }
-    else if (n <= 12) { t.group = 4; t.spl = 3; t.warps_per_block = 32; }
+    if (n <= 8) { t.group = 1; t.spl = 8; t.warps_per_block = 32; }
+    else if (n <= 12) { t.group = 1; t.spl = 12; t.warps_per_block = 16; }
     else if (n <= 16) { t.group = 4; t.spl = 4; t.warps_per_block = 32; }
     else if (n <= 20) { t.group = 4; t.spl = 5; t.warps_per_block = 32; }
     else if (n <= 32) { t.group = 4; t.spl = 8; t.warps_per_block = 32; }
@@ -138,7 +140,8 @@ CompTuning comp_default_tuning(uint32_t n)
 bool comp_tuning_supported(const CompTuning &t, uint32_t n, uint32_t k_eff)
 {
     const int s = t.spl;
-    const bool shape = (t.group == 4 && (s == 2 || s == 3 || s == 4 || s == 5 || s == 8 || s == 9)) ||
+    const bool shape = (t.group == 1 && (s == 8 || s == 12)) ||
+                       (t.group == 4 && (s == 2 || s == 3 || s == 4 || s == 5 || s == 8 || s == 9)) ||
                        (t.group == 8 && (s == 2 || s == 4 || s == 8 || s == 9 || s == 12 || s == 16 || s == 17 || s == 32)) ||
                        (t.group == 16 && (s == 4 || s == 8 || s == 12 || s == 16 || s == 17)) ||
                        (t.group == 32 && (s == 4 || s == 8 || s == 12 || s == 16 || s == 17 || s == 24 || s == 32));

@@ -215,9 +215,13 @@ template <int G>
 struct ShflNext {
     __device__ __forceinline__ void operator()(float t0x, float t0y, float t0z, float &nx, float &ny, float &nz) const
     {
-        nx = __shfl_down_sync(FULL, t0x, 1, G);
-        ny = __shfl_down_sync(FULL, t0y, 1, G);
-        nz = __shfl_down_sync(FULL, t0z, 1, G);
+        if constexpr (G == 1) {   // a one-lane chain has no next lane: its last slot is padding
+            nx = t0x; ny = t0y; nz = t0z;
+        } else {
+            nx = __shfl_down_sync(FULL, t0x, 1, G);
+            ny = __shfl_down_sync(FULL, t0y, 1, G);
+            nz = __shfl_down_sync(FULL, t0z, 1, G);
+        }
     }
 };
 
@@ -532,7 +536,8 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                 }
             }
             // chord x_right - x_left = sum of l_s t_s over the k segments left .. right-1
-            constexpr int R = (kMaxSubChain + G - 1) / G;
+            // (k <= N - 2 < G * SPL, so a sub-chain never needs more than SPL rounds)
+            constexpr int R = (kMaxSubChain + G - 1) / G < SPL ? (kMaxSubChain + G - 1) / G : SPL;
             // more than 4 rounds (8-lane groups) under the 64-register budget of 1024-thread
             // CTAs (SPL < 16): the rotation pass reloads its tangents instead of keeping every
             // round's in registers (measured: no spills, N <= 64 up to 27 % faster)
