@@ -65,6 +65,7 @@ __global__ void __launch_bounds__(MAXT, 1) batch_kernel(const BatchExp *__restri
             stage_table(smem4, e.tab, bins);
             tab = reinterpret_cast<const float2 *>(smem4);
         }
+        fill_lengths(s_len, e.init_seg, e.spec.n_segments, G * SPL);
         __syncthreads();
         ModeArgs ma{};
         ma.log10_abs = e.log10_abs;

@@ -375,6 +375,21 @@ __device__ __forceinline__ void receiver_grad(const float t3[3], const float t2[
     }
 }
 
+// The CTA's segment lengths from the initial segment vectors (padding segments 1), computed as
+// the chain body computes them (|v| = |v|^2 rsqrt(|v|^2)); the CTA synchronises before use.
+__device__ __forceinline__ void fill_lengths(float *s_len, const float *__restrict__ init_seg, uint32_t n, uint32_t slots)
+{
+    for (uint32_t s = threadIdx.x; s < slots; s += blockDim.x) {
+        float len = 1.f;
+        if (s < n) {
+            const float x = init_seg[3 * s], y = init_seg[3 * s + 1], z = init_seg[3 * s + 2];
+            const float ss = fmaf(x, x, fmaf(y, y, z * z));
+            len = ss * rsqrtf(ss);
+        }
+        s_len[s] = len;
+    }
+}
+
 // Stage a table of `bins` float2 entries into shared memory (float4 vector loads).
 __device__ __forceinline__ void stage_table(float4 *smem4, const float2 *__restrict__ tab_g, int bins)
 {
@@ -442,7 +457,6 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
         }
         st.xy[Lay::xy(gbase + j, m)] = make_float2(x, y);
         st.z[Lay::z(gbase + j, m)] = z;
-        st.l[s] = len;   // every chain of the CTA writes the same value
     }
 #pragma unroll
     for (int o = 1; o < G; o <<= 1) max_len = fmaxf(max_len, __shfl_xor_sync(FULL, max_len, o));

@@ -51,6 +51,7 @@ __global__ void __launch_bounds__(MAXT, 1) comp_chain_kernel(ChainSpec c, CompCo
     float *s_len = reinterpret_cast<float *>(s_state + (size_t)warps * Lay::WARP_BYTES);
     double *s_res = reinterpret_cast<double *>(s_state + (size_t)warps * Lay::WARP_BYTES + cta_len_bytes(G, SPL));
     if (!LUTG) stage_table(smem4, tab_g, bins);
+    fill_lengths(s_len, init_seg, c.n_segments, G * SPL);
     __syncthreads();
 
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
