@@ -954,19 +954,26 @@ twisty_status twisty_run_msegment(twisty_ctx *ctx, const twisty_bc *bc, twisty_r
         const uint64_t per_path = 3 * sizeof(float) * (uint64_t)(N + 1);
         const uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(total, (1ull << 30) / per_path));
         cudaStream_t st = ctx->stream;
-        DevBuf dpos, dw, dv, dch, dred;
+        DevBuf dpos, dw, dv, dch, dred, drg;
         struct Release {
-            DevBuf *b[5];
+            DevBuf *b[6];
             ~Release()
             {
                 for (DevBuf *x : b) x->release();
             }
-        } rel{{&dpos, &dw, &dv, &dch, &dred}};
+        } rel{{&dpos, &dw, &dv, &dch, &dred, &drg}};
+        // the samples of a chunk reduce in slices of kSlice, one CTA each, combined on the host
+        constexpr uint64_t kSlice = 16384;
+        const uint64_t max_slices = (chunk + kSlice - 1) / kSlice;
         ck(dpos.ensure(per_path * chunk), "alloc paths");
         ck(dw.ensure(sizeof(double) * chunk), "alloc weights");
         ck(dv.ensure(chunk), "alloc validity");
         ck(dch.ensure(sizeof(ChainOut) * chunk), "alloc samples");
-        ck(dred.ensure(sizeof(ReduceOut)), "alloc result");
+        ck(dred.ensure(sizeof(ReduceOut) * max_slices), "alloc result");
+        ck(drg.ensure(sizeof(uint2) * max_slices), "alloc slices");
+        std::vector<uint2> slices(max_slices);
+        for (uint64_t k = 0; k < max_slices; ++k) slices[k] = make_uint2((uint32_t)(k * kSlice), (uint32_t)kSlice);
+        std::vector<ReduceOut> parts(max_slices);
         const double af = (double)std::exp(-p.absorption * ds);
         const float inv_ds = (float)N / bc->arclength;
         const uint64_t seed = seed_of(p.perturb_seed);
@@ -989,28 +996,35 @@ twisty_status twisty_run_msegment(twisty_ctx *ctx, const twisty_bc *bc, twisty_r
                                      nullptr, st, ctx->lf),
                    "weigh kernel");
             ck(launch_pack_paths(dw.as<double>(), dv.as<uint8_t>(), n, dch.as<ChainOut>(), st), "pack");
-            ck(launch_reduce(dch.as<ChainOut>(), (uint32_t)n, dred.as<ReduceOut>(), st), "reduction");
+            const uint64_t ns = (n + kSlice - 1) / kSlice;
+            slices[ns - 1].y = (uint32_t)(n - (ns - 1) * kSlice);
+            ck(cudaMemcpyAsync(drg.p, slices.data(), sizeof(uint2) * ns, cudaMemcpyHostToDevice, st), "upload slices");
+            slices[ns - 1].y = (uint32_t)kSlice;
+            ck(launch_reduce_segments(dch.as<ChainOut>(), drg.as<uint2>(), (uint32_t)ns, dred.as<ReduceOut>(), st),
+               "reduction");
             ck(cudaEventRecord(ctx->ev[1], st), "event");
-            ReduceOut r{};
-            ck(cudaMemcpyAsync(&r, dred.p, sizeof(r), cudaMemcpyDeviceToHost, st), "read result");
+            ck(cudaMemcpyAsync(parts.data(), dred.p, sizeof(ReduceOut) * ns, cudaMemcpyDeviceToHost, st), "read result");
             ck(cudaStreamSynchronize(st), "M-segment chunk");
             float ms = 0.f;
             ck(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]), "event time");
             gpu_ms += ms;
-            valid += r.valid;
-            failed += r.failed;
-            if (r.valid && r.log10_sum > -std::numeric_limits<double>::infinity()) {
-                // running log-sum-exp of the chunk sums, absolute standard errors in quadrature
-                const double se = std::isnan(r.rel_se) ? 0.0 : r.rel_se;
-                if (r.log10_sum > m) {
-                    const double f = std::pow(10.0, m - r.log10_sum);
-                    sum *= f;
-                    var *= f * f;
-                    m = r.log10_sum;
+            for (uint64_t k = 0; k < ns; ++k) {
+                const ReduceOut &r = parts[k];
+                valid += r.valid;
+                failed += r.failed;
+                if (r.valid && r.log10_sum > -std::numeric_limits<double>::infinity()) {
+                    // running log-sum-exp of the chunk sums, absolute standard errors in quadrature
+                    const double se = std::isnan(r.rel_se) ? 0.0 : r.rel_se;
+                    if (r.log10_sum > m) {
+                        const double f = std::pow(10.0, m - r.log10_sum);
+                        sum *= f;
+                        var *= f * f;
+                        m = r.log10_sum;
+                    }
+                    const double x = std::pow(10.0, r.log10_sum - m);
+                    sum += x;
+                    var += (se * x) * (se * x);
                 }
-                const double x = std::pow(10.0, r.log10_sum - m);
-                sum += x;
-                var += (se * x) * (se * x);
             }
         }
         std::memset(res, 0, sizeof(*res));
