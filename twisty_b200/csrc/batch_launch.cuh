@@ -83,7 +83,7 @@ template <int G, int SPL, bool EXACT, bool LS, bool CL, bool SP>
 cudaError_t batch_t(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items, uint32_t *counter,
                     ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st)
 {
-    constexpr int MAXT = (SPL >= 12 || G <= 8) ? 512 : 1024;
+    constexpr int MAXT = batch_max_threads(G, SPL);
     if (s.warps * 32 > MAXT) return cudaErrorInvalidConfiguration;
     auto kern = batch_kernel<G, SPL, EXACT, LS, CL, SP, MAXT>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -95,7 +95,7 @@ cudaError_t batch_t(const BatchShape &s, const BatchExp *exps, const uint2 *item
 template <int G, int SPL, bool EXACT, bool LS, bool CL, bool SP>
 int batch_occ_t(const BatchShape &s, size_t smem)
 {
-    constexpr int MAXT = (SPL >= 12 || G <= 8) ? 512 : 1024;
+    constexpr int MAXT = batch_max_threads(G, SPL);
     auto kern = batch_kernel<G, SPL, EXACT, LS, CL, SP, MAXT>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
     int nb = 0;

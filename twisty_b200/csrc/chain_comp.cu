@@ -116,24 +116,24 @@ CompTuning comp_default_tuning(uint32_t n)
     CompTuning t;
     t.exact_blend = 0;
     if (n <= 8) { t.group = 1; t.spl = 8; t.warps_per_block = 32; }
-    else if (n <= 12) { t.group = 1; t.spl = 12; t.warps_per_block = 16; }
+    else if (n <= 12) { t.group = 1; t.spl = 12; t.warps_per_block = 24; }
     else if (n <= 16) { t.group = 4; t.spl = 4; t.warps_per_block = 32; }
     else if (n <= 20) { t.group = 4; t.spl = 5; t.warps_per_block = 32; }
     else if (n <= 32) { t.group = 4; t.spl = 8; t.warps_per_block = 32; }
     else if (n <= 36) { t.group = 4; t.spl = 9; t.warps_per_block = 32; }
     else if (n <= 64) { t.group = 8; t.spl = 8; t.warps_per_block = 32; }
     else if (n <= 72) { t.group = 8; t.spl = 9; t.warps_per_block = 32; }
-    else if (n <= 96) { t.group = 8; t.spl = 12; t.warps_per_block = 16; }
-    else if (n <= 128) { t.group = 8; t.spl = 16; t.warps_per_block = 16; }
-    else if (n <= 136) { t.group = 8; t.spl = 17; t.warps_per_block = 16; }
-    else if (n <= 192) { t.group = 16; t.spl = 12; t.warps_per_block = 16; }
-    else if (n <= 256) { t.group = 16; t.spl = 16; t.warps_per_block = 16; }
-    else if (n <= 272) { t.group = 16; t.spl = 17; t.warps_per_block = 16; }
-    else if (n <= 384) { t.group = 32; t.spl = 12; t.warps_per_block = 16; }
-    else if (n <= 512) { t.group = 32; t.spl = 16; t.warps_per_block = 16; }
-    else if (n <= 544) { t.group = 32; t.spl = 17; t.warps_per_block = 16; }
-    else if (n <= 768) { t.group = 32; t.spl = 24; t.warps_per_block = 12; }
-    else { t.group = 32; t.spl = 32; t.warps_per_block = 8; }
+    else if (n <= 96) { t.group = 8; t.spl = 12; t.warps_per_block = 24; }
+    else if (n <= 128) { t.group = 8; t.spl = 16; t.warps_per_block = 24; }
+    else if (n <= 136) { t.group = 8; t.spl = 17; t.warps_per_block = 24; }
+    else if (n <= 192) { t.group = 16; t.spl = 12; t.warps_per_block = 24; }
+    else if (n <= 256) { t.group = 16; t.spl = 16; t.warps_per_block = 24; }
+    else if (n <= 272) { t.group = 16; t.spl = 17; t.warps_per_block = 24; }
+    else if (n <= 384) { t.group = 32; t.spl = 12; t.warps_per_block = 24; }
+    else if (n <= 512) { t.group = 32; t.spl = 16; t.warps_per_block = 24; }
+    else if (n <= 544) { t.group = 32; t.spl = 17; t.warps_per_block = 24; }
+    else if (n <= 768) { t.group = 32; t.spl = 24; t.warps_per_block = 16; }
+    else { t.group = 32; t.spl = 32; t.warps_per_block = 12; }
     return t;
 }
 
@@ -146,7 +146,7 @@ bool comp_tuning_supported(const CompTuning &t, uint32_t n, uint32_t k_eff)
                        (t.group == 16 && (s == 4 || s == 8 || s == 12 || s == 16 || s == 17)) ||
                        (t.group == 32 && (s == 4 || s == 8 || s == 12 || s == 16 || s == 17 || s == 24 || s == 32));
     return shape && (uint32_t)(t.group * t.spl) >= n && n >= 4 && k_eff <= (uint32_t)kMaxSubChain &&
-           t.warps_per_block >= 1 && t.warps_per_block * 32 <= ((t.spl >= 12) ? 512 : 1024);
+           t.warps_per_block >= 1 && t.warps_per_block * 32 <= comp_max_threads(t.group, t.spl);
 }
 
 uint32_t comp_default_chains(uint32_t n, int sm_count)

@@ -326,6 +326,15 @@ constexpr size_t warp_state_bytes(int G, int SPL)
             (size_t)SPL * (32 + ((G / SPL) > 1 ? (G / SPL) : 1)) * 4 + 15) / 16 * 16;
 }
 
+// Threads per CTA the chain kernel of a shape is compiled for (its register budget: 65536 /
+// threads). With 12 or more segments per lane every shape fits 768 threads (24 warps) in 80
+// registers without spills (forward variants), and the extra warps pay: N = 256 +6 %, 512
+// +13 %, 1024 +24 % over the 16 (8) warps of a 512-thread budget.
+__host__ __device__ constexpr int comp_max_threads(int G, int SPL)
+{
+    return (SPL >= 12) ? 768 : 1024;
+}
+
 // The segment lengths, one array per CTA: rotations never change a length, and every chain of
 // a CTA starts from the same initial curve, so all its chains share them (G * SPL floats,
 // padding segments 1).

@@ -85,7 +85,7 @@ template <int G, int SPL, bool EXACT, bool CLAMP, bool SHIFT, int MODE, bool INC
 cudaError_t launch_t(const ChainSpec &c, const CompConsts &kc, int warps, const float *init_seg, const float2 *tab,
                      ChainOut *out, double2 *partials, const ModeArgs &ma, size_t smem, uint32_t blocks, cudaStream_t st)
 {
-    constexpr int MAXT = (SPL >= 12) ? 512 : 1024;
+    constexpr int MAXT = comp_max_threads(G, SPL);
     if (warps * 32 > MAXT) return cudaErrorInvalidConfiguration;
     auto kern = comp_chain_kernel<G, SPL, EXACT, CLAMP, SHIFT, MAXT, MODE, INCR, STEEP, LUTG>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

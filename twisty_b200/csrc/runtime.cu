@@ -499,7 +499,7 @@ void prepare(twisty_ctx *ctx, const twisty_bc *bcp)
             if (!p.comp_group || !p.comp_spl) fail(TWISTY_ERR_INVALID_CONFIG, "comp_group and comp_spl are set together");
             ctx->tuning.group = (int)p.comp_group;
             ctx->tuning.spl = (int)p.comp_spl;
-            if (!p.comp_warps) ctx->tuning.warps_per_block = (p.comp_spl >= 12) ? 16 : 32;
+            if (!p.comp_warps) ctx->tuning.warps_per_block = (p.comp_spl >= 12) ? 24 : 32;
         }
         if (p.comp_warps) ctx->tuning.warps_per_block = (int)p.comp_warps;
         ctx->tuning.exact_blend = ctx->exact_blend;
@@ -1292,7 +1292,7 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
         c.absorption_factor = (double)std::exp(-p.absorption * h.ds);
         if (!comp_tuning_supported(h.t, N, c.k_eff))
             fail(TWISTY_ERR_UNSUPPORTED, exp_msg(e, "no compensated kernel shape for this N / max_sub_chain"));
-        const int maxt = (h.t.spl >= 12 || h.t.group <= 8) ? 512 : 1024;
+        const int maxt = batch_max_threads(h.t.group, h.t.spl);
         h.t.warps_per_block = std::min(h.t.warps_per_block, maxt / 32);
         const uint64_t cpb = (uint64_t)h.t.warps_per_block * (32u / (uint32_t)h.t.group);
         uint64_t chains = p.num_chains;
