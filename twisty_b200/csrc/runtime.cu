@@ -505,10 +505,10 @@ void prepare(twisty_ctx *ctx, const twisty_bc *bcp)
         ctx->tuning.exact_blend = ctx->exact_blend;
         if (!comp_tuning_supported(ctx->tuning, N, c.k_eff)) fail(TWISTY_ERR_UNSUPPORTED, "no compensated kernel shape for this N / max_sub_chain");
         // A table too large to stage beside the chain state costs warps per CTA; when staging it
-        // would leave fewer than 2/3 of the shape's warps, forward passes of the full recompute
-        // read it through L1 instead (measured on B200 with 10000- and 20000-bin tables: L1
-        // 4-23 % below a staged table at full occupancy, 12-53 % above one at 1/4 to 1/2 of
-        // the warps). comp_table_memory 1 / 2 force the choice.
+        // would leave fewer than the shape's warps, forward passes of the full recompute read it
+        // through L1 instead (measured on B200: L1 at full occupancy 0-9 % below a staged table
+        // at full occupancy, and from even with one at 5/6 of the warps to +14 % at 2/3 and +40 %
+        // and more at 1/4 to 1/2). comp_table_memory 1 / 2 force the choice.
         ctx->tuning.lut_global = 0;
         const bool can_global = c.incr_resync <= 1 && !c.has_eval_shift;
         bool few_warps = false;
@@ -517,7 +517,7 @@ void prepare(twisty_ctx *ctx, const twisty_bc *bcp)
             while (!p.comp_warps && staged.warps_per_block > 4 && comp_smem_bytes(staged, p.num_curvature_steps) > kSmemCap)
                 staged.warps_per_block -= 4;
             few_warps = comp_smem_bytes(staged, p.num_curvature_steps) > kSmemCap ||
-                        3 * staged.warps_per_block < 2 * ctx->tuning.warps_per_block;
+                        staged.warps_per_block < ctx->tuning.warps_per_block;
         }
         if (p.comp_table_memory == 2 || few_warps) {
             if (!can_global)
