@@ -1,4 +1,4 @@
-// batch_shapes_a.cu -- batched kernel variants for the shapes 1 x 8, 1 x 12, 4 x 2, 4 x 3, 4 x 4, 4 x 5, 4 x 8, 4 x 9, 8 x 2, 8 x 4, 8 x 8, 8 x 9, 8 x 12, 8 x 16, 8 x 17, 16 x 4, 16 x 8, 16 x 12, 16 x 16, 16 x 17
+// batch_shapes_a.cu -- batched kernel variants for the shapes 1 x 8, 1 x 12, 4 x 2, 4 x 3, 4 x 4, 4 x 5, 4 x 8, 4 x 9, 4 x 16, 4 x 17, 8 x 2, 8 x 4, 8 x 8, 8 x 9, 8 x 12, 8 x 16, 8 x 17, 16 x 4, 16 x 8, 16 x 12, 16 x 16, 16 x 17
 // (lanes per chain x segments per lane).
 #include "batch_launch.cuh"
 
@@ -14,6 +14,8 @@ bool batch_shapes_a_launch(const BatchShape &s, const BatchExp *exps, const uint
     TWISTY_BATCH_SHAPE_LAUNCH(4, 3)
     TWISTY_BATCH_SHAPE_LAUNCH(4, 5)
     TWISTY_BATCH_SHAPE_LAUNCH(4, 9)
+    TWISTY_BATCH_SHAPE_LAUNCH(4, 16)
+    TWISTY_BATCH_SHAPE_LAUNCH(4, 17)
     TWISTY_BATCH_SHAPE_LAUNCH(1, 8)
     TWISTY_BATCH_SHAPE_LAUNCH(1, 12)
     TWISTY_BATCH_SHAPE_LAUNCH(8, 9)
@@ -39,6 +41,8 @@ bool batch_shapes_a_occ(const BatchShape &s, size_t smem, int &occ)
     TWISTY_BATCH_SHAPE_OCC(4, 3)
     TWISTY_BATCH_SHAPE_OCC(4, 5)
     TWISTY_BATCH_SHAPE_OCC(4, 9)
+    TWISTY_BATCH_SHAPE_OCC(4, 16)
+    TWISTY_BATCH_SHAPE_OCC(4, 17)
     TWISTY_BATCH_SHAPE_OCC(1, 8)
     TWISTY_BATCH_SHAPE_OCC(1, 12)
     TWISTY_BATCH_SHAPE_OCC(8, 9)

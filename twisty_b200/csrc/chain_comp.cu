@@ -121,7 +121,8 @@ CompTuning comp_default_tuning(uint32_t n)
     else if (n <= 20) { t.group = 4; t.spl = 5; t.warps_per_block = 32; }
     else if (n <= 32) { t.group = 4; t.spl = 8; t.warps_per_block = 32; }
     else if (n <= 36) { t.group = 4; t.spl = 9; t.warps_per_block = 32; }
-    else if (n <= 64) { t.group = 8; t.spl = 8; t.warps_per_block = 32; }
+    else if (n <= 64) { t.group = 4; t.spl = 16; t.warps_per_block = 24; }
+    else if (n <= 68) { t.group = 4; t.spl = 17; t.warps_per_block = 24; }
     else if (n <= 72) { t.group = 8; t.spl = 9; t.warps_per_block = 32; }
     else if (n <= 96) { t.group = 8; t.spl = 12; t.warps_per_block = 24; }
     else if (n <= 128) { t.group = 8; t.spl = 16; t.warps_per_block = 24; }
@@ -141,7 +142,7 @@ bool comp_tuning_supported(const CompTuning &t, uint32_t n, uint32_t k_eff)
 {
     const int s = t.spl;
     const bool shape = (t.group == 1 && (s == 8 || s == 12)) ||
-                       (t.group == 4 && (s == 2 || s == 3 || s == 4 || s == 5 || s == 8 || s == 9)) ||
+                       (t.group == 4 && (s == 2 || s == 3 || s == 4 || s == 5 || s == 8 || s == 9 || s == 16 || s == 17)) ||
                        (t.group == 8 && (s == 2 || s == 4 || s == 8 || s == 9 || s == 12 || s == 16 || s == 17 || s == 32)) ||
                        (t.group == 16 && (s == 4 || s == 8 || s == 12 || s == 16 || s == 17)) ||
                        (t.group == 32 && (s == 4 || s == 8 || s == 12 || s == 16 || s == 17 || s == 24 || s == 32));

@@ -24,7 +24,7 @@ struct CompLaunch {
 };
 
 // Each returns false when the launch's shape is not among its own, else launches and sets e.
-bool launch_comp_shapes_a(const CompLaunch &a, cudaError_t &e);   // 1 x {8, 12}, 4 x {2, 3, 4, 5, 8, 9}, 8 x {2, 4}
+bool launch_comp_shapes_a(const CompLaunch &a, cudaError_t &e);   // 1 x {8, 12}, 4 x {2..17}, 8 x {2, 4}
 bool launch_comp_shapes_b(const CompLaunch &a, cudaError_t &e);   // 8 x {8, 9, 12, 16, 17, 32}
 bool launch_comp_shapes_c(const CompLaunch &a, cudaError_t &e);   // 16 x {4, 8, 12, 16, 17}
 bool launch_comp_shapes_d(const CompLaunch &a, cudaError_t &e);   // 32 x {4, 8, 12, 17}
