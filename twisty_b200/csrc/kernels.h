@@ -175,7 +175,7 @@ void batch_pack_experiments(const BatchExpHost *in, uint32_t n, void *dst);
 bool batch_shape_supported(const BatchShape &s, uint32_t n_max, uint32_t k_eff);
 // Threads per CTA the batched kernel of a shape is compiled for (8-lane and narrower shapes
 // with few segments per lane keep 512: the work-item loop costs them registers).
-constexpr int batch_max_threads(int G, int SPL) { return SPL >= 12 ? 768 : (G <= 8 ? 512 : 1024); }
+constexpr int batch_max_threads(int G, int SPL) { return SPL >= 12 ? 768 : (G <= 8 ? 768 : 1024); }
 size_t batch_smem_bytes(const BatchShape &s, uint32_t bins);
 int batch_chains_per_block(const BatchShape &s);
 // Resident CTAs per SM of the shape's kernel (0 when it cannot launch).
