@@ -25,7 +25,7 @@ __global__ void __launch_bounds__(256) weigh_comp_kernel(const float *__restrict
             x = pp[3 * s + 3] - pp[3 * s];
             y = pp[3 * s + 4] - pp[3 * s + 1];
             z = pp[3 * s + 5] - pp[3 * s + 2];
-            const float r = rsqrtf(fmaf(x, x, fmaf(y, y, z * z)));
+            const float r = rsqrtf(fmaf(x, x, fmaf(y, y, z * z))) * kc.kscale;   // tangents at length kscale
             x *= r; y *= r; z *= r;
         } else {
             x = y = z = 0.f;

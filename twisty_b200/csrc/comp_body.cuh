@@ -61,7 +61,8 @@ namespace twisty {
 
 // Shared by the translation units that instantiate the chain kernels (plain structs).
 struct CompConsts {
-    float kscale;        // (N/S) / step : |t_{i+1}-t_i| -> fractional bin index
+    float kscale;        // (N/S) / step : |t_{i+1}-t_i| -> fractional bin index; the chain kernels keep
+                         // their tangents scaled to length kscale, so |t'_{i+1}-t'_i| is the index
     float roff;          // -min_k / step
     float rmax;          // (max_k - min_k) / step
     float rsnap;         // 1e-3 / step: overshoot that counts as clamped
@@ -167,7 +168,9 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float x)
 template <bool CLAMP>
 __device__ __forceinline__ float bin_of(float qq, const CompConsts &k, bool valid, uint32_t &clamped, int32_t &L)
 {
-    float r = fmaf(sqrt_approx(qq), k.kscale, k.roff);
+    // qq is |t'_{i+1} - t'_i|^2 of tangents scaled to length kscale: its root is the
+    // fractional bin of a table starting at curvature 0 (tables that need no clamping do)
+    float r = CLAMP ? sqrt_approx(qq) + k.roff : sqrt_approx(qq);
     if (CLAMP) {
         if (r < 0.0f) r = 0.0f;
         if (r > k.rmax) {
@@ -442,9 +445,11 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
     const uint32_t N = c.n_segments;
     using Lay = Layout<G, SPL>;
     // segment record (tangent, length) of segment index s = owner*SPL + m
+    // the tangents are stored at length kscale; records handed to export and the adjoint are unit
+    const float inv_ks = 1.0f / kc.kscale;
     auto load_rec = [&](uint32_t owner, uint32_t m) {
         const float2 a = st.xy[Lay::xy(gbase + owner, m)];
-        return make_float4(a.x, a.y, st.z[Lay::z(gbase + owner, m)], st.l[owner * SPL + m]);
+        return make_float4(a.x * inv_ks, a.y * inv_ks, st.z[Lay::z(gbase + owner, m)] * inv_ks, st.l[owner * SPL + m]);
     };
 
     float max_len = 0.f;
@@ -461,7 +466,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
             len = ss * r;
             x *= r; y *= r; z *= r;
             const float h = fmaf(-0.5f, fmaf(x, x, fmaf(y, y, z * z)), 1.5f);   // one Newton step to |t| = 1
-            x *= h; y *= h; z *= h;
+            x *= h * kc.kscale; y *= h * kc.kscale; z *= h * kc.kscale;       // stored at length kscale
             max_len = fmaxf(max_len, len);
         }
         st.xy[Lay::xy(gbase + j, m)] = make_float2(x, y);
@@ -470,7 +475,8 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
 #pragma unroll
     for (int o = 1; o < G; o <<= 1) max_len = fmaxf(max_len, __shfl_xor_sync(FULL, max_len, o));
     // fixed-point chord scale: a segment is at most 2^24 units, 64 of them at most 2^30
-    const float chord_scale = 16777216.0f / max_len;
+    const float chord_scale = 16777216.0f / (max_len * kc.kscale);   // the tangents have length kscale
+    const float renorm = -0.5f * inv_ks * inv_ks;   // Newton step to |t'| = kscale: 1.5 + renorm |t'|^2
     __syncwarp();
 
     const uint32_t steps_c = real_chain ? ((chain == c.n_chains - 1) ? c.last_steps : c.steps) : 0;
@@ -515,11 +521,11 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
         y = a.y;
         z = st.z[Lay::z(own, m)];
         if (SHIFT && j * SPL + m == N - 2) {
-            const float l = st.l[j * SPL + m];
+            const float l = st.l[j * SPL + m] * inv_ks;
             x = fmaf(l, x, c.eval_shift[0]);
             y = fmaf(l, y, c.eval_shift[1]);
             z = fmaf(l, z, c.eval_shift[2]);
-            const float r = rsqrtf(fmaf(x, x, fmaf(y, y, z * z)));
+            const float r = rsqrtf(fmaf(x, x, fmaf(y, y, z * z))) * kc.kscale;
             x *= r; y *= r; z *= r;
         }
     };
@@ -629,7 +635,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                     const float nx = fmaf(ax, ad, fmaf(sth, crx, fmaf(-omc, x, x)));
                     const float ny = fmaf(ay, ad, fmaf(sth, cry, fmaf(-omc, y, y)));
                     const float nz = fmaf(az, ad, fmaf(sth, crz, fmaf(-omc, z, z)));
-                    const float h = fmaf(-0.5f, fmaf(nx, nx, fmaf(ny, ny, nz * nz)), 1.5f);
+                    const float h = fmaf(renorm, fmaf(nx, nx, fmaf(ny, ny, nz * nz)), 1.5f);
                     st.xy[va[ri]] = make_float2(nx * h, ny * h);
                     st.z[vb[ri]] = nz * h;
                 }
@@ -758,7 +764,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                 // log10 weight and d/d(mu_s), d/d(eps) of this lane's segments (exact blend)
                 float s = 0.f, cc = 0.f, gmu = 0.f, geps = 0.f;
                 for_curvatures<G, SPL, false>(j, N, tan_smem, next_smem, [&](uint32_t, float qq, bool valid) {
-                    float r = fmaf(sqrt_approx(qq), kc.kscale, kc.roff);
+                    float r = sqrt_approx(qq) + kc.roff;   // scaled tangents: the root is the bin index
                     if (r < 0.f) r = 0.f;
                     if (r > kc.rmax) r = kc.rmax;
                     const int32_t L = min((int32_t)r, kc.bins - 1);
