@@ -104,6 +104,9 @@ bool comp_table_needs_clamp(float inv_ds, const LutMetaF &m)
 // per lane keep 16 independent table loads in flight per lane, which outweighs the halved
 // warp count above N = 64. The 12- and 24-segment shapes cover the N between powers of two
 // with less padding (measured: N = 192, 384, 768 18-27 % faster than the next power of two).
+// 32 x 24 runs 24 warps, which leaves no room to stage a table: through L1 it measured 3-5 %
+// above 16 warps with a staged table at N = 768 (4096 and 8192 bins). 32 x 32 stays at 12
+// warps: 16 warps through L1 measured even with it at N = 1024.
 // Up to N = 32, 4-lane groups put 8 chains in a warp, which share the per-step work of the
 // proposal broadcast, the group reductions and the log-sum-exp (N = 16: +23 %, 32: +12 %
 // over 8 lanes); up to N = 12 one lane carries a whole chain, 32 chains per warp, with no group
@@ -133,7 +136,7 @@ CompTuning comp_default_tuning(uint32_t n)
     else if (n <= 384) { t.group = 32; t.spl = 12; t.warps_per_block = 24; }
     else if (n <= 512) { t.group = 32; t.spl = 16; t.warps_per_block = 24; }
     else if (n <= 544) { t.group = 32; t.spl = 17; t.warps_per_block = 24; }
-    else if (n <= 768) { t.group = 32; t.spl = 24; t.warps_per_block = 16; }
+    else if (n <= 768) { t.group = 32; t.spl = 24; t.warps_per_block = 24; }
     else { t.group = 32; t.spl = 32; t.warps_per_block = 12; }
     return t;
 }
