@@ -104,9 +104,9 @@ bool comp_table_needs_clamp(float inv_ds, const LutMetaF &m)
 // per lane keep 16 independent table loads in flight per lane, which outweighs the halved
 // warp count above N = 64. The 12- and 24-segment shapes cover the N between powers of two
 // with less padding (measured: N = 192, 384, 768 18-27 % faster than the next power of two).
-// 32 x 24 runs 24 warps, which leaves no room to stage a table: through L1 it measured 3-5 %
-// above 16 warps with a staged table at N = 768 (4096 and 8192 bins). 32 x 32 stays at 12
-// warps: 16 warps through L1 measured even with it at N = 1024.
+// 32 x 24 runs 24 warps, which leave no room to stage a table: it stages one at 20 warps when
+// that fits (comp_stage_min_warps) and gathers it through L1 at 24 otherwise. 32 x 32 stays
+// at 12 warps: 16 warps through L1 measured even with it at N = 1024.
 // Up to N = 32, 4-lane groups put 8 chains in a warp, which share the per-step work of the
 // proposal broadcast, the group reductions and the log-sum-exp (N = 16: +23 %, 32: +12 %
 // over 8 lanes); up to N = 12 one lane carries a whole chain, 32 chains per warp, with no group
@@ -139,6 +139,16 @@ CompTuning comp_default_tuning(uint32_t n)
     else if (n <= 768) { t.group = 32; t.spl = 24; t.warps_per_block = 24; }
     else { t.group = 32; t.spl = 32; t.warps_per_block = 12; }
     return t;
+}
+
+// The fewest warps per CTA at which staging the table in shared memory is kept over gathering
+// it through L1 at the shape's full warps. 32 x 24 at 24 warps has no room for a table; at 20
+// warps a staged table measured 1-5 % above L1 at 24 (N = 640, 768; 2048 and 4096 bins) and L1
+// at 24 3-13 % above 16 staged warps (N = 600-768, 4096 to 20000 bins). Other shapes stage only
+// at full warps.
+int comp_stage_min_warps(const CompTuning &t)
+{
+    return (t.group == 32 && t.spl == 24 && t.warps_per_block == 24) ? 20 : t.warps_per_block;
 }
 
 bool comp_tuning_supported(const CompTuning &t, uint32_t n, uint32_t k_eff)

@@ -126,6 +126,7 @@ struct CompTuning {
                              // (forward passes only; the chain state keeps the shared memory)
 };
 CompTuning comp_default_tuning(uint32_t n_segments);
+int comp_stage_min_warps(const CompTuning &t);
 bool comp_tuning_supported(const CompTuning &t, uint32_t n_segments, uint32_t k_eff);
 uint32_t comp_default_chains(uint32_t n_segments, int sm_count);
 size_t comp_smem_bytes(const CompTuning &t, uint32_t bins);

@@ -517,7 +517,7 @@ void prepare(twisty_ctx *ctx, const twisty_bc *bcp)
             while (!p.comp_warps && staged.warps_per_block > 4 && comp_smem_bytes(staged, p.num_curvature_steps) > kSmemCap)
                 staged.warps_per_block -= 4;
             few_warps = comp_smem_bytes(staged, p.num_curvature_steps) > kSmemCap ||
-                        staged.warps_per_block < ctx->tuning.warps_per_block;
+                        staged.warps_per_block < comp_stage_min_warps(ctx->tuning);
         }
         if (p.comp_table_memory == 2 || few_warps) {
             if (!can_global)
@@ -1294,6 +1294,17 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
             fail(TWISTY_ERR_UNSUPPORTED, exp_msg(e, "no compensated kernel shape for this N / max_sub_chain"));
         const int maxt = batch_max_threads(h.t.group, h.t.spl);
         h.t.warps_per_block = std::min(h.t.warps_per_block, maxt / 32);
+        {
+            // a staged table may take the shape down to comp_stage_min_warps; below that the
+            // table is gathered through L1 at the shape's full warps
+            const int floor_w = comp_stage_min_warps(h.t);
+            auto staged_fits = [&](int w) {
+                return batch_smem_bytes(BatchShape{h.t.group, h.t.spl, w, 0, 1, 0, 1}, bins) <= kSmemCap;
+            };
+            int w = h.t.warps_per_block;
+            while (w - 4 >= floor_w && !staged_fits(w)) w -= 4;
+            if (staged_fits(w)) h.t.warps_per_block = w;
+        }
         const uint64_t cpb = (uint64_t)h.t.warps_per_block * (32u / (uint32_t)h.t.group);
         uint64_t chains = p.num_chains;
         if (!chains) chains = cpb * std::max<uint64_t>(1, (x.paths + cpb * 1024) / (cpb * 2048));
