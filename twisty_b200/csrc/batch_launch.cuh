@@ -1,5 +1,5 @@
 // batch_launch.cuh -- the batched persistent kernel and its per-shape launchers, included by
-// batch.cu (the host side of the batched form) and by batch_shapes_{a,b}.cu, which instantiate
+// batch.cu (the host side of the batched form) and by batch_shapes_{a,b,c}.cu, which instantiate
 // the kernel for a few shapes each so that the variants compile in parallel.
 #pragma once
 #include "comp_body.cuh"
@@ -31,8 +31,12 @@ bool batch_shapes_a_launch(const BatchShape &s, const BatchExp *exps, const uint
 bool batch_shapes_b_launch(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items,
                            uint32_t *counter, ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st,
                            cudaError_t &e);   // 32 x {4, 8, 12, 16, 17, 24, 32}
+bool batch_shapes_c_launch(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items,
+                           uint32_t *counter, ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st,
+                           cudaError_t &e);   // 16 x 20, 32 x {20, 28}
 bool batch_shapes_a_occ(const BatchShape &s, size_t smem, int &occ);
 bool batch_shapes_b_occ(const BatchShape &s, size_t smem, int &occ);
+bool batch_shapes_c_occ(const BatchShape &s, size_t smem, int &occ);
 
 namespace {
 

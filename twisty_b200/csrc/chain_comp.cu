@@ -1,6 +1,6 @@
 // chain_comp.cu -- single-run entry points of the compensated form: the weigher of given
 // paths, the launchers and the kernel-shape table. The chain kernel (comp_launch.cuh, body in
-// comp_body.cuh) is instantiated per shape in comp_shapes_{a..e}.cu, compiled in parallel.
+// comp_body.cuh) is instantiated per shape in comp_shapes_{a..f}.cu, compiled in parallel.
 #include "comp_launch.cuh"
 
 namespace twisty {
@@ -68,7 +68,7 @@ cudaError_t launch_mode(int mode, const ChainSpec &c, const CompTuning &t, const
     const CompLaunch a{mode, exact, clamp, shift, steep, c, kc, t, init_seg, tab, out, block_partials, mb, smem, blocks, st};
     cudaError_t e = cudaSuccess;
     if (launch_comp_shapes_a(a, e) || launch_comp_shapes_b(a, e) || launch_comp_shapes_c(a, e) ||
-        launch_comp_shapes_d(a, e) || launch_comp_shapes_e(a, e))
+        launch_comp_shapes_d(a, e) || launch_comp_shapes_e(a, e) || launch_comp_shapes_f(a, e))
         return e;
     return cudaErrorInvalidValue;
 }
@@ -133,10 +133,13 @@ CompTuning comp_default_tuning(uint32_t n)
     else if (n <= 192) { t.group = 16; t.spl = 12; t.warps_per_block = 24; }
     else if (n <= 256) { t.group = 16; t.spl = 16; t.warps_per_block = 24; }
     else if (n <= 272) { t.group = 16; t.spl = 17; t.warps_per_block = 24; }
+    else if (n <= 320) { t.group = 16; t.spl = 20; t.warps_per_block = 24; }
     else if (n <= 384) { t.group = 32; t.spl = 12; t.warps_per_block = 24; }
     else if (n <= 512) { t.group = 32; t.spl = 16; t.warps_per_block = 24; }
     else if (n <= 544) { t.group = 32; t.spl = 17; t.warps_per_block = 24; }
+    else if (n <= 640) { t.group = 32; t.spl = 20; t.warps_per_block = 24; }
     else if (n <= 768) { t.group = 32; t.spl = 24; t.warps_per_block = 24; }
+    else if (n <= 896) { t.group = 32; t.spl = 28; t.warps_per_block = 16; }
     else { t.group = 32; t.spl = 32; t.warps_per_block = 12; }
     return t;
 }
@@ -157,8 +160,9 @@ bool comp_tuning_supported(const CompTuning &t, uint32_t n, uint32_t k_eff)
     const bool shape = (t.group == 1 && (s == 8 || s == 12)) ||
                        (t.group == 4 && (s == 2 || s == 3 || s == 4 || s == 5 || s == 8 || s == 9 || s == 16 || s == 17)) ||
                        (t.group == 8 && (s == 2 || s == 4 || s == 8 || s == 9 || s == 12 || s == 16 || s == 17 || s == 32)) ||
-                       (t.group == 16 && (s == 4 || s == 8 || s == 12 || s == 16 || s == 17)) ||
-                       (t.group == 32 && (s == 4 || s == 8 || s == 12 || s == 16 || s == 17 || s == 24 || s == 32));
+                       (t.group == 16 && (s == 4 || s == 8 || s == 12 || s == 16 || s == 17 || s == 20)) ||
+                       (t.group == 32 && (s == 4 || s == 8 || s == 12 || s == 16 || s == 17 || s == 20 || s == 24 ||
+                                          s == 28 || s == 32));
     return shape && (uint32_t)(t.group * t.spl) >= n && n >= 4 && k_eff <= (uint32_t)kMaxSubChain &&
            t.warps_per_block >= 1 && t.warps_per_block * 32 <= comp_max_threads(t.group, t.spl);
 }

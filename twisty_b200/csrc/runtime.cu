@@ -1708,7 +1708,7 @@ twisty_status twisty_autotune(twisty_ctx *ctx, const twisty_bc *bc, uint64_t tri
         std::vector<Cand> cands;
         const CompTuning def = comp_default_tuning(N);
         for (int g : {1, 4, 8, 16, 32})
-            for (int spl : {2, 3, 4, 5, 6, 8, 9, 12, 16, 17, 24, 32})
+            for (int spl : {2, 3, 4, 5, 6, 8, 9, 12, 16, 17, 20, 24, 28, 32})
                 for (int w = 4; w <= 32; w += 4) {
                     CompTuning t{g, spl, w, 0};
                     const uint32_t k_eff = std::min<uint32_t>(saved.max_sub_chain, N - 2);
