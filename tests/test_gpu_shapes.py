@@ -17,7 +17,7 @@ import twisty_b200 as T
 pytestmark = pytest.mark.gpu
 
 NS = [4, 5, 6, 7, 8, 9, 10, 12, 16, 17, 18, 20, 31, 32, 33, 34, 36, 48, 64, 65, 66, 72, 96, 100, 128, 129, 130,
-      136, 192, 200, 256, 257, 258, 272, 300, 320, 384, 400, 512, 513, 514, 544, 600, 640, 768, 800, 850, 896,
+      136, 150, 160, 170, 192, 200, 256, 257, 258, 272, 300, 320, 350, 384, 400, 420, 448, 512, 513, 514, 544, 600, 640, 768, 800, 850, 896,
       1000, 1024]
 
 
@@ -48,7 +48,9 @@ def test_default_shape_matches_fp64(N):
 
 @pytest.mark.parametrize("N,shapes", [(24, [(4, 8, 32), (8, 4, 32), (16, 4, 16), (32, 4, 16)]),
                                       (150, [(16, 12, 16), (8, 32, 8), (16, 16, 16), (32, 8, 16)]),
+                                      (170, [(8, 24, 16), (16, 12, 16), (16, 16, 16)]),
                                       (300, [(16, 20, 16), (32, 12, 16)]),
+                                      (440, [(16, 28, 16), (32, 16, 16)]),
                                       (600, [(32, 20, 16), (32, 24, 16)]),
                                       (700, [(32, 24, 8), (32, 32, 8)]),
                                       (850, [(32, 28, 8), (32, 32, 8)])])

@@ -43,7 +43,8 @@ int batch_blocks_per_sm(const BatchShape &s, int bins)
 {
     const size_t smem = batch_smem_bytes(s, (uint32_t)bins);
     int occ = 0;
-    if (batch_shapes_a_occ(s, smem, occ) || batch_shapes_b_occ(s, smem, occ) || batch_shapes_c_occ(s, smem, occ))
+    if (batch_shapes_a_occ(s, smem, occ) || batch_shapes_b_occ(s, smem, occ) || batch_shapes_c_occ(s, smem, occ) ||
+        batch_shapes_d_occ(s, smem, occ))
         return occ;
     return 0;
 }
@@ -56,7 +57,8 @@ cudaError_t launch_batch(const BatchShape &s, const void *d_exps, const uint2 *d
     cudaError_t e = cudaSuccess;
     if (batch_shapes_a_launch(s, exps, d_items, n_items, d_counter, out, bins, grid, smem, st, e) ||
         batch_shapes_b_launch(s, exps, d_items, n_items, d_counter, out, bins, grid, smem, st, e) ||
-        batch_shapes_c_launch(s, exps, d_items, n_items, d_counter, out, bins, grid, smem, st, e))
+        batch_shapes_c_launch(s, exps, d_items, n_items, d_counter, out, bins, grid, smem, st, e) ||
+        batch_shapes_d_launch(s, exps, d_items, n_items, d_counter, out, bins, grid, smem, st, e))
         return e;
     return cudaErrorInvalidValue;
 }

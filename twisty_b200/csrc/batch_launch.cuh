@@ -34,9 +34,13 @@ bool batch_shapes_b_launch(const BatchShape &s, const BatchExp *exps, const uint
 bool batch_shapes_c_launch(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items,
                            uint32_t *counter, ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st,
                            cudaError_t &e);   // 16 x 20, 32 x {20, 28}
+bool batch_shapes_d_launch(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items,
+                           uint32_t *counter, ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st,
+                           cudaError_t &e);   // 8 x {20, 24}, 16 x {24, 28, 32}
 bool batch_shapes_a_occ(const BatchShape &s, size_t smem, int &occ);
 bool batch_shapes_b_occ(const BatchShape &s, size_t smem, int &occ);
 bool batch_shapes_c_occ(const BatchShape &s, size_t smem, int &occ);
+bool batch_shapes_d_occ(const BatchShape &s, size_t smem, int &occ);
 
 namespace {
 

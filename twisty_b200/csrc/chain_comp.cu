@@ -68,7 +68,8 @@ cudaError_t launch_mode(int mode, const ChainSpec &c, const CompTuning &t, const
     const CompLaunch a{mode, exact, clamp, shift, steep, c, kc, t, init_seg, tab, out, block_partials, mb, smem, blocks, st};
     cudaError_t e = cudaSuccess;
     if (launch_comp_shapes_a(a, e) || launch_comp_shapes_b(a, e) || launch_comp_shapes_c(a, e) ||
-        launch_comp_shapes_d(a, e) || launch_comp_shapes_e(a, e) || launch_comp_shapes_f(a, e))
+        launch_comp_shapes_d(a, e) || launch_comp_shapes_e(a, e) || launch_comp_shapes_f(a, e) ||
+        launch_comp_shapes_g(a, e))
         return e;
     return cudaErrorInvalidValue;
 }
@@ -104,9 +105,14 @@ bool comp_table_needs_clamp(float inv_ds, const LutMetaF &m)
 // per lane keep 16 independent table loads in flight per lane, which outweighs the halved
 // warp count above N = 64. The 12- and 24-segment shapes cover the N between powers of two
 // with less padding (measured: N = 192, 384, 768 18-27 % faster than the next power of two).
-// 32 x 24 runs 24 warps, which leave no room to stage a table: it stages one at 20 warps when
-// that fits (comp_stage_min_warps) and gathers it through L1 at 24 otherwise. 32 x 32 stays
-// at 12 warps: 16 warps through L1 measured even with it at N = 1024.
+// Fewer lanes per chain with more segments each (8 x {20, 24}, 16 x {20, 24, 28}) put two or
+// four chains in a warp and measured 13-32 % faster than the 16- and 32-lane shapes padded to
+// the same N (N = 160, 192, 320, 384, 448); 16 x 32 at N = 512 measured only 2 % above 32 x 16
+// and would drop to 12 warps through L1 for large tables, so 32 x 16 stays. The 24-segment
+// shapes run 24 warps, which leave no room to stage a table: they stage one at 20 warps when
+// that fits (comp_stage_min_warps) and gather it through L1 at 24 otherwise; 16 x 28 likewise
+// stages at 16 and gathers at 20. 32 x 32 stays at 12 warps: 16 warps through L1 measured even
+// with it at N = 1024.
 // Up to N = 32, 4-lane groups put 8 chains in a warp, which share the per-step work of the
 // proposal broadcast, the group reductions and the log-sum-exp (N = 16: +23 %, 32: +12 %
 // over 8 lanes); up to N = 12 one lane carries a whole chain, 32 chains per warp, with no group
@@ -130,11 +136,13 @@ CompTuning comp_default_tuning(uint32_t n)
     else if (n <= 96) { t.group = 8; t.spl = 12; t.warps_per_block = 24; }
     else if (n <= 128) { t.group = 8; t.spl = 16; t.warps_per_block = 24; }
     else if (n <= 136) { t.group = 8; t.spl = 17; t.warps_per_block = 24; }
-    else if (n <= 192) { t.group = 16; t.spl = 12; t.warps_per_block = 24; }
+    else if (n <= 160) { t.group = 8; t.spl = 20; t.warps_per_block = 24; }
+    else if (n <= 192) { t.group = 8; t.spl = 24; t.warps_per_block = 24; }
     else if (n <= 256) { t.group = 16; t.spl = 16; t.warps_per_block = 24; }
     else if (n <= 272) { t.group = 16; t.spl = 17; t.warps_per_block = 24; }
     else if (n <= 320) { t.group = 16; t.spl = 20; t.warps_per_block = 24; }
-    else if (n <= 384) { t.group = 32; t.spl = 12; t.warps_per_block = 24; }
+    else if (n <= 384) { t.group = 16; t.spl = 24; t.warps_per_block = 24; }
+    else if (n <= 448) { t.group = 16; t.spl = 28; t.warps_per_block = 20; }
     else if (n <= 512) { t.group = 32; t.spl = 16; t.warps_per_block = 24; }
     else if (n <= 544) { t.group = 32; t.spl = 17; t.warps_per_block = 24; }
     else if (n <= 640) { t.group = 32; t.spl = 20; t.warps_per_block = 24; }
@@ -145,13 +153,16 @@ CompTuning comp_default_tuning(uint32_t n)
 }
 
 // The fewest warps per CTA at which staging the table in shared memory is kept over gathering
-// it through L1 at the shape's full warps. 32 x 24 at 24 warps has no room for a table; at 20
-// warps a staged table measured 1-5 % above L1 at 24 (N = 640, 768; 2048 and 4096 bins) and L1
-// at 24 3-13 % above 16 staged warps (N = 600-768, 4096 to 20000 bins). Other shapes stage only
-// at full warps.
+// it through L1 at the shape's full warps. The 24-segment shapes at 24 warps have no room for a
+// table; at 20 warps a staged table measured above L1 at 24 (32 x 24: 1-5 % at N = 640, 768;
+// 16 x 24: 3 % at N = 384; 8 x 24: 4 % at N = 192, 4096 bins) and L1 at 24 3-13 % above 16
+// staged warps (32 x 24, N = 600-768, 4096 to 20000 bins). 16 x 28 staged at 16 warps measured
+// 5 % above L1 at 20 (N = 448). Other shapes stage only at full warps.
 int comp_stage_min_warps(const CompTuning &t)
 {
-    return (t.group == 32 && t.spl == 24 && t.warps_per_block == 24) ? 20 : t.warps_per_block;
+    if (t.spl == 24 && t.warps_per_block == 24) return 20;
+    if (t.group == 16 && t.spl == 28 && t.warps_per_block == 20) return 16;
+    return t.warps_per_block;
 }
 
 bool comp_tuning_supported(const CompTuning &t, uint32_t n, uint32_t k_eff)
@@ -159,8 +170,10 @@ bool comp_tuning_supported(const CompTuning &t, uint32_t n, uint32_t k_eff)
     const int s = t.spl;
     const bool shape = (t.group == 1 && (s == 8 || s == 12)) ||
                        (t.group == 4 && (s == 2 || s == 3 || s == 4 || s == 5 || s == 8 || s == 9 || s == 16 || s == 17)) ||
-                       (t.group == 8 && (s == 2 || s == 4 || s == 8 || s == 9 || s == 12 || s == 16 || s == 17 || s == 32)) ||
-                       (t.group == 16 && (s == 4 || s == 8 || s == 12 || s == 16 || s == 17 || s == 20)) ||
+                       (t.group == 8 && (s == 2 || s == 4 || s == 8 || s == 9 || s == 12 || s == 16 || s == 17 || s == 20 ||
+                                         s == 24 || s == 32)) ||
+                       (t.group == 16 && (s == 4 || s == 8 || s == 12 || s == 16 || s == 17 || s == 20 || s == 24 ||
+                                          s == 28 || s == 32)) ||
                        (t.group == 32 && (s == 4 || s == 8 || s == 12 || s == 16 || s == 17 || s == 20 || s == 24 ||
                                           s == 28 || s == 32));
     return shape && (uint32_t)(t.group * t.spl) >= n && n >= 4 && k_eff <= (uint32_t)kMaxSubChain &&

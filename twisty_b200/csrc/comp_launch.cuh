@@ -30,6 +30,7 @@ bool launch_comp_shapes_c(const CompLaunch &a, cudaError_t &e);   // 16 x {4, 8,
 bool launch_comp_shapes_d(const CompLaunch &a, cudaError_t &e);   // 32 x {4, 8, 12, 17}
 bool launch_comp_shapes_e(const CompLaunch &a, cudaError_t &e);   // 32 x {16, 24, 32}
 bool launch_comp_shapes_f(const CompLaunch &a, cudaError_t &e);   // 16 x 20, 32 x {20, 28}
+bool launch_comp_shapes_g(const CompLaunch &a, cudaError_t &e);   // 8 x {20, 24}, 16 x {24, 28, 32}
 
 namespace {
 
