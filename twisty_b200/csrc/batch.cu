@@ -1,6 +1,6 @@
 // batch.cu -- the host side of the batched persistent form: experiment packing, shape and
 // occupancy queries, and the launch, which dispatches to the kernel variants instantiated in
-// batch_shapes_{a,b,c}.cu (batch_launch.cuh holds the kernel; comp_body.cuh the chain body).
+// batch_shapes_{a..e}.cu (batch_launch.cuh holds the kernel; comp_body.cuh the chain body).
 #include "batch_launch.cuh"
 
 namespace twisty {
@@ -44,7 +44,7 @@ int batch_blocks_per_sm(const BatchShape &s, int bins)
     const size_t smem = batch_smem_bytes(s, (uint32_t)bins);
     int occ = 0;
     if (batch_shapes_a_occ(s, smem, occ) || batch_shapes_b_occ(s, smem, occ) || batch_shapes_c_occ(s, smem, occ) ||
-        batch_shapes_d_occ(s, smem, occ))
+        batch_shapes_d_occ(s, smem, occ) || batch_shapes_e_occ(s, smem, occ))
         return occ;
     return 0;
 }
@@ -58,7 +58,8 @@ cudaError_t launch_batch(const BatchShape &s, const void *d_exps, const uint2 *d
     if (batch_shapes_a_launch(s, exps, d_items, n_items, d_counter, out, bins, grid, smem, st, e) ||
         batch_shapes_b_launch(s, exps, d_items, n_items, d_counter, out, bins, grid, smem, st, e) ||
         batch_shapes_c_launch(s, exps, d_items, n_items, d_counter, out, bins, grid, smem, st, e) ||
-        batch_shapes_d_launch(s, exps, d_items, n_items, d_counter, out, bins, grid, smem, st, e))
+        batch_shapes_d_launch(s, exps, d_items, n_items, d_counter, out, bins, grid, smem, st, e) ||
+        batch_shapes_e_launch(s, exps, d_items, n_items, d_counter, out, bins, grid, smem, st, e))
         return e;
     return cudaErrorInvalidValue;
 }

@@ -1,5 +1,5 @@
 // batch_launch.cuh -- the batched persistent kernel and its per-shape launchers, included by
-// batch.cu (the host side of the batched form) and by batch_shapes_{a,b,c}.cu, which instantiate
+// batch.cu (the host side of the batched form) and by batch_shapes_{a..e}.cu, which instantiate
 // the kernel for a few shapes each so that the variants compile in parallel.
 #pragma once
 #include "comp_body.cuh"
@@ -37,10 +37,14 @@ bool batch_shapes_c_launch(const BatchShape &s, const BatchExp *exps, const uint
 bool batch_shapes_d_launch(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items,
                            uint32_t *counter, ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st,
                            cudaError_t &e);   // 8 x {20, 24}, 16 x {24, 28, 32}
+bool batch_shapes_e_launch(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items,
+                           uint32_t *counter, ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st,
+                           cudaError_t &e);   // 4 x {20, 24, 28, 32}
 bool batch_shapes_a_occ(const BatchShape &s, size_t smem, int &occ);
 bool batch_shapes_b_occ(const BatchShape &s, size_t smem, int &occ);
 bool batch_shapes_c_occ(const BatchShape &s, size_t smem, int &occ);
 bool batch_shapes_d_occ(const BatchShape &s, size_t smem, int &occ);
+bool batch_shapes_e_occ(const BatchShape &s, size_t smem, int &occ);
 
 namespace {
 

@@ -1,6 +1,6 @@
 // chain_comp.cu -- single-run entry points of the compensated form: the weigher of given
 // paths, the launchers and the kernel-shape table. The chain kernel (comp_launch.cuh, body in
-// comp_body.cuh) is instantiated per shape in comp_shapes_{a..f}.cu, compiled in parallel.
+// comp_body.cuh) is instantiated per shape in comp_shapes_{a..h}.cu, compiled in parallel.
 #include "comp_launch.cuh"
 
 namespace twisty {
@@ -69,7 +69,7 @@ cudaError_t launch_mode(int mode, const ChainSpec &c, const CompTuning &t, const
     cudaError_t e = cudaSuccess;
     if (launch_comp_shapes_a(a, e) || launch_comp_shapes_b(a, e) || launch_comp_shapes_c(a, e) ||
         launch_comp_shapes_d(a, e) || launch_comp_shapes_e(a, e) || launch_comp_shapes_f(a, e) ||
-        launch_comp_shapes_g(a, e))
+        launch_comp_shapes_g(a, e) || launch_comp_shapes_h(a, e))
         return e;
     return cudaErrorInvalidValue;
 }
@@ -107,7 +107,9 @@ bool comp_table_needs_clamp(float inv_ds, const LutMetaF &m)
 // with less padding (measured: N = 192, 384, 768 18-27 % faster than the next power of two).
 // Fewer lanes per chain with more segments each (8 x {20, 24}, 16 x {20, 24, 28}) put two or
 // four chains in a warp and measured 13-32 % faster than the 16- and 32-lane shapes padded to
-// the same N (N = 160, 192, 320, 384, 448); 16 x 32 at N = 512 measured only 2 % above 32 x 16
+// the same N (N = 160, 192, 320, 384, 448), 4 x 20 11 % above 8 x 12 at N = 80 (4 x 24, 4 x 28
+// within 1 % of 8 x 12 / 8 x 16 at N = 96, 112; 4 x 32 below 8 x 16 at 128); 16 x 32 at N = 512
+// measured only 2 % above 32 x 16
 // and would drop to 12 warps through L1 for large tables, so 32 x 16 stays. The 24-segment
 // shapes run 24 warps, which leave no room to stage a table: they stage one at 20 warps when
 // that fits (comp_stage_min_warps) and gather it through L1 at 24 otherwise; 16 x 28 likewise
@@ -133,6 +135,7 @@ CompTuning comp_default_tuning(uint32_t n)
     else if (n <= 64) { t.group = 4; t.spl = 16; t.warps_per_block = 24; }
     else if (n <= 68) { t.group = 4; t.spl = 17; t.warps_per_block = 24; }
     else if (n <= 72) { t.group = 8; t.spl = 9; t.warps_per_block = 32; }
+    else if (n <= 80) { t.group = 4; t.spl = 20; t.warps_per_block = 24; }
     else if (n <= 96) { t.group = 8; t.spl = 12; t.warps_per_block = 24; }
     else if (n <= 128) { t.group = 8; t.spl = 16; t.warps_per_block = 24; }
     else if (n <= 136) { t.group = 8; t.spl = 17; t.warps_per_block = 24; }
@@ -169,7 +172,8 @@ bool comp_tuning_supported(const CompTuning &t, uint32_t n, uint32_t k_eff)
 {
     const int s = t.spl;
     const bool shape = (t.group == 1 && (s == 8 || s == 12)) ||
-                       (t.group == 4 && (s == 2 || s == 3 || s == 4 || s == 5 || s == 8 || s == 9 || s == 16 || s == 17)) ||
+                       (t.group == 4 && (s == 2 || s == 3 || s == 4 || s == 5 || s == 8 || s == 9 || s == 16 || s == 17 || s == 20 ||
+                                         s == 24 || s == 28 || s == 32)) ||
                        (t.group == 8 && (s == 2 || s == 4 || s == 8 || s == 9 || s == 12 || s == 16 || s == 17 || s == 20 ||
                                          s == 24 || s == 32)) ||
                        (t.group == 16 && (s == 4 || s == 8 || s == 12 || s == 16 || s == 17 || s == 20 || s == 24 ||

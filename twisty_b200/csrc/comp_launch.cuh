@@ -1,5 +1,5 @@
 // comp_launch.cuh -- the compensated chain kernel and its per-shape launcher, included by the
-// translation units that instantiate it (comp_shapes_{a..f}.cu, a few shapes each, so that the
+// translation units that instantiate it (comp_shapes_{a..h}.cu, a few shapes each, so that the
 // many template variants compile in parallel) and by chain_comp.cu, which dispatches to them.
 #pragma once
 #include "comp_body.cuh"
@@ -31,6 +31,7 @@ bool launch_comp_shapes_d(const CompLaunch &a, cudaError_t &e);   // 32 x {4, 8,
 bool launch_comp_shapes_e(const CompLaunch &a, cudaError_t &e);   // 32 x {16, 24, 32}
 bool launch_comp_shapes_f(const CompLaunch &a, cudaError_t &e);   // 16 x 20, 32 x {20, 28}
 bool launch_comp_shapes_g(const CompLaunch &a, cudaError_t &e);   // 8 x {20, 24}, 16 x {24, 28, 32}
+bool launch_comp_shapes_h(const CompLaunch &a, cudaError_t &e);   // 4 x {20, 24, 28, 32}
 
 namespace {
 
