@@ -38,3 +38,21 @@ def test_autotune_rejects_other_forms():
     with T.Context(_params(100, form=T.FORM_PLAIN_FP32)) as ctx:
         with pytest.raises(T.TwistyError):
             ctx.autotune(bc, 1 << 16)
+
+
+def test_batch_keeps_the_default_for_a_tuned_shape_it_has_no_kernel_for(tmp_path):
+    """A tuning-cache entry for a single-run-only shape (8 x 32) is used by single runs of its
+    N and table size; batched runs of that N keep the default shape instead of failing."""
+    import torch
+    N, bins, paths = 222, 768, 1 << 14
+    f = tmp_path / "tune.json"
+    f.write_text('{"entries": [{"device": "%s", "n": %d, "bins": %d, "group": 8, "spl": 32, "warps": 16, '
+                 '"path_segments_per_s": 1.0}]}' % (torch.cuda.get_device_name(0), N, bins))
+    T.tuning_cache_load(str(f))
+    bc = T.make_bc((0, 0, 0), (0, 0, 1), (0, 0, 15), (0, 0, 1), 30.0)
+    with T.Context(_params(N, num_curvature_steps=bins, paths_to_generate=paths)) as ctx:
+        res = ctx.run_batch([T.make_experiment(bc, N, 10.0, 0.01, paths)])
+        r = ctx.run(bc)
+    assert len(res) == 1 and res[0].total_paths == paths and res[0].failed_paths == 0
+    assert math.isfinite(res[0].log10_weight)
+    assert r.total_paths == paths and r.failed_paths == 0 and math.isfinite(r.log10_weight)

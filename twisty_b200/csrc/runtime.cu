@@ -1276,7 +1276,14 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
         n_seg_floats += 3 * N;
         // kernel shape and chain layout: whole CTAs of chains, ~2048 steps per chain
         h.t = comp_default_tuning(N);
-        tune_lookup(ctx->device_name, N, bins, h.t);
+        {
+            // a tuned shape the batched kernel does not have keeps the default
+            CompTuning tuned = h.t;
+            if (tune_lookup(ctx->device_name, N, bins, tuned)) {
+                const int w = std::min(tuned.warps_per_block, batch_max_threads(tuned.group, tuned.spl) / 32);
+                if (batch_shape_supported(BatchShape{tuned.group, tuned.spl, w, 0, 1, 0, 0}, N, 2)) h.t = tuned;
+            }
+        }
         ChainSpec &c = h.spec;
         c = ChainSpec{};
         c.n_segments = N;
