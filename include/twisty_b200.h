@@ -120,7 +120,10 @@ typedef struct twisty_params {
     twisty_vec3 eval_end_shift;  /* weights evaluated with the receiver moved by this vector,
                                     the chain itself unchanged (finite-difference checks) */
     /* compensated-form kernel shape; 0 = chosen from N. comp_group lanes per chain (1, 4, 8, 16,
-       32) x comp_spl segments per lane (>= N in total), comp_warps warps per CTA. */
+       32) x comp_spl segments per lane (>= N in total), comp_warps warps per CTA. Shapes:
+       1 x {8, 12}; 4 x {2, 3, 4, 5, 8, 9, 16, 17, 20, 24, 28, 32}; 8 x {2, 4, 8, 9, 12, 16, 17, 20,
+       24, 32}; 16 x {4, 8, 12, 16, 17, 20, 24, 28, 32}; 32 x {4, 8, 12, 16, 17, 20, 24, 28, 32}
+       (batched runs: all but 8 x 32). */
     uint32_t comp_group;
     uint32_t comp_spl;
     uint32_t comp_warps;

@@ -118,7 +118,7 @@ struct LogFixed {
     int32_t steep;           // bins whose secant slope is NaN (paths crossing them are re-weighed exactly)
 };
 struct CompTuning {
-    int group;               // lanes per chain (4, 8, 16, 32)
+    int group;               // lanes per chain (1, 4, 8, 16, 32)
     int spl;                 // segments per lane
     int warps_per_block;
     int exact_blend;         // 1: interpolate the linear table and take log2 (MUFU)
