@@ -329,6 +329,22 @@ twisty_status twisty_autotune(twisty_ctx *ctx, const twisty_bc *bc, uint64_t tri
 twisty_status twisty_tuning_cache_save(const char *path);
 twisty_status twisty_tuning_cache_load(const char *path);
 
+/* No counterpart in the reference. The kernel shape and table placement that a compensated
+ * forward pass of num_segments segments with a bins-bin weight table takes when the shape
+ * knobs are zero, comp_table_memory is 0 and the tuning cache has no entry for them
+ * (comp_default_tuning and the placement rule of twisty_run). Host-only: needs no device.
+ * TWISTY_ERR_INVALID_ARGUMENT for a null out, N < 4 or bins < 2; TWISTY_ERR_UNSUPPORTED
+ * when no shape covers N (N > 1024). */
+typedef struct twisty_shape {
+    uint32_t group;         /* lanes per chain */
+    uint32_t spl;           /* segments per lane */
+    uint32_t warps;         /* warps per CTA */
+    uint32_t table_in_l1;   /* 1: the table is gathered through L1; 0: staged in shared memory */
+    uint32_t smem_bytes;    /* dynamic shared memory per CTA */
+    uint32_t batched;       /* 1: twisty_run_batch has a kernel of this shape */
+} twisty_shape;
+twisty_status twisty_default_shape(uint32_t num_segments, uint32_t bins, twisty_shape *out);
+
 /* ------------------------------------------------------- allocation-free pass */
 /* No counterpart in the reference. For callers that cannot allocate device memory when
  * they run a pass: an application whose own caching allocator holds nearly all of the

@@ -194,3 +194,29 @@ def test_reference_bootstrapper_refuses_other_n():
     pos = T.bootstrap_curve(T.default_params(num_segments=64, bootstrap_kind=0), bc)   # auto: the arc
     seg = np.linalg.norm(np.diff(pos.astype(np.float64), axis=0), axis=1)
     assert np.allclose(seg, 10.0 / 64, rtol=1e-5)
+
+
+def test_default_shape_covers_every_n_and_table_size():
+    """twisty_default_shape (host-only): every N from 4 to 1024 has a shape that covers it, fits
+    in shared memory with its table staged or through L1, and has a batched kernel; tables of up
+    to 4096 bins are staged, 100000-bin tables go through L1."""
+    import twisty_b200 as T
+    for bins in (256, 2048, 4096, 8192, 20000, 100000):
+        for n in range(4, 1025):
+            s = T.default_shape(n, bins)
+            assert s["group"] * s["spl"] >= n, (n, bins, s)
+            assert 1 <= s["warps"] and s["warps"] * 32 <= 1024, (n, bins, s)
+            assert s["smem_bytes"] <= 227 * 1024, (n, bins, s)
+            assert s["batched"] == 1, (n, bins, s)
+            if bins <= 4096:
+                assert s["table_in_l1"] == 0, (n, bins, s)
+            if bins == 100000:
+                assert s["table_in_l1"] == 1, (n, bins, s)
+    # the benchmark's shape, and a shape that stages below its full warps
+    s = T.default_shape(256, 8192)
+    assert (s["group"], s["spl"], s["warps"], s["table_in_l1"]) == (16, 16, 24, 0)
+    assert (T.default_shape(768, 4096)["warps"], T.default_shape(768, 4096)["table_in_l1"]) == (20, 0)
+    assert (T.default_shape(768, 20000)["warps"], T.default_shape(768, 20000)["table_in_l1"]) == (24, 1)
+    for n, bins in ((3, 4096), (1025, 4096), (256, 1)):
+        with pytest.raises(T.TwistyError):
+            T.default_shape(n, bins)

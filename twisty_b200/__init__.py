@@ -231,6 +231,14 @@ def tuning_cache_load(path: str):
     _check(_lib().twisty_tuning_cache_load(path.encode()))
 
 
+def default_shape(num_segments: int, bins: int) -> dict:
+    """The kernel shape and table placement a compensated forward pass of N segments with a
+    bins-bin table takes with the shape knobs at zero (twisty_default_shape; no device needed)."""
+    s = _abi.Shape()
+    _check(_lib().twisty_default_shape(int(num_segments), int(bins), C.byref(s)))
+    return {k: int(getattr(s, k)) for k, _ in _abi.Shape._fields_}
+
+
 def bootstrap_curve(params: _abi.Params, bc: _abi.BC) -> np.ndarray:
     pos = np.zeros((params.num_segments + 1, 3), np.float32)
     _check(_lib().twisty_bootstrap_curve(C.byref(params), C.byref(bc), _fptr(pos)))

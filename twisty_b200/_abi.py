@@ -138,6 +138,12 @@ class NoAllocResult(C.Structure):
                 ("valid_paths", C.c_uint64), ("failed_paths", C.c_uint64), ("clamped_curvatures", C.c_uint64)]
 
 
+class Shape(C.Structure):
+    """twisty_shape: a kernel shape and its table placement."""
+    _fields_ = [("group", C.c_uint32), ("spl", C.c_uint32), ("warps", C.c_uint32), ("table_in_l1", C.c_uint32),
+                ("smem_bytes", C.c_uint32), ("batched", C.c_uint32)]
+
+
 # (name, restype, argtypes): every entry point declared in include/twisty_b200.h
 _P = C.c_void_p
 SIGNATURES = [
@@ -171,6 +177,7 @@ SIGNATURES = [
     ("twisty_multi_ds_tables", C.c_int, [_P, C.c_float, C.c_float, C.c_uint32, C.c_char_p]),
     ("twisty_tuning_cache_save", C.c_int, [C.c_char_p]),
     ("twisty_tuning_cache_load", C.c_int, [C.c_char_p]),
+    ("twisty_default_shape", C.c_int, [C.c_uint32, C.c_uint32, C.POINTER(Shape)]),
 ]
 
 _lib = None

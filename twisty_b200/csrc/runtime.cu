@@ -432,6 +432,21 @@ void fit_table_smem(CompTuning &t, uint32_t bins, bool may_shrink)
         fail(TWISTY_ERR_UNSUPPORTED, "weight table too large to stage in shared memory");
 }
 
+// Forward passes of the full recompute: whether the table goes through L1. A table too large
+// to stage beside the chain state costs warps per CTA; when staging it would leave fewer than
+// comp_stage_min_warps (normally all of the shape's warps), it is gathered through L1 at the
+// shape's warps instead (measured on B200: L1 at full occupancy 0-9 % below a staged table at
+// full occupancy, and from even with one at 5/6 of the warps to +14 % at 2/3 and +40 % and more
+// at 1/4 to 1/2). may_shrink false: the warps were set by the caller.
+bool table_through_l1(const CompTuning &t, uint32_t bins, bool may_shrink)
+{
+    CompTuning staged = t;
+    staged.lut_global = 0;
+    while (may_shrink && staged.warps_per_block > 4 && comp_smem_bytes(staged, bins) > kSmemCap)
+        staged.warps_per_block -= 4;
+    return comp_smem_bytes(staged, bins) > kSmemCap || staged.warps_per_block < comp_stage_min_warps(t);
+}
+
 // The context's shape for the passes that stage the table (export, adjoint).
 CompTuning staged_tuning(const twisty_ctx *ctx)
 {
@@ -504,21 +519,11 @@ void prepare(twisty_ctx *ctx, const twisty_bc *bcp)
         if (p.comp_warps) ctx->tuning.warps_per_block = (int)p.comp_warps;
         ctx->tuning.exact_blend = ctx->exact_blend;
         if (!comp_tuning_supported(ctx->tuning, N, c.k_eff)) fail(TWISTY_ERR_UNSUPPORTED, "no compensated kernel shape for this N / max_sub_chain");
-        // A table too large to stage beside the chain state costs warps per CTA; when staging it
-        // would leave fewer than the shape's warps, forward passes of the full recompute read it
-        // through L1 instead (measured on B200: L1 at full occupancy 0-9 % below a staged table
-        // at full occupancy, and from even with one at 5/6 of the warps to +14 % at 2/3 and +40 %
-        // and more at 1/4 to 1/2). comp_table_memory 1 / 2 force the choice.
+        // the table's placement (table_through_l1); comp_table_memory 1 / 2 force the choice
         ctx->tuning.lut_global = 0;
         const bool can_global = c.incr_resync <= 1 && !c.has_eval_shift;
-        bool few_warps = false;
-        if (p.comp_table_memory == 0 && can_global) {
-            CompTuning staged = ctx->tuning;
-            while (!p.comp_warps && staged.warps_per_block > 4 && comp_smem_bytes(staged, p.num_curvature_steps) > kSmemCap)
-                staged.warps_per_block -= 4;
-            few_warps = comp_smem_bytes(staged, p.num_curvature_steps) > kSmemCap ||
-                        staged.warps_per_block < comp_stage_min_warps(ctx->tuning);
-        }
+        const bool few_warps = p.comp_table_memory == 0 && can_global &&
+                               table_through_l1(ctx->tuning, p.num_curvature_steps, p.comp_warps == 0);
         if (p.comp_table_memory == 2 || few_warps) {
             if (!can_global)
                 fail(TWISTY_ERR_UNSUPPORTED, "comp_table_memory 2 serves plain forward passes (no incremental or shifted runs)");
@@ -1772,6 +1777,36 @@ twisty_status twisty_autotune(twisty_ctx *ctx, const twisty_bc *bc, uint64_t tri
         best->warps = (uint32_t)bestc.warps;
         best->path_segments_per_s = best_rate;
     });
+}
+
+twisty_status twisty_default_shape(uint32_t num_segments, uint32_t bins, twisty_shape *out)
+{
+    if (!out || num_segments < 4 || bins < 2) {
+        g_free_err = "twisty_default_shape: null out, N < 4 or bins < 2";
+        return TWISTY_ERR_INVALID_ARGUMENT;
+    }
+    CompTuning t = comp_default_tuning(num_segments);
+    if (!comp_tuning_supported(t, num_segments, 2)) {
+        g_free_err = "no compensated kernel shape for this N";
+        return TWISTY_ERR_UNSUPPORTED;
+    }
+    if (table_through_l1(t, bins, true)) {
+        t.lut_global = 1;
+    } else {
+        while (t.warps_per_block > 4 && comp_smem_bytes(t, bins) > kSmemCap) t.warps_per_block -= 4;
+    }
+    if (comp_smem_bytes(t, bins) > kSmemCap) {
+        g_free_err = "chain state does not fit in shared memory";
+        return TWISTY_ERR_UNSUPPORTED;
+    }
+    const int bw = std::min(t.warps_per_block, batch_max_threads(t.group, t.spl) / 32);
+    out->group = (uint32_t)t.group;
+    out->spl = (uint32_t)t.spl;
+    out->warps = (uint32_t)t.warps_per_block;
+    out->table_in_l1 = (uint32_t)t.lut_global;
+    out->smem_bytes = (uint32_t)comp_smem_bytes(t, bins);
+    out->batched = batch_shape_supported(BatchShape{t.group, t.spl, bw, 0, 1, 0, 0}, num_segments, 2) ? 1u : 0u;
+    return TWISTY_OK;
 }
 
 twisty_status twisty_tuning_cache_save(const char *path)
