@@ -362,8 +362,15 @@ twisty_status twisty_default_shape(uint32_t num_segments, uint32_t bins, twisty_
  * scratch array; make that first call before any stream capture on the device. Every
  * call writes each scratch entry it later reads, so nothing carries over between calls,
  * but all calls share the one array: calls that overlap on the GPU (concurrent streams,
- * threads) race on it and must be ordered by the caller. */
+ * threads) race on it and must be ordered by the caller. The looked-up address lives as long
+ * as the device's context: do not call this entry point again after cudaDeviceReset in the
+ * same process.
+ *
+ * The kernel shape and table placement are twisty_run's defaults for N and bins
+ * (twisty_default_shape): the table is staged in shared memory when it fits beside the
+ * chain state, else gathered through L1. bins is at most TWISTY_NOALLOC_MAX_BINS. */
 #define TWISTY_NOALLOC_MAX_CHAINS 16384u
+#define TWISTY_NOALLOC_MAX_BINS (1u << 24)
 
 typedef struct twisty_noalloc_args {
     const void *table;           /* device float2[bins]: (L_i, L_{i+1} - L_i); last (L_{bins-1}, 0) */

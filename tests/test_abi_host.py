@@ -37,10 +37,9 @@ def test_library_exports_every_declared_symbol():
     assert sorted(n for n, _, _ in _abi.SIGNATURES) == names
 
 
-def test_struct_sizes_match_header():
+def test_struct_sizes_match_header(tmp_path):
     # compile a probe against the header and compare struct sizes with the ctypes mirror
-    src = os.path.join(ROOT, "_work", "abi_probe.c")
-    os.makedirs(os.path.dirname(src), exist_ok=True)
+    src = str(tmp_path / "abi_probe.c")
     with open(src, "w") as f:
         f.write('#include "twisty_b200.h"\n#include <stdio.h>\n#include <stddef.h>\n'
                 'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(twisty_params), sizeof(twisty_bc),'
@@ -220,3 +219,13 @@ def test_default_shape_covers_every_n_and_table_size():
     for n, bins in ((3, 4096), (1025, 4096), (256, 1)):
         with pytest.raises(T.TwistyError):
             T.default_shape(n, bins)
+
+
+def test_benchmark_curve_fixture_is_the_bootstrappers():
+    """bench.py's reference arm reads the N = 256 initial curve of the precision workload from a
+    committed fixture (so that it never loads this library); it must be the curve this library's
+    bootstrapper gives for that workload (arc bootstrapper, bootstrap seed 7)."""
+    import bench
+    pos = T.bootstrap_curve(T.default_params(num_segments=256, bootstrap_seed=7), bench.workload_bc(T))
+    fix = np.load(bench.BENCH_CURVE)
+    assert np.array_equal(pos.view(np.uint32), fix.view(np.uint32))

@@ -121,6 +121,7 @@ class Tuning(C.Structure):
 
 
 NOALLOC_MAX_CHAINS = 16384
+NOALLOC_MAX_BINS = 1 << 24
 
 
 class NoAllocArgs(C.Structure):

@@ -130,6 +130,16 @@ int comp_stage_min_warps(const CompTuning &t);
 bool comp_tuning_supported(const CompTuning &t, uint32_t n_segments, uint32_t k_eff);
 uint32_t comp_default_chains(uint32_t n_segments, int sm_count);
 size_t comp_smem_bytes(const CompTuning &t, uint32_t bins);
+// Shared memory a CTA may use (B200: 227 KB).
+constexpr size_t kCompSmemCap = 227 * 1024;
+// Table placement of a forward pass of the full recompute: true when the table is gathered
+// through L1 at the shape's warps, because staging it would leave fewer than
+// comp_stage_min_warps(t) warps (or does not fit at all). may_shrink false: the warps were set
+// by the caller and stay.
+bool comp_table_through_l1(const CompTuning &t, uint32_t bins, bool may_shrink);
+// Fewer warps per CTA (steps of 4, down to 4) until the chain state, and the table when it is
+// staged (t.lut_global = 0), fit in shared memory; false when they do not fit even then.
+bool comp_fit_smem(CompTuning &t, uint32_t bins, bool may_shrink);
 cudaError_t launch_comp_chains(const ChainSpec &c, const CompTuning &t, const float *init_seg,
                                const float2 *fixtab, const float2 *lintab, LutMetaF m,
                                ChainOut *out, double2 *block_partials, cudaStream_t st,

@@ -55,7 +55,10 @@ extern "C" twisty_status twisty_run_noalloc(const twisty_noalloc_args *a, void *
     if (!a) return bad("args is NULL");
     if (!a->table || !a->init_segments || !a->result) return bad("table, init_segments and result must be device pointers");
     if (a->num_segments < 4 || a->num_segments > 1024) return bad("num_segments must be in [4, 1024]");
-    if (a->bins < 2 || !(a->curvature_step > 0.0f) || !(a->max_curvature > a->min_curvature))
+    // the cap comes first: the size arithmetic below (shared-memory bytes, the signed bin count
+    // the kernel clamps to) must not wrap
+    if (a->bins < 2 || a->bins > TWISTY_NOALLOC_MAX_BINS) return bad("bins must be in [2, TWISTY_NOALLOC_MAX_BINS = 2^24]");
+    if (!(a->curvature_step > 0.0f) || !(a->max_curvature > a->min_curvature))
         return bad("table metadata is invalid");
     if (a->num_chains == 0 || a->num_chains > TWISTY_NOALLOC_MAX_CHAINS)
         return bad("num_chains must be in [1, TWISTY_NOALLOC_MAX_CHAINS = 16384]: the fixed scratch holds 16384 chains");
@@ -68,7 +71,8 @@ extern "C" twisty_status twisty_run_noalloc(const twisty_noalloc_args *a, void *
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     if (dev < 0 || dev >= kMaxDevices) return bad("device ordinal beyond the supported range");
-    // Set-up, once per device, with that device current.
+    // Set-up, once per device, with that device current. The address stays valid for the life of
+    // the device's primary context; after cudaDeviceReset it is stale (documented in the header).
     void *scratch = g_scratch_addr[dev].load(std::memory_order_acquire);
     if (!scratch) {
         e = cudaGetSymbolAddress(&scratch, g_noalloc_chains);
@@ -97,10 +101,13 @@ extern "C" twisty_status twisty_run_noalloc(const twisty_noalloc_args *a, void *
     c.absorption_factor = (double)std::exp(-a->absorption * c.ds);
     c.has_eval_shift = 0;
 
+    // the default shape and table placement of twisty_run's forward pass (shared memory when the
+    // table fits beside the shape's chain state, else gathered through L1)
     CompTuning t = comp_default_tuning(N);
     t.exact_blend = 1;  // the table is the linear (L_i, L_{i+1} - L_i) form
     if (!comp_tuning_supported(t, N, c.k_eff)) return bad("no compensated kernel shape for this N");
-    if (comp_smem_bytes(t, a->bins) > 227 * 1024) return bad("table too large to stage in shared memory");
+    t.lut_global = comp_table_through_l1(t, a->bins, true) ? 1 : 0;
+    if (!comp_fit_smem(t, a->bins, true)) return bad("the chain state of this N does not fit in shared memory");
     const LutMetaF m{a->min_curvature, a->max_curvature, a->curvature_step, (int32_t)a->bins};
     cudaStream_t st = (cudaStream_t)stream;
     e = launch_comp_chains(c, t, a->init_segments, static_cast<const float2 *>(a->table),

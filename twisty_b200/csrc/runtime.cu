@@ -421,30 +421,22 @@ void layout(twisty_ctx *ctx, uint64_t paths, uint32_t requested, uint32_t max_st
     c.last_steps = (uint32_t)(paths - (C - 1) * L);
 }
 
-constexpr size_t kSmemCap = 227 * 1024;
+constexpr size_t kSmemCap = kCompSmemCap;
 
 // Fewer warps per CTA until the table (when staged) and the chain state fit in shared memory;
 // fails when even 4 warps do not fit.
 void fit_table_smem(CompTuning &t, uint32_t bins, bool may_shrink)
 {
-    while (may_shrink && t.warps_per_block > 4 && comp_smem_bytes(t, bins) > kSmemCap) t.warps_per_block -= 4;
-    if (comp_smem_bytes(t, bins) > kSmemCap)
-        fail(TWISTY_ERR_UNSUPPORTED, "weight table too large to stage in shared memory");
+    if (!comp_fit_smem(t, bins, may_shrink)) fail(TWISTY_ERR_UNSUPPORTED, "weight table too large to stage in shared memory");
 }
 
 // Forward passes of the full recompute: whether the table goes through L1. A table too large
 // to stage beside the chain state costs warps per CTA; when staging it would leave fewer than
 // comp_stage_min_warps (normally all of the shape's warps), it is gathered through L1 at the
-// shape's warps instead (measured on B200: L1 at full occupancy 0-9 % below a staged table at
-// full occupancy, and from even with one at 5/6 of the warps to +14 % at 2/3 and +40 % and more
-// at 1/4 to 1/2). may_shrink false: the warps were set by the caller.
+// shape's warps instead. may_shrink false: the warps were set by the caller.
 bool table_through_l1(const CompTuning &t, uint32_t bins, bool may_shrink)
 {
-    CompTuning staged = t;
-    staged.lut_global = 0;
-    while (may_shrink && staged.warps_per_block > 4 && comp_smem_bytes(staged, bins) > kSmemCap)
-        staged.warps_per_block -= 4;
-    return comp_smem_bytes(staged, bins) > kSmemCap || staged.warps_per_block < comp_stage_min_warps(t);
+    return comp_table_through_l1(t, bins, may_shrink);
 }
 
 // The context's shape for the passes that stage the table (export, adjoint).
@@ -1790,12 +1782,8 @@ twisty_status twisty_default_shape(uint32_t num_segments, uint32_t bins, twisty_
         g_free_err = "no compensated kernel shape for this N";
         return TWISTY_ERR_UNSUPPORTED;
     }
-    if (table_through_l1(t, bins, true)) {
-        t.lut_global = 1;
-    } else {
-        while (t.warps_per_block > 4 && comp_smem_bytes(t, bins) > kSmemCap) t.warps_per_block -= 4;
-    }
-    if (comp_smem_bytes(t, bins) > kSmemCap) {
+    t.lut_global = table_through_l1(t, bins, true) ? 1 : 0;
+    if (!comp_fit_smem(t, bins, true)) {
         g_free_err = "chain state does not fit in shared memory";
         return TWISTY_ERR_UNSUPPORTED;
     }

@@ -9,7 +9,7 @@ receivers, rebuilt as one batched pass (twisty_run_batch) each.
   sphere of radius sphereRadius around the source, the direction drawn as the reference draws
   it from std::mt19937(targetSeed) with std::uniform_real_distribution<float> (the same
   stream: the first receiver is the reference's). The reference hands RunExperiment boundary
-  conditions without an arclength (:269, SURVEY note); here arclength_scale times the minimum
+  conditions without an arclength (:269); here arclength_scale times the minimum
   arclength (CalculateMinimumArclength, Twisty/PathGeneration.cpp:12-43) is used.
 * ``image_plane_experiments`` -- the pixel loop of the image drivers
   (Experiments/NoisyCircleExperiment.cpp:259-361): a grid of receivers on a plane, one
