@@ -40,6 +40,11 @@ class LutMeta64(C.Structure):
                 ("bins", C.c_uint32), ("pad", C.c_uint32)]
 
 
+class ChainOpts(C.Structure):
+    _fields_ = [("has_shift", C.c_int), ("eval_shift", C.c_double * 3), ("ref_log10", C.c_double),
+                ("grad_chains", C.c_void_p)]
+
+
 class CW(C.Structure):
     _fields_ = [("max_log10", C.c_double), ("total", C.c_double), ("offset", C.c_double),
                 ("n", C.c_uint32), ("pad", C.c_uint32)]
@@ -98,6 +103,10 @@ def lib() -> C.CDLL:
                                          C.c_uint32, C.c_uint32, C.c_uint32, C.c_float,
                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_int]
+        L.tor_run_chains_f64_opts.argtypes = [f32p, C.c_uint32, C.c_double, f64p, C.POINTER(LutMeta64),
+                                              C.c_double, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32,
+                                              C.c_uint32, C.c_uint32, C.c_uint32, C.c_float,
+                                              C.c_void_p, C.c_void_p, C.POINTER(ChainOpts), C.c_int]
         _lib = L
     return _lib
 
@@ -223,3 +232,78 @@ def run_chains(init_pos, n_segments, arclength, lut, meta, *, seed, n_chains, st
         raise ValueError("invalid chain parameters")
     return {"path_log10": pl, "path_valid": pv, "chain_log10": cl, "chain_valid": cv,
             "final_pos": fp}
+
+
+def run_chains_f64_opts(init_pos, n_segments, arclength, lut, meta, *, seed, n_chains, steps, burn_in=0, k_max=25,
+                        max_angle=float(np.float32(np.pi)), experiment=0, chain0=0, absorption=0.0,
+                        eval_shift=None, grad_ref_log10=None, threads=os.cpu_count() or 1):
+    """FP64 twin chains with the receiver moved when weighing (eval_shift) and/or the pathwise
+    receiver gradient (grad_ref_log10: the reference the path weights are scaled by).
+    Returns log10 of the summed weights and, with a gradient, d log10 W / d receiver (3)."""
+    init_pos = np.ascontiguousarray(init_pos, np.float32).reshape(-1)
+    cl = np.zeros(n_chains, np.float64)
+    cv = np.zeros(n_chains, np.uint64)
+    o = ChainOpts()
+    if eval_shift is not None:
+        o.has_shift = 1
+        for q in range(3):
+            o.eval_shift[q] = float(eval_shift[q])
+    g = None
+    if grad_ref_log10 is not None:
+        g = np.zeros((n_chains, 4), np.float64)
+        o.ref_log10 = float(grad_ref_log10)
+        o.grad_chains = g.ctypes.data_as(C.c_void_p).value
+    rc = lib().tor_run_chains_f64_opts(init_pos, n_segments, arclength, lut, C.byref(meta), absorption, seed,
+                                       experiment, chain0, n_chains, steps, burn_in, k_max, max_angle,
+                                       _ptr(cl), _ptr(cv), C.byref(o), threads)
+    if rc != 0:
+        raise ValueError("invalid chain parameters")
+    out = {"log10": log10_sum(cl), "valid": int(cv.sum())}
+    if g is not None:
+        tot = g.sum(axis=0)
+        out["grad_receiver"] = tot[:3] / tot[3]
+    return out
+
+
+def fd_gradient_f64(init_pos, n_segments, arclength, mu, eps, scatter, absorption, num_steps_int, bins, *, seed,
+                    n_chains, steps, burn_in, k_max, max_angle, h=1e-3, h_receiver=None, richardson=True,
+                    threads=os.cpu_count() or 1):
+    """FP64 CPU central finite differences of log10 experimentWeight with respect to
+    (mu_s, sigma, receiver x, y, z): the FP64 twin of the reference's table build
+    (PathWeightUtils.cpp:281-433, maxBound = 10/eps) and weigher (PathWeighters.cpp:27-104)
+    re-run with common random numbers (the same Philox proposals). mu_s and sigma = sqrt(eps)
+    move by h relative; the receiver by h_receiver (absolute) along each axis, the chain held.
+    With richardson, each difference is extrapolated from steps h and 2h,
+    (4 D(h) - D(2h)) / 3, which cancels the O(h^2) term of the central difference."""
+    ds = float(np.float32(arclength) / np.float32(n_segments))
+
+    def table(mus, e):
+        wp = wparams(mu, e, mus, absorption, num_steps_int, bins)
+        return lut_f64(wp, ds, threads)
+
+    def run(tab, shift=None):
+        lut, meta = tab
+        return run_chains_f64_opts(init_pos, n_segments, arclength, lut, meta, seed=seed, n_chains=n_chains,
+                                   steps=steps, burn_in=burn_in, k_max=k_max, max_angle=max_angle,
+                                   absorption=absorption, eval_shift=shift, threads=threads)["log10"]
+
+    def central(f, x, step):
+        d1 = (f(x + step) - f(x - step)) / (2 * step)
+        if not richardson:
+            return d1
+        d2 = (f(x + 2 * step) - f(x - 2 * step)) / (4 * step)
+        return (4 * d1 - d2) / 3
+
+    sigma = float(np.sqrt(np.float64(np.float32(eps))))
+    base = table(scatter, eps)
+    g_mu = central(lambda m: run(table(float(np.float32(m)), eps)), scatter, h * scatter)
+    g_sig = central(lambda sg: run(table(scatter, float(np.float32(sg) * np.float32(sg)))), sigma, h * sigma)
+    hr = h_receiver if h_receiver is not None else 1e-2 * ds
+    g_rx = []
+    for axis in range(3):
+        def f(t, axis=axis):
+            e = np.zeros(3)
+            e[axis] = t
+            return run(base, e)
+        g_rx.append(central(f, 0.0, hr))
+    return np.array([g_mu, g_sig, *g_rx])

@@ -674,6 +674,7 @@ typedef struct {
     uint64_t *chain_valid;
     float *final32;
     double *final64;
+    const tor_chain_opts *opts;
 } chain_job;
 
 typedef struct {
@@ -745,6 +746,56 @@ static void *chain_worker_f32(void *arg)
     return NULL;
 }
 
+/* d log10 v / d kappa of the FP64 table's segment weight, as the adjoint defines it. The
+ * reference's blend moves within a bin by (L_{b+1} - L_b) per unit of curvature (its
+ * interpolation weight is in curvature units, PathWeighters.cpp:79-82) and jumps by nearly
+ * L_{b+1} - L_b at every bin edge, so its pathwise derivative misses almost all of the change
+ * that an expectation over paths sees. The adjoint takes the slope of the expected weight
+ * instead: averaged over a bin, the staircase equals the linear interpolant of the table taken
+ * half a bin to the left, whose slope at kappa is (L_{j+1} - L_j) / step with
+ * j = floor(kappa / step - 1/2); divided by the weight itself. Clamped curvatures are flat. */
+static double dlog10_dkappa_f64(double kappa, const double *lut, const tor_lut_meta64 *m)
+{
+    if (!(kappa >= m->min_k) || kappa > m->max_k) return 0.0;
+    const int32_t size = (int32_t)m->bins;
+    const double dist = kappa - m->min_k;
+    int32_t left = (int32_t)floor(dist / m->step);
+    if (left > size - 1) left = size - 1;
+    const int32_t right = left == size - 1 ? left : left + 1;
+    const double interp = dist - (double)left * m->step;
+    const double v = lut[left] * (1.0 - interp) + lut[right] * interp;
+    int32_t jl = (int32_t)floor(dist / m->step - 0.5);
+    if (jl < 0) jl = 0;
+    if (jl > size - 2) jl = size - 2;
+    return (lut[jl + 1] - lut[jl]) / m->step / (v * M_LN10);
+}
+
+/* Receiver-position gradient of one path's log10 weight (FP64): moving points N-1 and N
+ * together changes only the segment vector v_{N-2}, hence t_{N-2} and the curvatures
+ * kappa_{N-3} = |t_{N-2} - t_{N-3}| N/S and kappa_{N-2} = |t_{N-1} - t_{N-2}| N/S. */
+static void receiver_grad_f64(const double *pos, const double *tan, const double *cv, uint32_t n, double arclength,
+                              const double *lut, const tor_lut_meta64 *m, double g[3])
+{
+    const double inv_ds = (double)n / arclength;
+    const double *t3 = tan + 3 * (n - 3), *t2 = tan + 3 * (n - 2), *t1 = tan + 3 * (n - 1);
+    const double vx = pos[3 * (n - 1)] - pos[3 * (n - 2)], vy = pos[3 * (n - 1) + 1] - pos[3 * (n - 2) + 1],
+                 vz = pos[3 * (n - 1) + 2] - pos[3 * (n - 2) + 2];
+    const double len2 = sqrt(vx * vx + vy * vy + vz * vz);
+    g[0] = g[1] = g[2] = 0.0;
+    for (int which = 0; which < 2; ++which) {
+        double d[3];
+        double sign;
+        if (which == 0) { for (int q = 0; q < 3; ++q) d[q] = t2[q] - t3[q]; sign = 1.0; }
+        else { for (int q = 0; q < 3; ++q) d[q] = t1[q] - t2[q]; sign = -1.0; }
+        const double dn = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        if (!(dn > 0.0)) continue;
+        const double dl = dlog10_dkappa_f64(cv[n - 3 + which], lut, m);
+        const double dk = dl * inv_ds * sign / dn;
+        const double dt = d[0] * t2[0] + d[1] * t2[1] + d[2] * t2[2];
+        for (int q = 0; q < 3; ++q) g[q] += dk * (d[q] - dt * t2[q]) / len2;
+    }
+}
+
 /* The FP64 twin chain: positions, rotation and weighting in double; the proposal
  * (k, left, angle) is the same Philox draw, its half-angle sine/cosine taken in double. */
 static void *chain_worker_f64(void *arg)
@@ -752,11 +803,15 @@ static void *chain_worker_f64(void *arg)
     chain_job *j = (chain_job *)arg;
     const uint32_t n = j->n;
     double *pos = (double *)malloc(sizeof(double) * 3 * (n + 1));
+    double *pw = (double *)malloc(sizeof(double) * 3 * (n + 1));
     double *tan = (double *)malloc(sizeof(double) * 3 * n);
     double *cv = (double *)malloc(sizeof(double) * (n - 1));
+    const tor_chain_opts *o = j->opts;
+    const int shift = o && o->has_shift;
     for (uint32_t c = j->c0; c < j->c1; ++c) {
         for (uint32_t i = 0; i < 3 * (n + 1); ++i) pos[i] = (double)j->init_pos[i];
         lse_acc acc = {0.0L, 0.0L, 0};
+        long double gacc[4] = {0.0L, 0.0L, 0.0L, 0.0L};
         const uint32_t total = j->burn_in + j->steps;
         for (uint32_t s = 0; s < total; ++s) {
             uint32_t k, left;
@@ -781,7 +836,15 @@ static void *chain_worker_f64(void *arg)
                 pos[3 * i + 2] = r20 * vx + r21 * vy + r22 * vz + lz;
             }
             if (s < j->burn_in) continue;
-            tangents_f64(pos, n, tan);
+            const double *pe = pos;
+            if (shift) {
+                /* the weights see the receiver moved: points N-1 and N shifted, the chain unchanged */
+                memcpy(pw, pos, sizeof(double) * 3 * (n + 1));
+                for (uint32_t i = n - 1; i <= n; ++i)
+                    for (int q = 0; q < 3; ++q) pw[3 * i + q] += o->eval_shift[q];
+                pe = pw;
+            }
+            tangents_f64(pe, n, tan);
             curvatures_f64(tan, n, j->arclength, cv);
             double w = 0.0;
             const int ok = weight_curvatures_f64(cv, n - 1, j->lut64, j->m64, j->absorption, &w, NULL);
@@ -789,12 +852,22 @@ static void *chain_worker_f64(void *arg)
             if (j->path_log10) j->path_log10[pi] = w;
             if (j->path_valid) j->path_valid[pi] = (uint8_t)ok;
             if (ok) lse_add(&acc, w);
+            if (ok && o && o->grad_chains) {
+                double g[3];
+                receiver_grad_f64(pe, tan, cv, n, j->arclength, j->lut64, j->m64, g);
+                const long double wt = powl(10.0L, (long double)w - (long double)o->ref_log10);
+                for (int q = 0; q < 3; ++q) gacc[q] += wt * (long double)g[q];
+                gacc[3] += wt;
+            }
         }
         if (j->chain_log10) j->chain_log10[c] = lse_value(&acc);
         if (j->chain_valid) j->chain_valid[c] = acc.n;
         if (j->final64) memcpy(j->final64 + (uint64_t)c * 3 * (n + 1), pos, sizeof(double) * 3 * (n + 1));
+        if (o && o->grad_chains)
+            for (int q = 0; q < 4; ++q) o->grad_chains[(uint64_t)c * 4 + q] = (double)gacc[q];
     }
     free(pos);
+    free(pw);
     free(tan);
     free(cv);
     return NULL;
@@ -833,6 +906,24 @@ int tor_run_chains_f32(const float *init_pos, uint32_t n_segments, float arcleng
     j.experiment = experiment; j.chain0 = chain0; j.steps = steps; j.burn_in = burn_in;
     j.k_max = k_max; j.max_angle = max_angle; j.path_log10 = path_log10; j.path_valid = path_valid;
     j.chain_log10 = chain_log10; j.chain_valid = chain_valid; j.final32 = final_pos;
+    return run_chains(&j, n_chains, n_threads);
+}
+
+int tor_run_chains_f64_opts(const float *init_pos, uint32_t n_segments, double arclength,
+                            const double *lut, const tor_lut_meta64 *m, double absorption,
+                            uint64_t seed, uint32_t experiment, uint32_t chain0, uint32_t n_chains,
+                            uint32_t steps, uint32_t burn_in, uint32_t k_max, float max_angle,
+                            double *chain_log10, uint64_t *chain_valid, const tor_chain_opts *opts,
+                            int n_threads)
+{
+    if (n_segments < 4) return -1;
+    chain_job j;
+    memset(&j, 0, sizeof(j));
+    j.f64 = 1; j.init_pos = init_pos; j.n = n_segments; j.arclength = arclength;
+    j.lut64 = lut; j.m64 = m; j.absorption = absorption; j.seed = seed;
+    j.experiment = experiment; j.chain0 = chain0; j.steps = steps; j.burn_in = burn_in;
+    j.k_max = k_max; j.max_angle = max_angle;
+    j.chain_log10 = chain_log10; j.chain_valid = chain_valid; j.opts = opts;
     return run_chains(&j, n_chains, n_threads);
 }
 

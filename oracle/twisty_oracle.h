@@ -114,6 +114,29 @@ int tor_run_chains_f64(const float *init_pos, uint32_t n_segments, double arclen
                        double *path_log10, uint8_t *path_valid, double *chain_log10,
                        uint64_t *chain_valid, double *final_pos, int n_threads);
 
+/* The FP64 twin chains with the options of a gradient check:
+ *   has_shift, eval_shift  weights evaluated with the receiver (points N-1 and N) moved by
+ *                          eval_shift, the chain itself unchanged (finite differences of the
+ *                          estimate with respect to the receiver, common random numbers);
+ *   grad_chains            nullable, [n_chains][4]: per chain, the sum over its valid paths of
+ *                          10^(w - ref_log10) d log10 w / d receiver (x, y, z) and of
+ *                          10^(w - ref_log10) -- the pathwise receiver gradient in FP64, with
+ *                          the table slope taken as the slope of the expected segment weight
+ *                          (see dlog10_dkappa_f64). */
+typedef struct {
+    int has_shift;
+    double eval_shift[3];
+    double ref_log10;
+    double *grad_chains;
+} tor_chain_opts;
+
+int tor_run_chains_f64_opts(const float *init_pos, uint32_t n_segments, double arclength,
+                            const double *lut, const tor_lut_meta64 *m, double absorption,
+                            uint64_t seed, uint32_t experiment, uint32_t chain0, uint32_t n_chains,
+                            uint32_t steps, uint32_t burn_in, uint32_t k_max, float max_angle,
+                            double *chain_log10, uint64_t *chain_valid, const tor_chain_opts *opts,
+                            int n_threads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -11,13 +11,23 @@ oracle/_ref/ref_harness:
                    UpdateCurvaturesFromTangents_RadiativeTransfer, WeightCurveViaCurvatureLog10_CudaSafe)
   rotate.npz       RotateVectorByQuaternion on random inputs
   cw.npz           CombinedWeightValues_C add / combine / extract sequences
-  norm.json        log10 Norm(N, ds, bc) for N = 4 (and 5)
+  norm.json        log10 Norm(N, ds, bc) for N = 4, 5 and 6 (the N = 5, 6 records take the
+                   reference's 1e10-term quadrature, about a minute each; `--only norm`)
   boot_*.npy       reference bootstrap curves (ResolveEvenNumberOfSegments)
   chain_*.json     full runs of the reference's Markov-chain loop (GeometryRandom) for the
                    statistical comparison, with per-1e6-path chunk sums
   msegment_*.json  the reference's independent-sample estimator (MSegmentPathGenerationMC's
                    per-path work through its own functions): mean weight and relative SE
                    (`--msegment-only` regenerates just these)
+  lut_D/E, paths_D/E, boot_258, chain_D/E.json
+                   the same fixtures at the configurations the benchmark metric is quoted on
+                   (`--only baseline`): D is the plain-form configuration (N = 66, S = 10,
+                   receiver (8,0,0) along x, 4096-bin table), E the precision-form one (N = 258,
+                   S = 20, receiver (0,0,12) along z, 8192-bin table from a 20000-step rule);
+                   N = 66 and 258 because the reference's bootstrapper resolves only N - 2 in
+                   {4, 6, 8, 12, 16, 24, ...}. Their path batches include chain states under the
+                   benchmark's own proposals (k <= 32, angles within +-0.1 and +-0.05) beside the
+                   reference's (k <= 25, angles in (-pi, pi)).
 The path batches are perturbed with the oracle's chain runner so they cover curved
 configurations; their weights still come from the reference weigher. This script reads
 the reference tree only through oracle/_ref, and is never run by the tests themselves.
@@ -48,11 +58,19 @@ LUTS = [
     ("B", 1.0, 0.01, 10.0, 0.05, 2000, 2048, 34, 12.0),
     ("C", 0.3, 0.0025, 50.0, 0.0, 4000, 512, 18, 6.0),
 ]
+# the benchmark configurations (plain form, precision form)
+BASELINE_LUTS = [
+    ("D", 1.0, 0.01, 10.0, 0.0, 4000, 4096, 66, 10.0),
+    ("E", 1.0, 0.01, 10.0, 0.0, 20000, 8192, 258, 20.0),
+]
+# the benchmark's proposals per set: (k_max, max_angle)
+BASELINE_PROPOSALS = {"D": (32, 0.1), "E": (32, 0.05)}
 GEOM = {  # N -> (startPos, startDir, endPos, endDir)
     66: ((0, 0, 0), (1, 0, 0), (8, 0, 0), (1, 0, 0)),
     34: ((0, 0, 0), (0, 0, 1), (0, 0, 7), (0, 0, 1)),
     18: ((0, 0, 0), (1, 0, 0), (2.5, 1.0, 0.5), (0, 1, 0)),
     10: ((0, 0, 0), (1, 0, 0), (3, 0, 0), (1, 0, 0)),
+    258: ((0, 0, 0), (0, 0, 1), (0, 0, 12), (0, 0, 1)),
 }
 
 
@@ -144,9 +162,99 @@ def make_msegment(tmp):
             json.dump(ms, f, indent=1)
 
 
+def weighed_batch(tmp, name, mu, eps, scatter, absorption, nsteps, bins, N, S, init, proposals=None):
+    """Reference table for the set, and a path batch weighed by the reference weigher: the
+    initial curve, chain states after a few rotations of U(-pi, pi) (the reference's own
+    proposals), after longer runs of the benchmark's proposals when given, and a straight path."""
+    ds = F32(S) / F32(N)
+    lf, hdr, lut = ref_lut(tmp, mu, eps, scatter, absorption, nsteps, bins, ds)
+    np.savez(os.path.join(OUT, f"lut_{name}.npz"), lut=lut, hdr=hdr,
+             params=np.array([mu, eps, scatter, absorption, nsteps, bins, N, S], np.float64))
+    wp = O.wparams(mu, eps, scatter, absorption, nsteps, bins)
+    olut, meta = O.lut_f32(wp, ds)
+    pos = [init[None]]
+    for seed, steps in ((11, 3), (12, 17), (13, 60)):
+        r = O.run_chains(init, N, S, olut, meta, seed=seed, n_chains=20, steps=steps, want_final=True)
+        pos.append(r["final_pos"])
+    if proposals:
+        k_max, angle = proposals
+        for seed, steps in ((14, 200), (15, 2000)):
+            r = O.run_chains(init, N, S, olut, meta, seed=seed, n_chains=20, steps=steps, want_final=True,
+                             k_max=k_max, max_angle=angle)
+            pos.append(r["final_pos"])
+    st = np.zeros((1, N + 1, 3), F32)
+    st[0, :, 0] = np.arange(N + 1, dtype=F32) * ds
+    pos.append(st)
+    pos = np.concatenate(pos).astype(F32)
+    w, valid, curv, rbins = ref_weigh(tmp, lf, N, S, absorption, pos)
+    np.savez(os.path.join(OUT, f"paths_{name}.npz"), pos=pos, log10w=w, valid=valid, curv=curv, bins=rbins)
+    print(f"lut/paths {name}: {pos.shape[0]} paths, N={N}")
+
+
+def reference_chain_run(tmp, key, N, S, paths, threads, mu, eps, scatter, absorption, nsteps, bins, curve, skip=1000):
+    cfg = make_config(N, S, paths, skip, 4321, mu, eps, scatter, absorption, nsteps, bins, threads)
+    cf = os.path.join(tmp, f"chain_{key}.json")
+    json.dump(cfg, open(cf, "w"))
+    np.asarray(curve, F32).tofile(cf + ".curve")
+    run(["chain", cf, cf + ".curve", threads, paths, cf + ".out"])
+    res = json.load(open(cf + ".out"))
+    res["config"] = cfg
+    json.dump(res, open(os.path.join(OUT, f"chain_{key}.json"), "w"))
+    print(f"chain {key} N={N}: log10 W = {res['log10_weight']:.6f} in {res['perturb_ms']:.0f} ms")
+
+
+def make_baseline_sets(tmp):
+    """Fixtures at the benchmark configurations: tables, weighed batches and runner runs."""
+    threads = os.cpu_count() or 1
+    boot66 = ref_bootstrap(tmp, 66, 10.0, 7)
+    assert np.array_equal(boot66, np.load(os.path.join(OUT, "boot_66.npy")))
+    boot258 = ref_bootstrap(tmp, 258, 20.0, 7)
+    np.save(os.path.join(OUT, "boot_258.npy"), boot258)
+    boots = {66: boot66, 258: boot258}
+    for name, mu, eps, scatter, absorption, nsteps, bins, N, S in BASELINE_LUTS:
+        if "--runs-only" not in sys.argv:
+            weighed_batch(tmp, name, mu, eps, scatter, absorption, nsteps, bins, N, S, boots[N],
+                          BASELINE_PROPOSALS[name])
+        # burn-in per chain: at N = 66 the reference's chains forget the initial curve within
+        # 1000 steps; at N = 258 (S = 20 on a 12-unit chord) their first million steps still
+        # relax (chunk sums 30 decades above the later ones), so that run skips 3e6 steps
+        reference_chain_run(tmp, name, N, S, 16_000_000, threads, mu, eps, scatter, absorption, nsteps, bins,
+                            boots[N], skip=1000 if N < 200 else 3_000_000)
+
+
+NORM_CASES = [
+    (4, 0.25, [0, 0, 0, 0, 0, 1, 0.3, 0.1, 0.4, 0, 0, 1]),
+    (4, 0.5, [0, 0, 0, 1, 0, 0, 0.7, 0.2, 0.1, 0, 1, 0]),
+    (4, 0.1, [0, 0, 0, 0, 0, 1, 0, 0, 0.25, 0, 0, 1]),
+    # N = 5 and 6 run the reference's nested 1e10-term quadrature (K5 and K6 both expand to the
+    # same sum over F7, PathWeightUtils.cpp:705); z = 1.83 and 1.87, inside the K4 support
+    (5, 0.25, [0, 0, 0, 0, 0, 1, 0.2, 0.1, 0.9, 0, 0, 1]),
+    (6, 0.2, [0, 0, 0, 0, 0, 1, 0.1, 0.2, 0.7, 0, 0, 1]),
+]
+
+
+def make_norm():
+    norm = []
+    for N, ds, bc in NORM_CASES:
+        out = run(["norm", N, repr(ds), *bc]).stdout.strip().splitlines()[-1]
+        norm.append({"N": N, "ds": ds, "bc": bc, "log10": float(out)})
+        print(f"norm N={N} ds={ds}: {float(out)!r}")
+    json.dump(norm, open(os.path.join(OUT, "norm.json"), "w"), indent=1)
+
+
 def main():
     if not os.path.exists(H):
         sys.exit("build the reference first: make -C oracle ref")
+    if "--only" in sys.argv:
+        what = sys.argv[sys.argv.index("--only") + 1]
+        with tempfile.TemporaryDirectory() as tmp:
+            if what == "baseline":
+                make_baseline_sets(tmp)
+            elif what == "norm":
+                make_norm()
+            else:
+                sys.exit(f"unknown --only {what}")
+        return
     rng = np.random.default_rng(20261203)
     with tempfile.TemporaryDirectory() as tmp:
         # ---- bootstrap curves
@@ -160,26 +268,7 @@ def main():
             return
         # ---- tables and weighed path batches
         for name, mu, eps, scatter, absorption, nsteps, bins, N, S in LUTS:
-            ds = F32(S) / F32(N)
-            lf, hdr, lut = ref_lut(tmp, mu, eps, scatter, absorption, nsteps, bins, ds)
-            np.savez(os.path.join(OUT, f"lut_{name}.npz"), lut=lut, hdr=hdr,
-                     params=np.array([mu, eps, scatter, absorption, nsteps, bins, N, S], np.float64))
-            wp = O.wparams(mu, eps, scatter, absorption, nsteps, bins)
-            olut, meta = O.lut_f32(wp, ds)
-            init = boots[N]
-            pos = [init[None]]
-            # curved configurations: chain states after a few rotations of U(-pi, pi)
-            for seed, steps in ((11, 3), (12, 17), (13, 60)):
-                r = O.run_chains(init, N, S, olut, meta, seed=seed, n_chains=20, steps=steps, want_final=True)
-                pos.append(r["final_pos"])
-            # a fully stretched straight path (all curvatures 0) on the same N
-            st = np.zeros((1, N + 1, 3), F32)
-            st[0, :, 0] = np.arange(N + 1, dtype=F32) * ds
-            pos.append(st)
-            pos = np.concatenate(pos).astype(F32)
-            w, valid, curv, rbins = ref_weigh(tmp, lf, N, S, absorption, pos)
-            np.savez(os.path.join(OUT, f"paths_{name}.npz"), pos=pos, log10w=w, valid=valid, curv=curv, bins=rbins)
-            print(f"lut/paths {name}: {pos.shape[0]} paths, N={N}")
+            weighed_batch(tmp, name, mu, eps, scatter, absorption, nsteps, bins, N, S, boots[N])
         # ---- rotation
         n = 512
         q = rng.normal(size=(n, 4)).astype(F32)
@@ -208,27 +297,12 @@ def main():
                          "extract_log10": list(struct.unpack("<ddd", b[96:120]))})
         json.dump(recs, open(os.path.join(OUT, "cw.json"), "w"))
         # ---- normaliser
-        norm = []
-        for N, ds, bc in ((4, 0.25, [0, 0, 0, 0, 0, 1, 0.3, 0.1, 0.4, 0, 0, 1]),
-                          (4, 0.5, [0, 0, 0, 1, 0, 0, 0.7, 0.2, 0.1, 0, 1, 0]),
-                          (4, 0.1, [0, 0, 0, 0, 0, 1, 0, 0, 0.25, 0, 0, 1])):
-            out = run(["norm", N, repr(ds), *bc]).stdout.strip().splitlines()[-1]
-            norm.append({"N": N, "ds": ds, "bc": bc, "log10": float(out)})
-        if os.environ.get("TWISTY_GOLDEN_NORM5"):
-            out = run(["norm", 5, repr(0.25), 0, 0, 0, 0, 0, 1, 0.2, 0.1, 0.9, 0, 0, 1]).stdout.strip().splitlines()[-1]
-            norm.append({"N": 5, "ds": 0.25, "bc": [0, 0, 0, 0, 0, 1, 0.2, 0.1, 0.9, 0, 0, 1], "log10": float(out)})
-        json.dump(norm, open(os.path.join(OUT, "norm.json"), "w"), indent=1)
+        make_norm()
         # ---- reference Markov-chain runs (statistical parity): theta ~ U(-pi, pi), k <= 25
         for N, S, paths, threads in ((10, 5.0, 32_000_000, 8), (18, 6.0, 16_000_000, 8), (66, 10.0, 16_000_000, 8)):
-            cfg = make_config(N, S, paths, 1000, 4321, 1.0, 0.01, 10.0, 0.0, 2000, 1024, threads)
-            cf = os.path.join(tmp, f"chain_{N}.json")
-            json.dump(cfg, open(cf, "w"))
-            np.asarray(boots[N], F32).tofile(cf + ".curve")
-            run(["chain", cf, cf + ".curve", threads, paths, cf + ".out"])
-            res = json.load(open(cf + ".out"))
-            res["config"] = cfg
-            json.dump(res, open(os.path.join(OUT, f"chain_{N}.json"), "w"))
-            print(f"chain N={N}: log10 W = {res['log10_weight']:.6f} in {res['perturb_ms']:.0f} ms")
+            reference_chain_run(tmp, str(N), N, S, paths, threads, 1.0, 0.01, 10.0, 0.0, 2000, 1024, boots[N])
+        # ---- the benchmark configurations
+        make_baseline_sets(tmp)
 
 
 if __name__ == "__main__":

@@ -91,3 +91,31 @@ def test_batch_empty_experiment_and_empty_batch():
         res = ctx.run_batch(exps)
     assert res[1].total_paths == 0 and res[1].num_chains == 0
     assert res[0].total_paths == exps[0].paths
+
+
+def test_batch_matches_oracle_fp64_twin(oracle):
+    """Each experiment of a batch of uneven N against the oracle's FP64 twin chains on the same
+    proposals (Philox stream of the experiment, chain ids, burn-in), the same initial curve and
+    its own FP64 table (mu_s, eps, maxBound = 10/eps per experiment): within 1e-4 relative.
+    Small rotation angles keep the FP32 and FP64 trajectories together."""
+    base = {**BASE, "max_angle": 0.1}
+    chains, steps = 256, 64
+    exps = _experiments()[:5]
+    for x in exps:
+        x.paths = chains * steps
+    with T.Context(T.default_params(num_segments=16, eps=0.01, scatter=10.0, num_chains=chains, **base)) as ctx:
+        res = ctx.run_batch(exps)
+    for i, (x, r) in enumerate(zip(exps, res)):
+        assert r.num_chains == chains and r.steps_per_chain == steps and r.total_paths == chains * steps
+        N = x.num_segments
+        p = T.default_params(num_segments=N, **{**base, "bootstrap_seed": base["bootstrap_seed"] + i})
+        init = T.bootstrap_curve(p, x.bc)
+        ds = float(np.float32(x.bc.arclength) / np.float32(N))
+        lut, meta = oracle.lut_f64(oracle.wparams(base["mu"], x.eps, x.scatter, 0.0, base["num_steps_int"],
+                                                  base["num_curvature_steps"]), ds)
+        o = oracle.run_chains(init, N, x.bc.arclength, lut, meta, seed=base["perturb_seed"], n_chains=chains,
+                              steps=steps, burn_in=base["paths_to_skip"], k_max=base["max_sub_chain"],
+                              max_angle=base["max_angle"], experiment=base["experiment_id"] + i, f64=True)
+        ref = oracle.log10_sum(o["chain_log10"])
+        rel = abs(10 ** (r.log10_weight - ref) - 1)
+        assert rel < 1e-4, (i, N, r.log10_weight, ref, rel)

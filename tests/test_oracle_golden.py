@@ -57,8 +57,9 @@ def test_weigher_bit_exact(oracle, name):
     assert np.array_equal(w, p["log10w"])
     assert np.array_equal(curv.view(np.uint32), p["curv"].view(np.uint32))
     assert np.array_equal(b, p["bins"])
-    # the straight path (last) has every curvature exactly 0 and bin 0
-    assert np.all(p["curv"][-1] == 0) and np.all(p["bins"][-1] == 0)
+    # the straight path (last) has every curvature 0 up to the rounding of its unit tangents
+    # (x (1/sqrtf(x x)) need not be exactly 1), and bin 0
+    assert np.all(p["curv"][-1] < 1e-5) and np.all(p["bins"][-1] == 0)
 
 
 def test_rotation_bit_exact(oracle):

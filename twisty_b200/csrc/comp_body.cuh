@@ -356,9 +356,12 @@ enum { kModeForward = 0, kModeExport = 1, kModeAdjoint = 2 };
 // Receiver-position gradient of one path's log10 weight, computed by one lane from the last
 // three segments: moving the receiver moves points N-1 and N together, so only the segment
 // vector v_{N-2} changes, hence t_{N-2} and the curvatures kappa_{N-3}, kappa_{N-2}. The
-// table's slope is taken per bin, (L_{i+1} - L_i) / step, the derivative of the curve the table
-// samples (the reference's interpolation weight in curvature units makes its own weight
-// almost piecewise constant within a bin, a slope finite differences do not see).
+// reference's interpolation weight is in curvature units (PathWeighters.cpp:79-82), so its
+// segment weight is almost constant within a bin and jumps by nearly L_{b+1} - L_b at each
+// edge: its pathwise derivative misses almost all of the change an expectation over paths
+// sees. The slope taken is that of the expected weight: averaged over a bin the staircase is
+// the table's linear interpolant taken half a bin to the left, whose slope at fractional bin r
+// is (L_{J+1} - L_J) / step with J = floor(r - 1/2); divided by the weight itself.
 __device__ __forceinline__ void receiver_grad(const float t3[3], const float t2[3], const float t1[3], float len2,
                                               const float *__restrict__ lut, const CompConsts &k, float inv_ds,
                                               float g[3])
@@ -380,7 +383,9 @@ __device__ __forceinline__ void receiver_grad(const float t3[3], const float t2[
         const float lv = __ldg(lut + L), rv = __ldg(lut + R);
         const float dd = (r - (float)L) * k.step;
         const float blend = fmaf(dd, rv - lv, lv);
-        const float dlog = (rv - lv) / (k.step * blend) * kInvLn10;  // d log10 w / d kappa
+        const int32_t J = min(max((int32_t)floorf(r - 0.5f), 0), k.bins - 2);
+        const float sl = __ldg(lut + J + 1) - __ldg(lut + J);
+        const float dlog = sl / (k.step * blend) * kInvLn10;  // d log10 w / d kappa
         const float dk = dlog * inv_ds * sign / dn;                  // d kappa / d t = inv_ds d/|d|
         const float dt = d[0] * t2[0] + d[1] * t2[1] + d[2] * t2[2];
         for (int q = 0; q < 3; ++q) g[q] += dk * (d[q] - dt * t2[q]) * r2;
