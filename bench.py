@@ -15,9 +15,9 @@ Metric: path-segments weighted per second = weighted paths x N / time.
   value  device time of the pass (chain kernel + FP64 reduction), CUDA events on the
          launching stream, L2 flushed between steps, max over ranks;
   e2e    the same metric through the C ABI with host buffers, one experiment per step as the
-         reference's callers run one: a fresh context, twisty_run (table built on the device,
-         normaliser, initial curve, host-to-device copies, the pass, the result copied back),
-         the context destroyed.
+         reference's callers run one: the experiment's parameters set on the caller's context
+         (the table is built again), twisty_run (table built on the device, normaliser, initial
+         curve, host-to-device copies, the pass, the result copied back).
 The JSON line also carries the FP64 error of the estimate, the plain FP32 drop-in's
 throughput on the same workload, the roofline of the chain kernel, and a CPU baseline
 (the reference's own chain loop, compiled from its sources, on this host's cores).
@@ -316,6 +316,19 @@ def run_image_workload(args, T, torch, device, ws, rank, pg):
     t0 = time.perf_counter()
     ctx.run_batch(exps, iterations=1)
     e2e_ms = (time.perf_counter() - t0) * 1e3
+    adjoint = None
+    if not args.no_adjoint:
+        # gradients of the image's total log-energy with respect to sigma and mu_s: one forward
+        # pass and one batched adjoint replay of every pixel's chains (twisty_adjoint_batch)
+        t0 = time.perf_counter()
+        _, grad, total, tms = ctx.adjoint_batch(exps)
+        adj_ms = (time.perf_counter() - t0) * 1e3
+        adjoint = {"call_ms": adj_ms, "derivative_tables_ms": float(tms[0]), "replay_ms": float(tms[1]),
+                   "log10_total_energy": float(total[0]), "d_log10_total_d_mu_s": float(total[1]),
+                   "d_log10_total_d_sigma": float(total[2]),
+                   "replay_path_segments_per_s": sum(r.total_paths * I["N"] for r in res) / (float(tms[1]) / 1e3),
+                   "note": "call = forward pass + derivative tables + adjoint replay; replay recomputes every "
+                           "curvature (exact blend) and stores nothing per step"}
     if pg:
         t = torch.tensor([per_step, e2e_ms], dtype=torch.float64, device=f"cuda:{device}")
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
@@ -343,63 +356,99 @@ def run_image_workload(args, T, torch, device, ws, rank, pg):
                              "unit": "Tinstr/s", "frac": achieved_ti / peak_ti, "traffic": None,
                              "basis": f"{INSTR_PER_SEGMENT:g} FP32 instructions per path-segment"},
                 "cpu_baseline": None, "clocks": clk.summary(), "gpu_launches": launches * args.steps}
+        if adjoint:
+            line["adjoint"] = adjoint
         print(json.dumps(line))
     if pg:
         pg.destroy_process_group()
     return 0
 
 
-def run_batch_workload(args, T, torch, device, ws, rank, pg):
-    """The batching workload through twisty_run_batch: every rank runs all experiments on its own
-    chain range (chain_offset), and the per-experiment results combine across ranks."""
-    exps = batch_experiments(T)
-    segs = sum(x.paths * x.num_segments for x in exps)
+def measure_batch(T, device, steps, warmup, exps=None, first=0, chain_offset=0):
+    """The batching workload through twisty_run_batch on one device: device time per replay of
+    the captured pass, end-to-end time per whole call (host experiments in, results out), and
+    the results. `first` numbers the experiments from that index of the full batch (their
+    Philox streams and bootstrap seeds), so that a rank's sub-batch gives the full batch's
+    results."""
+    if exps is None:
+        exps = batch_experiments(T)
     params = batch_params(T, device=device)
-    with T.Context(params) as probe:   # the chain layout every rank uses
-        chains = probe.run_batch(exps[:1])[0].num_chains
-    params.chain_offset = rank * 1_000_000
+    params.experiment_id += first
+    params.bootstrap_seed += first
+    params.chain_offset = chain_offset
     ctx = T.Context(params)
-    ctx.run_batch(exps, iterations=max(1, args.warmup))
+    ctx.run_batch(exps, iterations=max(1, warmup))
     with ClockSampler(device) as clk:
-        res = ctx.run_batch(exps, iterations=args.steps)
+        res = ctx.run_batch(exps, iterations=steps)
     launches = ctx.kernels_per_launch()
-    per_step = res[0].perturb_ms
-    setup_ms = res[0].setup_ms
-    if pg:
-        pg.barrier()
+    per_step = res[0].perturb_ms if res else 0.0
+    setup_ms = res[0].setup_ms if res else 0.0
     # end to end: `steps` whole calls (host inputs in, results out), averaged
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        e2e = ctx.run_batch(exps, iterations=1)
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
-    if pg:
-        t = torch.tensor([per_step, e2e_ms], dtype=torch.float64, device=f"cuda:{device}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        per_step, e2e_ms = t.tolist()
+    for _ in range(steps):
+        ctx.run_batch(exps, iterations=1)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / steps
     ctx.close()
     done = sum(r.total_paths * x.num_segments for r, x in zip(res, exps))
-    value = done * ws / (per_step / 1e3)
+    return dict(res=res, exps=exps, per_step=per_step, setup_ms=setup_ms, e2e_ms=e2e_ms, done=done,
+                launches=launches, clocks=clk.summary())
+
+
+def batch_roofline(done, per_step):
     peaks = load_peaks()
     sm_max = peaks.get("sm_max_mhz", 1965.0)
     peak_ti = SMS * LANES_PER_SM * sm_max * 1e6 / 1e12
     achieved_ti = INSTR_PER_SEGMENT * done / (per_step / 1e3) / 1e12
+    return {"bound": "fp32", "kernel": "batch_kernel", "achieved": achieved_ti, "peak": peak_ti, "unit": "Tinstr/s",
+            "frac": achieved_ti / peak_ti, "traffic": None,
+            "basis": f"{INSTR_PER_SEGMENT:g} FP32 instructions per path-segment; peak = {SMS} SMs x {LANES_PER_SM} "
+                     f"lanes x {sm_max:g} MHz"}
+
+
+def run_batch_workload(args, T, torch, device, ws, rank, pg):
+    """The batching workload through twisty_run_batch. Over several ranks the experiments are
+    split by experiment (a contiguous range per rank with its share of the work, the full
+    batch's stream ids) and every experiment's result is gathered on every rank."""
+    from twisty_b200 import dist as D
+    allx = batch_experiments(T)
+    idx = D.partition_experiments(allx, rank, ws) if ws > 1 else list(range(len(allx)))
+    mine = [allx[i] for i in idx]
+    if pg:
+        pg.barrier()
+    m = measure_batch(T, device, args.steps, args.warmup, exps=mine, first=idx[0] if idx else 0)
+    per_step, e2e_ms = m["per_step"], m["e2e_ms"]
+    combined = None
+    if pg:
+        t = torch.tensor([per_step, e2e_ms], dtype=torch.float64, device=f"cuda:{device}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        per_step, e2e_ms = t.tolist()
+        full = D.gather_partitioned(m["res"], idx, len(allx), device=f"cuda:{device}")
+        combined = {"experiments": len(full), "total_paths": sum(r["total_paths"] for r in full),
+                    "failed_paths": sum(r["failed_paths"] for r in full)}
+        dn = torch.tensor([float(m["done"])], dtype=torch.float64, device=f"cuda:{device}")
+        pg.all_reduce(dn)
+        done_all = dn.item()
+    else:
+        done_all = m["done"]
+    value = done_all / (per_step / 1e3)
     if rank == 0:
         import ctypes
-        h2d = ctypes.sizeof(T._abi.Experiment) * len(exps)   # the experiment array; tables are built on the device
-        d2h = ctypes.sizeof(T._abi.Result) * len(exps)
+        h2d = ctypes.sizeof(T._abi.Experiment) * len(allx)   # the experiment array; tables are built on the device
+        d2h = ctypes.sizeof(T._abi.Result) * len(allx)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": per_step, "higher_is_better": True, "scaling": "weak",
+                "warmup": args.warmup, "ms_per_step": per_step, "higher_is_better": True,
+                "scaling": "strong" if ws > 1 else "weak",
                 "vs_baseline": None, "dtype": "f32 (f64 cross-chain)", "data": "synthetic",
-                "config": {"workload": BATCH_NAME, "form": "compensated", "experiments": len(exps),
-                           "path_segments_per_step": segs, "chains_first_experiment": chains,
+                "config": {"workload": BATCH_NAME, "form": "compensated", "experiments": len(allx),
+                           "path_segments_per_step": sum(x.paths * x.num_segments for x in allx),
                            "l2": "inputs larger than L2 (4096 tables of 4096 bins, 134 MB fixed-point + 134 MB linear)",
-                           "parallelism": f"independent chains x{ws}"},
-                "e2e": {"value": done * ws / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms,
-                        "setup_ms": setup_ms, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-                "roofline": {"bound": "fp32", "kernel": "batch_kernel", "achieved": achieved_ti, "peak": peak_ti,
-                             "unit": "Tinstr/s", "frac": achieved_ti / peak_ti, "traffic": None,
-                             "basis": f"{INSTR_PER_SEGMENT:g} FP32 instructions per path-segment"},
-                "cpu_baseline": None, "clocks": clk.summary(), "gpu_launches": launches * args.steps}
+                           "parallelism": f"experiments split over {ws} ranks" if ws > 1 else "one GPU"},
+                "e2e": {"value": done_all / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms,
+                        "setup_ms": m["setup_ms"], "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "roofline": batch_roofline(m["done"], m["per_step"]),
+                "cpu_baseline": None, "clocks": m["clocks"], "gpu_launches": m["launches"] * args.steps}
+        if combined:
+            line["combined"] = combined
         print(json.dumps(line))
     if pg:
         pg.destroy_process_group()
@@ -416,6 +465,8 @@ def main():
     ap.add_argument("--no-error", action="store_true", help="skip the FP64 error measurement")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP32 drop-in")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-batch", action="store_true", help="skip timing the batching workload")
+    ap.add_argument("--no-adjoint", action="store_true", help="image workload: skip the batched adjoint")
     ap.add_argument("--paths", type=int, default=0, help="paths per pass (default 2^26; smaller for profiling)")
     ap.add_argument("--workload", default="precision", choices=["precision", "batch", "image"],
                     help="precision: one N=256 experiment (the headline); batch: 4096 uneven experiments; "
@@ -468,24 +519,27 @@ def main():
     segs = res.total_paths * W["N"]
     value = segs * ws / (per_step / 1e3)
 
-    # End to end through the C ABI with host buffers, as a caller of the reference runs an
-    # experiment (Experiments/FullExperiment.cpp:204-230: construct the runner, RunExperiment):
-    # every step creates a context, builds the table (RunExperiment builds its table on every
-    # call, FullExperimentRunnerOptimalPerturb.cpp:59-69), bootstraps and uploads the initial
-    # curve, runs the pass, reads the result back and destroys the context.
+    # End to end through the C ABI with host buffers, one experiment per step as a caller of the
+    # reference runs one (Experiments/FullExperiment.cpp:204-230): the context is the caller's
+    # runner, kept across experiments; every step sets the experiment's parameters
+    # (twisty_update_params, after which the table is built again, as RunExperiment builds its
+    # table on every call, FullExperimentRunnerOptimalPerturb.cpp:59-69) and runs it
+    # (twisty_run: the table on the device, the initial curve, the uploads, the pass, the result
+    # read back).
     e2e_params = workload_params(T, form, num_chains=chains, chain_offset=rank * chains, device=device)
-    with T.Context(e2e_params) as warm:
-        warm.run(bc)   # module load and first-touch costs, outside the timed region
+    e2e_ctx = T.Context(e2e_params)
+    e2e_ctx.run(bc)   # module load and the context's first allocations, outside the timed region
     reps = max(1, min(args.steps, 5))
     if pg:
         pg.barrier()
     torch.cuda.synchronize(device)
     t0 = time.perf_counter()
     for _ in range(reps):
-        with T.Context(e2e_params) as e2e_ctx:
-            er = e2e_ctx.run(bc)
+        e2e_ctx.set_params(e2e_params)
+        er = e2e_ctx.run(bc)
     torch.cuda.synchronize(device)
     e2e_ms = (time.perf_counter() - t0) * 1e3 / reps
+    e2e_ctx.close()
     if pg:
         t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{device}")
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
@@ -536,6 +590,26 @@ def main():
                                 "note": "weights updated from the two curvatures each rotation changes, full "
                                         "recompute every resync_every-th weighted step; not the headline"}
 
+    if rank == 0 and form == T.FORM_COMPENSATED and not args.no_batch:
+        # the batching form on its own workload (4096 uneven experiments), timed in this run
+        bm = measure_batch(T, device, max(3, min(args.steps, 10)), 1)
+        import ctypes
+        extra["batching"] = {
+            "workload": BATCH_NAME, "value": bm["done"] / (bm["per_step"] / 1e3), "unit": UNIT,
+            "ms_per_step": bm["per_step"], "steps": max(3, min(args.steps, 10)),
+            "e2e": {"value": bm["done"] / (bm["e2e_ms"] / 1e3), "unit": UNIT, "ms_per_step": bm["e2e_ms"],
+                    "setup_ms": bm["setup_ms"],
+                    "h2d_bytes_per_step": ctypes.sizeof(T._abi.Experiment) * len(bm["exps"]),
+                    "d2h_bytes_per_step": ctypes.sizeof(T._abi.Result) * len(bm["exps"])},
+            "roofline": batch_roofline(bm["done"], bm["per_step"]), "gpu_launches_per_step": bm["launches"],
+            "failed_paths": sum(r.failed_paths for r in bm["res"]), "clocks": bm["clocks"]}
+
+    combined = None
+    if pg:
+        # the one exchange step: every rank's (log10 sum, relative SE, counts) combined
+        from twisty_b200 import dist as D
+        combined = D.all_combine(res, device=f"cuda:{device}")
+
     peaks = load_peaks()
     clocks = clk.summary()
     sm_max = peaks.get("sm_max_mhz", 1965.0)
@@ -569,10 +643,13 @@ def main():
                            "l2": "flushed between steps (256 MB write)", "parallelism": f"independent chains x{ws}"},
                 "e2e": {"value": segs * ws / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms,
                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                        "per_step": "context create + table build + initial curve + pass + result + destroy",
+                        "per_step": "twisty_update_params + twisty_run: table build, initial curve, uploads, pass, "
+                                    "result read back",
                         "setup_ms": er.setup_ms},
                 "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
                 "gpu_launches": ctx.kernels_per_launch() * args.steps, **extra}
+        if combined:
+            line["combined"] = combined
         print(json.dumps(line))
     ctx.close()
     if pg:

@@ -209,6 +209,8 @@ twisty_status twisty_params_from_config(const char *text, int is_yaml, twisty_pa
 twisty_status twisty_create(const twisty_params *p, twisty_ctx **out);
 void twisty_destroy(twisty_ctx *ctx);
 const char *twisty_last_error(const twisty_ctx *ctx);
+/* New parameters for the context's next runs; the next run builds its weight tables again
+ * (as every RunExperiment of the reference builds its table). */
 twisty_status twisty_update_params(twisty_ctx *ctx, const twisty_params *p);
 
 /* ----------------------------------------------------------- experiments */
@@ -227,6 +229,13 @@ twisty_status twisty_launch(twisty_ctx *ctx, void *stream);
 twisty_status twisty_collect(twisty_ctx *ctx, twisty_result *res);
 /* Number of kernels twisty_launch enqueues (for launch accounting). */
 uint32_t twisty_launch_kernel_count(const twisty_ctx *ctx);
+
+/* Per-chain outcomes of the context's last pass (twisty_run, twisty_launch): log10 of each
+ * chain's summed path weights (normaliser applied) and its count of valid paths; valid may be
+ * NULL, n_chains must be the pass's chain count (twisty_result.num_chains). The reference's
+ * runner keeps per-thread running sums for its convergence records
+ * (FullExperimentRunnerOptimalPerturb.cpp:96-109,358-365); a chain here is a thread there. */
+twisty_status twisty_chain_results(twisty_ctx *ctx, double *log10_sum, uint64_t *valid, uint32_t n_chains);
 
 /* Many experiments (uneven N, S, mu_s, eps) in one persistent launch fed by a device
  * work queue; the pass is captured once as a CUDA graph and replayed `iterations` times
@@ -296,6 +305,20 @@ twisty_status twisty_export_paths(twisty_ctx *ctx, const twisty_bc *bc, const ch
  * (pathwise estimator). grad has 5 entries. */
 twisty_status twisty_adjoint(twisty_ctx *ctx, const twisty_bc *bc, const twisty_result *fwd,
                              double grad[5]);
+
+/* The adjoint of a batch: the receiver/pixel loops of the reference's image drivers
+ * (Experiments/BeamSpreadExperiment.cpp:240-269, NoisyCircleExperiment.cpp:259-361) call
+ * RunExperiment per pixel; differentiating the image takes one forward pass of the batch
+ * (twisty_run_batch, results in res[n]) and one persistent adjoint replay of every experiment's
+ * chains (curvatures recomputed, derivative tables d/d(mu_s), d/d(eps) built in FP64 on the
+ * device). grad[n][5]: d log10 W_e / d (mu_s, sigma, receiver x, y, z) of each experiment, for
+ * its own mu_s, sigma = sqrt(eps) and receiver, as twisty_adjoint defines them. total (nullable):
+ * {log10 sum_e W_e, d / d mu_s, d / d sigma} of the batch's total -- the image's total
+ * log-energy -- for a mu_s and sigma shared by all experiments (each experiment's derivative
+ * weighted by its share of the total). timing_ms (nullable): device time of the derivative
+ * tables and of the replay. Needs lut_mode FP64 or MULTI_DS. */
+twisty_status twisty_adjoint_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, twisty_result *res,
+                                   double *grad, double total[3], double timing_ms[2]);
 
 /* CachedMultiArclengthWeightLookupTable (Twisty/PathWeightUtils.cpp:123-278): n_ds tables for
  * ds_i = min_ds + i (max_ds - min_ds) / (n_ds - 1) (float arithmetic, :170-173) with the

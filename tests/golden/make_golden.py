@@ -191,14 +191,32 @@ def weighed_batch(tmp, name, mu, eps, scatter, absorption, nsteps, bins, N, S, i
     print(f"lut/paths {name}: {pos.shape[0]} paths, N={N}")
 
 
-def reference_chain_run(tmp, key, N, S, paths, threads, mu, eps, scatter, absorption, nsteps, bins, curve, skip=1000):
-    cfg = make_config(N, S, paths, skip, 4321, mu, eps, scatter, absorption, nsteps, bins, threads)
-    cf = os.path.join(tmp, f"chain_{key}.json")
-    json.dump(cfg, open(cf, "w"))
-    np.asarray(curve, F32).tofile(cf + ".curve")
-    run(["chain", cf, cf + ".curve", threads, paths, cf + ".out"])
-    res = json.load(open(cf + ".out"))
-    res["config"] = cfg
+def reference_chain_run(tmp, key, N, S, paths, threads, mu, eps, scatter, absorption, nsteps, bins, curve, skip=1000,
+                        repeats=1):
+    """The reference's runner loop on `threads` chains (perturbSeed 4321 + thread); with repeats
+    > 1, further runs on the next seeds (4321 + r * threads + thread), their 1e6-path chunks
+    pooled into one record (the runner uses at most one chain per host core)."""
+    recs = []
+    for r in range(repeats):
+        cfg = make_config(N, S, paths, skip, 4321 + r * threads, mu, eps, scatter, absorption, nsteps, bins, threads)
+        cf = os.path.join(tmp, f"chain_{key}.json")
+        json.dump(cfg, open(cf, "w"))
+        np.asarray(curve, F32).tofile(cf + ".curve")
+        run(["chain", cf, cf + ".curve", threads, paths, cf + ".out"])
+        res = json.load(open(cf + ".out"))
+        res["config"] = cfg
+        recs.append(res)
+    res = recs[0]
+    if repeats > 1:
+        res["chunk_log10"] = [x for r in recs for x in r["chunk_log10"]]
+        res["chunk_paths"] = [x for r in recs for x in r["chunk_paths"]]
+        res["paths"] = sum(r["paths"] for r in recs)
+        res["perturb_ms"] = sum(r["perturb_ms"] for r in recs)
+        res["runs"] = [{"perturbSeed": r["config"]["experiment"]["experimentParams"]["random"]["perturbSeed"],
+                        "log10_weight": r["log10_weight"]} for r in recs]
+        x = np.array([v for v, n in zip(res["chunk_log10"], res["chunk_paths"]) if n > 0])
+        res["log10_weight"] = float(x.max() + np.log10((10.0 ** (x - x.max())).sum()) + res["log10_normalizer"])
+        res["config"]["experiment"]["experimentParams"]["pathsToGenerate"] = res["paths"]
     json.dump(res, open(os.path.join(OUT, f"chain_{key}.json"), "w"))
     print(f"chain {key} N={N}: log10 W = {res['log10_weight']:.6f} in {res['perturb_ms']:.0f} ms")
 
@@ -217,9 +235,16 @@ def make_baseline_sets(tmp):
                           BASELINE_PROPOSALS[name])
         # burn-in per chain: at N = 66 the reference's chains forget the initial curve within
         # 1000 steps; at N = 258 (S = 20 on a 12-unit chord) their first million steps still
-        # relax (chunk sums 30 decades above the later ones), so that run skips 3e6 steps
-        reference_chain_run(tmp, name, N, S, 16_000_000, threads, mu, eps, scatter, absorption, nsteps, bins,
-                            boots[N], skip=1000 if N < 200 else 3_000_000)
+        # relax (chunk sums 30 decades above the later ones), so that run skips 3e6 steps, and
+        # runs 16 chains of one 1e6-path chunk each (its heavy-tailed weights want the standard
+        # error from independent chains, not from consecutive chunks of a few: two runs of
+        # 8 chains on distinct seeds)
+        if N < 200:
+            reference_chain_run(tmp, name, N, S, 16_000_000, threads, mu, eps, scatter, absorption, nsteps, bins,
+                                boots[N])
+        else:
+            reference_chain_run(tmp, name, N, S, 8_000_000, 8, mu, eps, scatter, absorption, nsteps, bins, boots[N],
+                                skip=3_000_000, repeats=2)
 
 
 NORM_CASES = [

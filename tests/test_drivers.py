@@ -68,3 +68,26 @@ def test_ring_sweep_as_one_batch_matches_single_runs():
         with T.Context(p) as c:
             s = c.run(e.bc)
         assert abs(s.log10_weight - r.log10_weight) < 1e-6
+
+
+@pytest.mark.gpu
+def test_beam_spread_batch_matches_oracle_fp64_twin(oracle):
+    """The BeamSpread receivers (the reference's own draws) as one batch, each experiment against
+    the oracle's FP64 twin chains on the same proposals, initial curve and its own FP64 table:
+    within 1e-4 relative (small rotation angles keep FP32 and FP64 trajectories together)."""
+    chains, steps = 256, 64
+    ex = D.beam_spread_experiments((0, 0, 0), (0, 0, 1), 3.0, 4, 42, 48, 20.0, 0.0225, chains * steps)
+    base = dict(num_segments=48, mu=1.0, eps=0.0225, scatter=20.0, num_steps_int=2000, num_curvature_steps=1024,
+                form=T.FORM_COMPENSATED, lut_mode=T.LUT_FP64, perturb_seed=9, paths_to_skip=32, max_sub_chain=32,
+                max_angle=0.1, num_chains=chains, bootstrap_seed=21, experiment_id=3)
+    with T.Context(T.default_params(**base)) as ctx:
+        res = D.run(ctx, ex)
+    for i, (e, r) in enumerate(zip(ex, res)):
+        assert r.num_chains == chains and r.steps_per_chain == steps
+        init = T.bootstrap_curve(T.default_params(**dict(base, bootstrap_seed=21 + i)), e.bc)
+        ds = float(F32(e.bc.arclength) / F32(48))
+        lut, meta = oracle.lut_f64(oracle.wparams(1.0, e.eps, e.scatter, 0.0, 2000, 1024), ds)
+        o = oracle.run_chains(init, 48, e.bc.arclength, lut, meta, seed=9, n_chains=chains, steps=steps, burn_in=32,
+                              k_max=32, max_angle=0.1, experiment=3 + i, f64=True)
+        ref = oracle.log10_sum(o["chain_log10"])
+        assert abs(10 ** (r.log10_weight - ref) - 1) < 1e-4, (i, r.log10_weight, ref)

@@ -218,10 +218,9 @@ def test_long_paths_compensated_within_1e4_of_fp64(N):
     assert rel < 1e-4, rel
 
 
-# (reference run, chains, weighted steps per chain) of the GPU side: the runs with the
-# reference's 1000-step burn-in use many short chains; the N = 258 run, whose chains need
-# millions of steps to forget the initial curve, fewer chains with the reference's burn-in
-STAT_RUNS = [("10", 8000, 1000), ("18", 8000, 1000), ("66", 8000, 1000), ("D", 8000, 1000), ("E", 2048, 2000)]
+# (reference run, chains, weighted steps per chain) of the GPU side, every chain with the
+# reference run's 1000-step burn-in
+STAT_RUNS = [("10", 8000, 1000), ("18", 8000, 1000), ("66", 8000, 1000), ("D", 8000, 1000)]
 
 
 @pytest.mark.parametrize("key,chains,steps", STAT_RUNS)
@@ -250,6 +249,40 @@ def test_statistics_match_reference_runner(key, chains, steps, form):
     got_mean = r.log10_mean_weight
     tol = 3 * np.hypot(ref_se, r.rel_std_error) / np.log(10)
     assert abs(got_mean - ref_mean) < tol, (got_mean, ref_mean, r.rel_std_error, ref_se)
+
+
+@pytest.mark.parametrize("form", [T.FORM_COMPENSATED, T.FORM_PLAIN_FP32])
+def test_chain_sums_match_reference_runner_n258(form):
+    """The precision-form configuration (N = 258, S = 20, receiver (0,0,12), 8192 bins) under the
+    reference's proposals. Its chains need millions of steps to forget the initial curve, and
+    their path weights are heavy-tailed: the reference's 16 chains (3e6 burn-in steps, then one
+    1e6-path chunk each) have sums spread over 3 decades, and its two runs of 8 chains differ by
+    1.5 decades in total. The mean of so few chains, and its standard error, are dominated by the
+    largest one or two, so a 3-standard-error test of means is not informative here; the chains
+    are compared as distributions instead: 256 chains of the same length and burn-in, their
+    log10 sums against the reference's 16 by a two-sided Mann-Whitney test at level 1e-3, and
+    their medians within the spread of the reference's."""
+    from scipy.stats import mannwhitneyu
+    rec = golden_json("chain_E.json")
+    ep = rec["config"]["experiment"]["experimentParams"]
+    w = ep["weighting"]
+    N = ep["numSegments"]
+    S = rec["config"]["experiment"]["basicExperiment"]["arclength"]
+    ref = np.array([v for v, n in zip(rec["chunk_log10"], rec["chunk_paths"]) if n == 1_000_000])
+    assert ref.size == 16
+    chains, steps = 256, 1_000_000
+    p = T.default_params(num_segments=N, mu=w["mu"], eps=w["eps"], scatter=w["scatter"], absorption=w["absorption"],
+                         num_steps_int=w["numStepsInt"], num_curvature_steps=w["numCurvatureSteps"], form=form,
+                         perturb_seed=2024, paths_to_generate=chains * steps, paths_to_skip=ep["pathsToSkip"],
+                         num_chains=chains, lut_mode=T.LUT_FAITHFUL)
+    with T.Context(p) as ctx:
+        ctx.set_initial_curve(np.load("tests/golden/boot_258.npy"))
+        r = ctx.run(geom_bc(N, S))
+        mine, valid = ctx.chain_results(r.num_chains)
+    assert r.num_chains == chains and r.steps_per_chain == steps and np.all(valid == steps)
+    pval = mannwhitneyu(mine, ref, alternative="two-sided").pvalue
+    assert pval > 1e-3, (pval, np.median(mine), np.median(ref), ref.min(), ref.max())
+    assert ref.min() <= np.median(mine) <= ref.max()
 
 
 def test_runs_are_deterministic_and_split_api_matches():

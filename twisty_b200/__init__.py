@@ -121,10 +121,22 @@ class Context:
             self.params.max_bound = float(np.float32(10.0) / np.float32(kw["eps"]))
         _check(_lib().twisty_update_params(self._h, C.byref(self.params)), self._h)
 
+    def set_params(self, params: _abi.Params):
+        """Replace the parameters (twisty_update_params); the next run builds its tables again."""
+        self.params = params
+        _check(_lib().twisty_update_params(self._h, C.byref(self.params)), self._h)
+
     def run(self, bc: _abi.BC) -> _abi.Result:
         r = _abi.Result()
         _check(_lib().twisty_run(self._h, C.byref(bc), C.byref(r)), self._h)
         return r
+
+    def chain_results(self, n_chains: int):
+        """Per-chain log10 sums (normaliser applied) and valid-path counts of the last pass."""
+        lw = np.zeros(n_chains, np.float64)
+        v = np.zeros(n_chains, np.uint64)
+        _check(_lib().twisty_chain_results(self._h, _fptr(lw), _fptr(v), n_chains), self._h)
+        return lw, v
 
     def run_msegment(self, bc: _abi.BC) -> _abi.Result:
         """Independent-sample M-segment MC: paths_to_generate fresh bootstrap curves, mean weight."""
@@ -212,6 +224,20 @@ class Context:
         t = _abi.Tuning()
         _check(_lib().twisty_autotune(self._h, C.byref(bc), int(trial_paths), C.byref(t)), self._h)
         return {f: getattr(t, f) for f, _ in _abi.Tuning._fields_}
+
+    def adjoint_batch(self, experiments: Sequence[_abi.Experiment]):
+        """Forward pass of the batch and the adjoint replay of its chains (twisty_adjoint_batch):
+        (results, grad[n, 5] = d log10 W_e / d (mu_s, sigma, receiver xyz), total[3] =
+        (log10 sum W_e, d/d mu_s, d/d sigma of it for a shared mu_s and sigma), timing_ms[2])."""
+        n = len(experiments)
+        arr = (_abi.Experiment * n)(*experiments)
+        res = (_abi.Result * n)()
+        grad = np.zeros((n, 5), np.float64)
+        total = (C.c_double * 3)()
+        timing = (C.c_double * 2)()
+        _check(_lib().twisty_adjoint_batch(self._h, arr, n, res, grad.ctypes.data_as(C.POINTER(C.c_double)), total,
+                                           timing), self._h)
+        return list(res), grad, np.array(list(total)), np.array(list(timing))
 
     def run_batch(self, experiments: Sequence[_abi.Experiment], iterations: int = 1):
         n = len(experiments)

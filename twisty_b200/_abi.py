@@ -161,6 +161,7 @@ SIGNATURES = [
     ("twisty_launch", C.c_int, [_P, _P]),
     ("twisty_collect", C.c_int, [_P, C.POINTER(Result)]),
     ("twisty_launch_kernel_count", C.c_uint32, [_P]),
+    ("twisty_chain_results", C.c_int, [_P, _P, _P, C.c_uint32]),
     ("twisty_run_batch", C.c_int, [_P, C.POINTER(Experiment), C.c_uint32, C.c_uint32, C.POINTER(Result)]),
     ("twisty_run_msegment", C.c_int, [_P, C.POINTER(BC), C.POINTER(Result)]),
     ("twisty_weight_paths", C.c_int, [_P, C.POINTER(BC), _P, C.c_uint64, C.c_int32, _P, _P, _P]),
@@ -173,6 +174,8 @@ SIGNATURES = [
     ("twisty_export_paths", C.c_int, [_P, C.POINTER(BC), C.c_char_p, C.c_uint64, _P, _P, C.POINTER(C.c_uint64),
                                       C.POINTER(Result)]),
     ("twisty_adjoint", C.c_int, [_P, C.POINTER(BC), C.POINTER(Result), C.POINTER(C.c_double)]),
+    ("twisty_adjoint_batch", C.c_int, [_P, C.POINTER(Experiment), C.c_uint32, C.POINTER(Result),
+                                       C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("twisty_run_noalloc", C.c_int, [C.POINTER(NoAllocArgs), _P]),
     ("twisty_autotune", C.c_int, [_P, C.POINTER(BC), C.c_uint64, C.POINTER(Tuning)]),
     ("twisty_multi_ds_tables", C.c_int, [_P, C.c_float, C.c_float, C.c_uint32, C.c_char_p]),

@@ -65,4 +65,53 @@ cudaError_t launch_batch(const BatchShape &s, const void *d_exps, const uint2 *d
     return cudaErrorInvalidValue;
 }
 
+// --------------------------------------------------------------------- batched adjoint
+size_t batch_adj_bytes() { return sizeof(BatchAdjExp); }
+
+void batch_pack_adjoint(const BatchAdjHost *in, uint32_t n, void *dst)
+{
+    BatchAdjExp *d = static_cast<BatchAdjExp *>(dst);
+    for (uint32_t i = 0; i < n; ++i) d[i] = BatchAdjExp{in[i].lut, in[i].dmu, in[i].deps, in[i].ref_log10, 0u};
+}
+
+namespace {
+bool adjoint_dispatch(const BatchShape &s, const BatchExp *exps, const BatchAdjExp *adj, const uint2 *items,
+                      uint32_t n_items, uint32_t *counter, double *grad, int bins, int grid, size_t smem,
+                      cudaStream_t st, cudaError_t &e, int *occ)
+{
+    return batch_shapes_a_adjoint(s, exps, adj, items, n_items, counter, grad, bins, grid, smem, st, e, occ) ||
+           batch_shapes_b_adjoint(s, exps, adj, items, n_items, counter, grad, bins, grid, smem, st, e, occ) ||
+           batch_shapes_c_adjoint(s, exps, adj, items, n_items, counter, grad, bins, grid, smem, st, e, occ) ||
+           batch_shapes_d_adjoint(s, exps, adj, items, n_items, counter, grad, bins, grid, smem, st, e, occ) ||
+           batch_shapes_e_adjoint(s, exps, adj, items, n_items, counter, grad, bins, grid, smem, st, e, occ);
+}
+}  // namespace
+
+int batch_adjoint_blocks_per_sm(const BatchShape &s, int bins)
+{
+    BatchShape t = s;
+    t.lut_smem = 1;
+    const size_t smem = batch_smem_bytes(t, (uint32_t)bins);
+    int occ = 0;
+    cudaError_t e = cudaSuccess;
+    if (!adjoint_dispatch(t, nullptr, nullptr, nullptr, 0, nullptr, nullptr, bins, 0, smem, nullptr, e, &occ) ||
+        e != cudaSuccess)
+        return 0;
+    return occ;
+}
+
+cudaError_t launch_batch_adjoint(const BatchShape &s, const void *d_exps, const void *d_adj, const uint2 *d_items,
+                                 uint32_t n_items, uint32_t *d_counter, double *grad, int bins, int grid,
+                                 cudaStream_t st)
+{
+    BatchShape t = s;
+    t.lut_smem = 1;
+    const size_t smem = batch_smem_bytes(t, (uint32_t)bins);
+    cudaError_t e = cudaSuccess;
+    if (adjoint_dispatch(t, static_cast<const BatchExp *>(d_exps), static_cast<const BatchAdjExp *>(d_adj), d_items,
+                         n_items, d_counter, grad, bins, grid, smem, st, e, nullptr))
+        return e;
+    return cudaErrorInvalidValue;
+}
+
 }  // namespace twisty

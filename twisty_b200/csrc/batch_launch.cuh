@@ -23,6 +23,17 @@ struct BatchExp {
     uint32_t pad;
 };
 
+// Per-experiment inputs of the batched adjoint replay beyond BatchExp (whose table is then the
+// linear table, staged in shared memory): the float table and its derivatives with respect to
+// mu_s and eps, and the reference the path weights are scaled by.
+struct BatchAdjExp {
+    const float *lut;
+    const float *dmu;
+    const float *deps;
+    float ref_log10;
+    uint32_t pad;
+};
+
 // Each returns false when the shape is not among its own; else launches (sets e) or reports
 // the occupancy (sets occ).
 bool batch_shapes_a_launch(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items,
@@ -40,6 +51,22 @@ bool batch_shapes_d_launch(const BatchShape &s, const BatchExp *exps, const uint
 bool batch_shapes_e_launch(const BatchShape &s, const BatchExp *exps, const uint2 *items, uint32_t n_items,
                            uint32_t *counter, ChainOut *out, int bins, int grid, size_t smem, cudaStream_t st,
                            cudaError_t &e);   // 4 x {20, 24, 28, 32}
+// The adjoint replay of the same shapes (table staged, exact blend, clamping).
+bool batch_shapes_a_adjoint(const BatchShape &s, const BatchExp *exps, const BatchAdjExp *adj, const uint2 *items,
+                            uint32_t n_items, uint32_t *counter, double *grad, int bins, int grid, size_t smem,
+                            cudaStream_t st, cudaError_t &e, int *occ);
+bool batch_shapes_b_adjoint(const BatchShape &s, const BatchExp *exps, const BatchAdjExp *adj, const uint2 *items,
+                            uint32_t n_items, uint32_t *counter, double *grad, int bins, int grid, size_t smem,
+                            cudaStream_t st, cudaError_t &e, int *occ);
+bool batch_shapes_c_adjoint(const BatchShape &s, const BatchExp *exps, const BatchAdjExp *adj, const uint2 *items,
+                            uint32_t n_items, uint32_t *counter, double *grad, int bins, int grid, size_t smem,
+                            cudaStream_t st, cudaError_t &e, int *occ);
+bool batch_shapes_d_adjoint(const BatchShape &s, const BatchExp *exps, const BatchAdjExp *adj, const uint2 *items,
+                            uint32_t n_items, uint32_t *counter, double *grad, int bins, int grid, size_t smem,
+                            cudaStream_t st, cudaError_t &e, int *occ);
+bool batch_shapes_e_adjoint(const BatchShape &s, const BatchExp *exps, const BatchAdjExp *adj, const uint2 *items,
+                            uint32_t n_items, uint32_t *counter, double *grad, int bins, int grid, size_t smem,
+                            cudaStream_t st, cudaError_t &e, int *occ);
 bool batch_shapes_a_occ(const BatchShape &s, size_t smem, int &occ);
 bool batch_shapes_b_occ(const BatchShape &s, size_t smem, int &occ);
 bool batch_shapes_c_occ(const BatchShape &s, size_t smem, int &occ);
@@ -89,6 +116,70 @@ __global__ void __launch_bounds__(MAXT, 1) batch_kernel(const BatchExp *__restri
                                                                             out + e.out_offset, ma);
         __syncthreads();
     }
+}
+
+// Adjoint replay of a batch: the forward pass's work items, each CTA staging its experiment's
+// linear table and running the chains in the adjoint mode of the chain body (exact blend,
+// curvatures recomputed, nothing stored per step); per-chain gradient sums go to
+// grad[(out_offset + chain) * 6 ...].
+template <int G, int SPL, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1) batch_adjoint_kernel(const BatchExp *__restrict__ exps,
+                                                                const BatchAdjExp *__restrict__ adj,
+                                                                const uint2 *__restrict__ items, uint32_t n_items,
+                                                                uint32_t *__restrict__ counter,
+                                                                double *__restrict__ grad, int bins)
+{
+    extern __shared__ float4 smem4[];
+    __shared__ uint32_t s_item;
+    const int tab_f4 = (bins + 1) / 2;
+    unsigned char *s_state = reinterpret_cast<unsigned char *>(smem4 + tab_f4);
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t q = lane / G, j = lane % G;
+    constexpr int CPW = 32 / G;
+    using Lay = Layout<G, SPL>;
+    unsigned char *wb = s_state + (size_t)warp * Lay::WARP_BYTES;
+    float *s_len = reinterpret_cast<float *>(s_state + (size_t)(blockDim.x >> 5) * Lay::WARP_BYTES);
+    const Planes st{reinterpret_cast<float2 *>(wb), reinterpret_cast<float *>(wb + Lay::XY_BYTES), s_len};
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1u);
+        __syncthreads();
+        const uint32_t item = s_item;
+        if (item >= n_items) break;
+        const uint2 it = items[item];
+        const BatchExp &e = exps[it.x];
+        const BatchAdjExp &a = adj[it.x];
+        stage_table(smem4, e.tab, bins);
+        fill_lengths(s_len, e.init_seg, e.spec.n_segments, G * SPL);
+        __syncthreads();
+        ModeArgs ma{};
+        ma.log10_abs = e.log10_abs;
+        ma.lin = e.lin;
+        ma.lut = a.lut;
+        ma.dmu = a.dmu;
+        ma.deps = a.deps;
+        ma.ref_log10 = a.ref_log10;
+        ma.grad = grad + (size_t)e.out_offset * 6;
+        const uint32_t chain = it.y + warp * CPW + q;
+        chain_body<G, SPL, true, true, false, kModeAdjoint>(e.spec, e.kc, e.init_seg,
+                                                            reinterpret_cast<const float2 *>(smem4), st, q * G, j,
+                                                            chain, chain < e.spec.n_chains, nullptr, ma);
+        __syncthreads();
+    }
+}
+
+template <int G, int SPL>
+cudaError_t batch_adjoint_g(const BatchShape &s, const BatchExp *exps, const BatchAdjExp *adj, const uint2 *items,
+                            uint32_t n_items, uint32_t *counter, double *grad, int bins, int grid, size_t smem,
+                            cudaStream_t st, int *occ)
+{
+    constexpr int MAXT = batch_max_threads(G, SPL);
+    if (s.warps * 32 > MAXT) return cudaErrorInvalidConfiguration;
+    auto kern = batch_adjoint_kernel<G, SPL, MAXT>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, s.warps * 32, smem);
+    kern<<<grid, s.warps * 32, smem, st>>>(exps, adj, items, n_items, counter, grad, bins);
+    return cudaGetLastError();
 }
 
 template <int G, int SPL, bool EXACT, bool LS, bool CL, bool SP>
@@ -148,6 +239,11 @@ cudaError_t batch_g(const BatchShape &s, const BatchExp *exps, const uint2 *item
     if (s.group == GG && s.spl == SS) {   \
         e = batch_g<GG, SS>(s, exps, items, n_items, counter, out, bins, grid, smem, st); \
         return true;                       \
+    }
+#define TWISTY_BATCH_SHAPE_ADJ(GG, SS)                                                                  \
+    if (s.group == GG && s.spl == SS) {                                                                 \
+        e = batch_adjoint_g<GG, SS>(s, exps, adj, items, n_items, counter, grad, bins, grid, smem, st, occ); \
+        return true;                                                                                    \
     }
 #define TWISTY_BATCH_SHAPE_OCC(GG, SS)   \
     if (s.group == GG && s.spl == SS) { \

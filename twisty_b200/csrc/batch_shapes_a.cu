@@ -60,4 +60,33 @@ bool batch_shapes_a_occ(const BatchShape &s, size_t smem, int &occ)
     return false;
 }
 
+bool batch_shapes_a_adjoint(const BatchShape &s, const BatchExp *exps, const BatchAdjExp *adj, const uint2 *items,
+                            uint32_t n_items, uint32_t *counter, double *grad, int bins, int grid, size_t smem,
+                            cudaStream_t st, cudaError_t &e, int *occ)
+{
+    TWISTY_BATCH_SHAPE_ADJ(4, 4)
+    TWISTY_BATCH_SHAPE_ADJ(4, 8)
+    TWISTY_BATCH_SHAPE_ADJ(4, 2)
+    TWISTY_BATCH_SHAPE_ADJ(4, 3)
+    TWISTY_BATCH_SHAPE_ADJ(4, 5)
+    TWISTY_BATCH_SHAPE_ADJ(4, 9)
+    TWISTY_BATCH_SHAPE_ADJ(4, 16)
+    TWISTY_BATCH_SHAPE_ADJ(4, 17)
+    TWISTY_BATCH_SHAPE_ADJ(1, 8)
+    TWISTY_BATCH_SHAPE_ADJ(1, 12)
+    TWISTY_BATCH_SHAPE_ADJ(8, 9)
+    TWISTY_BATCH_SHAPE_ADJ(8, 17)
+    TWISTY_BATCH_SHAPE_ADJ(16, 17)
+    TWISTY_BATCH_SHAPE_ADJ(8, 2)
+    TWISTY_BATCH_SHAPE_ADJ(8, 4)
+    TWISTY_BATCH_SHAPE_ADJ(8, 8)
+    TWISTY_BATCH_SHAPE_ADJ(8, 12)
+    TWISTY_BATCH_SHAPE_ADJ(8, 16)
+    TWISTY_BATCH_SHAPE_ADJ(16, 4)
+    TWISTY_BATCH_SHAPE_ADJ(16, 8)
+    TWISTY_BATCH_SHAPE_ADJ(16, 12)
+    TWISTY_BATCH_SHAPE_ADJ(16, 16)
+    return false;
+}
+
 }  // namespace twisty

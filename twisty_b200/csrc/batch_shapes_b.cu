@@ -30,4 +30,18 @@ bool batch_shapes_b_occ(const BatchShape &s, size_t smem, int &occ)
     return false;
 }
 
+bool batch_shapes_b_adjoint(const BatchShape &s, const BatchExp *exps, const BatchAdjExp *adj, const uint2 *items,
+                            uint32_t n_items, uint32_t *counter, double *grad, int bins, int grid, size_t smem,
+                            cudaStream_t st, cudaError_t &e, int *occ)
+{
+    TWISTY_BATCH_SHAPE_ADJ(32, 4)
+    TWISTY_BATCH_SHAPE_ADJ(32, 8)
+    TWISTY_BATCH_SHAPE_ADJ(32, 12)
+    TWISTY_BATCH_SHAPE_ADJ(32, 17)
+    TWISTY_BATCH_SHAPE_ADJ(32, 16)
+    TWISTY_BATCH_SHAPE_ADJ(32, 24)
+    TWISTY_BATCH_SHAPE_ADJ(32, 32)
+    return false;
+}
+
 }  // namespace twisty

@@ -22,4 +22,14 @@ bool batch_shapes_c_occ(const BatchShape &s, size_t smem, int &occ)
     return false;
 }
 
+bool batch_shapes_c_adjoint(const BatchShape &s, const BatchExp *exps, const BatchAdjExp *adj, const uint2 *items,
+                            uint32_t n_items, uint32_t *counter, double *grad, int bins, int grid, size_t smem,
+                            cudaStream_t st, cudaError_t &e, int *occ)
+{
+    TWISTY_BATCH_SHAPE_ADJ(16, 20)
+    TWISTY_BATCH_SHAPE_ADJ(32, 20)
+    TWISTY_BATCH_SHAPE_ADJ(32, 28)
+    return false;
+}
+
 }  // namespace twisty

@@ -24,4 +24,15 @@ bool batch_shapes_e_occ(const BatchShape &s, size_t smem, int &occ)
     return false;
 }
 
+bool batch_shapes_e_adjoint(const BatchShape &s, const BatchExp *exps, const BatchAdjExp *adj, const uint2 *items,
+                            uint32_t n_items, uint32_t *counter, double *grad, int bins, int grid, size_t smem,
+                            cudaStream_t st, cudaError_t &e, int *occ)
+{
+    TWISTY_BATCH_SHAPE_ADJ(4, 20)
+    TWISTY_BATCH_SHAPE_ADJ(4, 24)
+    TWISTY_BATCH_SHAPE_ADJ(4, 28)
+    TWISTY_BATCH_SHAPE_ADJ(4, 32)
+    return false;
+}
+
 }  // namespace twisty

@@ -93,7 +93,52 @@ __global__ void __launch_bounds__(1024) grad_reduce_kernel(const double *__restr
     }
 }
 
+// One CTA per range of chains: the sums of their 6 gradient entries (the batched adjoint).
+__global__ void __launch_bounds__(256) grad_reduce_segments_kernel(const double *__restrict__ g,
+                                                                   const uint2 *__restrict__ ranges,
+                                                                   double *__restrict__ out)
+{
+    __shared__ double red[6][8];
+    const uint2 r = ranges[blockIdx.x];
+    double a[6] = {0, 0, 0, 0, 0, 0};
+    for (uint32_t i = threadIdx.x; i < r.y; i += blockDim.x)
+        for (int k = 0; k < 6; ++k) a[k] += g[(size_t)(r.x + i) * 6 + k];
+    for (int k = 0; k < 6; ++k)
+        for (int o = 16; o > 0; o >>= 1) a[k] += __shfl_xor_sync(FULL, a[k], o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0)
+        for (int k = 0; k < 6; ++k) red[k][w] = a[k];
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double v = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) v += red[threadIdx.x][i];
+        out[(size_t)blockIdx.x * 6 + threadIdx.x] = v;
+    }
+}
+
+__global__ void f64_to_f32_kernel(const double *__restrict__ in, float *__restrict__ out, size_t n)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = (float)in[i];
+}
+
 }  // namespace
+
+cudaError_t launch_grad_reduce_segments(const double *grad_chains, const uint2 *ranges, uint32_t n, double *out,
+                                        cudaStream_t st)
+{
+    if (n == 0) return cudaSuccess;
+    grad_reduce_segments_kernel<<<n, 256, 0, st>>>(grad_chains, ranges, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_f64_to_f32(const double *in, float *out, size_t n, cudaStream_t st)
+{
+    if (n == 0) return cudaSuccess;
+    const size_t blocks = std::min<size_t>((n + 255) / 256, 148 * 16);
+    f64_to_f32_kernel<<<(unsigned)blocks, 256, 0, st>>>(in, out, n);
+    return cudaGetLastError();
+}
 
 
 bool comp_table_needs_clamp(float inv_ds, const LutMetaF &m)

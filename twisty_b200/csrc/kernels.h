@@ -194,6 +194,28 @@ int batch_blocks_per_sm(const BatchShape &s, int bins);
 cudaError_t launch_batch(const BatchShape &s, const void *d_exps, const uint2 *d_items, uint32_t n_items,
                          uint32_t *d_counter, ChainOut *out, int bins, int grid, cudaStream_t st);
 
+// Batched adjoint replay: the experiments packed as for launch_batch (their table being the
+// linear one, staged in shared memory by every shape), plus per experiment the float table,
+// its derivatives d/d(mu_s) and d/d(eps) (device, float[bins] each) and the log10 reference
+// the path weights are scaled by (the experiment's forward log10 sum without absorption).
+// grad[(out_offset + chain) * 6 + k]: the chain's sums of 10^(w - ref) d log10 w / d (mu_s,
+// eps, receiver x, y, z) and of 10^(w - ref).
+struct BatchAdjHost {
+    const float *lut, *dmu, *deps;
+    float ref_log10;
+};
+size_t batch_adj_bytes();
+void batch_pack_adjoint(const BatchAdjHost *in, uint32_t n, void *dst);
+int batch_adjoint_blocks_per_sm(const BatchShape &s, int bins);
+cudaError_t launch_batch_adjoint(const BatchShape &s, const void *d_exps, const void *d_adj, const uint2 *d_items,
+                                 uint32_t n_items, uint32_t *d_counter, double *grad, int bins, int grid,
+                                 cudaStream_t st);
+// Per range ranges[x] = (first chain, count): the sums over its chains of the 6 gradient entries.
+cudaError_t launch_grad_reduce_segments(const double *grad_chains, const uint2 *ranges, uint32_t n, double *out,
+                                        cudaStream_t st);
+// Element-wise double -> float.
+cudaError_t launch_f64_to_f32(const double *in, float *out, size_t n, cudaStream_t st);
+
 // ----------------------------------------------------------- reduction (chain_plain.cu)
 cudaError_t launch_reduce(const ChainOut *chains, uint32_t n, ReduceOut *out, cudaStream_t st);
 // One reduction per range: ranges[x] = (first chain, count) -> out[x].

@@ -82,15 +82,24 @@ uint64_t seed_of(uint32_t s)
 }  // namespace
 
 // Device buffers of batched runs, kept by the context so that repeated batches of the same
-// size allocate nothing (DevBuf::ensure only grows).
+// size allocate nothing (DevBuf::ensure only grows). The last row serves the batched adjoint.
 struct BatchBufs {
     DevBuf specs, lut64, lut32, fix, lin, steps, nsegs, lf, ok, init_seg, exps, items, counters, chain_out, ranges, red;
+    DevBuf dmu, deps, d64mu, d64eps, d64scratch, adj_exps, adj_aux, adj_items, adj_counters, grad, grad_sum;
     void release()
     {
         DevBuf *all[] = {&specs, &lut64, &lut32, &fix, &lin, &steps, &nsegs, &lf, &ok, &init_seg, &exps, &items,
-                         &counters, &chain_out, &ranges, &red};
+                         &counters, &chain_out, &ranges, &red, &dmu, &deps, &d64mu, &d64eps, &d64scratch,
+                         &adj_exps, &adj_aux, &adj_items, &adj_counters, &grad, &grad_sum};
         for (DevBuf *b : all) b->release();
     }
+};
+
+// Outputs of the batched adjoint (twisty_adjoint_batch); every pointer nullable but grad.
+struct BatchAdjointOut {
+    double *grad;     // [n][5]
+    double *total;    // [3]
+    double *timing;   // [2]
 };
 
 struct twisty_ctx {
@@ -880,6 +889,7 @@ twisty_status twisty_update_params(twisty_ctx *ctx, const twisty_params *p)
         ctx->p = *p;
         ctx->prepared = false;
         ctx->launched = false;
+        ctx->lut_ready = false;   // the next run builds its tables again
     });
 }
 
@@ -1190,7 +1200,8 @@ std::string exp_msg(uint32_t e, const std::string &m)
 //  4. one segmented FP64 reduction (a CTA per experiment).
 // Steps 3-4 are captured once as a CUDA graph and replayed `iters` times; results are those
 // of the last replay, perturb_ms the mean replay time.
-void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_t iters, twisty_result *res)
+void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_t iters, twisty_result *res,
+               const BatchAdjointOut *adj = nullptr)
 {
     const double t0 = now_ms();
     const twisty_params p = ctx->p;
@@ -1208,7 +1219,13 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
     if (n > 65535u) fail(TWISTY_ERR_INVALID_ARGUMENT, "at most 65535 experiments per batch");
     set_device(ctx);
     for (uint32_t e = 0; e < n; ++e) std::memset(&res[e], 0, sizeof(twisty_result));
-    if (n == 0) return;
+    if (n == 0) {
+        if (adj && adj->total) {
+            adj->total[0] = -std::numeric_limits<double>::infinity();
+            adj->total[1] = adj->total[2] = std::numeric_limits<double>::quiet_NaN();
+        }
+        return;
+    }
     const uint32_t bins = p.num_curvature_steps;
     cudaStream_t st = ctx->stream;
 
@@ -1541,6 +1558,164 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
         r.weighting_ms = 0.0;
         r.total_ms = total_ms;
     }
+    if (!adj) return;
+
+    // ---- adjoint replay of the same chains (twisty_adjoint_batch)
+    // derivative tables d/d(mu_s), d/d(eps) in FP64 on the device: one per experiment, or one per
+    // table of the multi-ds set the experiments take theirs from
+    const uint32_t ntab = multi ? ctx->multi.n : n;
+    ck(B.dmu.ensure(sizeof(float) * (size_t)bins * ntab), "alloc derivative tables");
+    ck(B.deps.ensure(sizeof(float) * (size_t)bins * ntab), "alloc derivative tables");
+    ck(B.d64mu.ensure(sizeof(double) * (size_t)bins * ntab), "alloc derivative tables");
+    ck(B.d64eps.ensure(sizeof(double) * (size_t)bins * ntab), "alloc derivative tables");
+    ck(B.d64scratch.ensure(sizeof(double) * (size_t)bins), "alloc derivative tables");
+    std::vector<char> tab_used(ntab, multi ? 0 : 1);
+    if (multi)
+        for (uint32_t e = 0; e < n; ++e) tab_used[eh[e].multi_index] = 1;
+    ck(cudaEventRecord(ctx->ev[0], st), "event");
+    for (uint32_t t = 0; t < ntab; ++t) {
+        if (!tab_used[t]) continue;
+        LutBuildSpec s{};
+        if (multi) {
+            s.mu = p.mu;
+            s.eps = p.eps;
+            s.scatter = p.scatter;
+            s.min_bound = p.min_bound;
+            s.max_bound = p.max_bound;
+            s.bias = p.bias;
+            s.num_steps_int = p.num_steps_int;
+            s.bins = bins;
+            s.ds = ctx->multi.ds[t];
+            s.min_k = 0.0f;
+            s.step = ctx->multi.meta[t].step;
+            s.step64 = ((2.0 / (double)s.ds) * 1.01) / (double)(bins - 1);
+        } else {
+            s = specs[t];
+        }
+        s.faithful = 0;
+        s.derivatives = 1;
+        ck(launch_lut_build(s, B.d64scratch.as<double>(), B.d64mu.as<double>() + (size_t)t * bins,
+                            B.d64eps.as<double>() + (size_t)t * bins, st),
+           "derivative tables");
+    }
+    ck(launch_f64_to_f32(B.d64mu.as<double>(), B.dmu.as<float>(), (size_t)bins * ntab, st), "derivative tables");
+    ck(launch_f64_to_f32(B.d64eps.as<double>(), B.deps.as<float>(), (size_t)bins * ntab, st), "derivative tables");
+    ck(cudaEventRecord(ctx->ev[1], st), "event");
+
+    // experiments for the replay: the linear table staged in shared memory, the exact blend
+    std::vector<BatchExpHost> bx(n);
+    std::vector<BatchAdjHost> ax(n);
+    struct AdjBucket {
+        BatchShape shape;
+        std::vector<uint2> items;
+        int grid = 0;
+        uint32_t item_off = 0;
+    };
+    std::vector<AdjBucket> abk;
+    for (uint32_t e = 0; e < n; ++e) {
+        const ExpHost &h = eh[e];
+        bx[e] = bh[e];
+        bx[e].lf = LogFixed{0.0, 0.0, 0, 0};
+        bx[e].tab = B.lin.as<float2>() + (size_t)e * bins;
+        const uint32_t t = multi ? h.multi_index : e;
+        const double log10_abs = std::log10(h.spec.absorption_factor);
+        const bool ok = red[e].valid > 0 && std::isfinite(red[e].log10_sum);
+        ax[e] = BatchAdjHost{B.lut32.as<float>() + (size_t)e * bins, B.dmu.as<float>() + (size_t)t * bins,
+                             B.deps.as<float>() + (size_t)t * bins,
+                             ok ? (float)(red[e].log10_sum - (double)(h.N - 1) * log10_abs) : 0.0f};
+        if (h.spec.n_chains == 0) continue;
+        BatchShape sh{h.t.group, h.t.spl, std::min(h.t.warps_per_block, batch_max_threads(h.t.group, h.t.spl) / 32), 1, 1,
+                      1, 0};
+        while (sh.warps > 4 && batch_smem_bytes(sh, bins) > kSmemCap) sh.warps -= 4;
+        if (batch_smem_bytes(sh, bins) > kSmemCap)
+            fail(TWISTY_ERR_UNSUPPORTED, exp_msg(e, "weight table too large to stage for the adjoint"));
+        AdjBucket *bk = nullptr;
+        for (AdjBucket &b : abk)
+            if (b.shape.group == sh.group && b.shape.spl == sh.spl && b.shape.warps == sh.warps) bk = &b;
+        if (!bk) {
+            abk.push_back(AdjBucket{});
+            abk.back().shape = sh;
+            bk = &abk.back();
+        }
+        const uint32_t cpb = (uint32_t)batch_chains_per_block(sh);
+        for (uint32_t c0 = 0; c0 < h.spec.n_chains; c0 += cpb) bk->items.push_back(make_uint2(e, c0));
+    }
+    std::vector<uint2> aitems;
+    for (AdjBucket &bk : abk) {
+        std::stable_sort(bk.items.begin(), bk.items.end(), [&](const uint2 &a, const uint2 &b) {
+            const ExpHost &x = eh[a.x], &y = eh[b.x];
+            return (double)(x.spec.burn_in + x.spec.steps) * x.N > (double)(y.spec.burn_in + y.spec.steps) * y.N;
+        });
+        bk.item_off = (uint32_t)aitems.size();
+        aitems.insert(aitems.end(), bk.items.begin(), bk.items.end());
+        const int occ = batch_adjoint_blocks_per_sm(bk.shape, (int)bins);
+        if (occ <= 0) fail(TWISTY_ERR_UNSUPPORTED, "batched adjoint shape cannot launch");
+        bk.grid = (int)std::min<uint64_t>((uint64_t)ctx->sm_count * occ, std::max<size_t>(1, bk.items.size()));
+    }
+    std::vector<unsigned char> pexp(batch_exp_bytes() * n), padj(batch_adj_bytes() * n);
+    batch_pack_experiments(bx.data(), n, pexp.data());
+    batch_pack_adjoint(ax.data(), n, padj.data());
+    ck(B.adj_exps.ensure(pexp.size()), "alloc adjoint");
+    ck(B.adj_aux.ensure(padj.size()), "alloc adjoint");
+    ck(B.adj_items.ensure(sizeof(uint2) * std::max<size_t>(1, aitems.size())), "alloc adjoint");
+    ck(B.adj_counters.ensure(sizeof(uint32_t) * std::max<size_t>(1, abk.size())), "alloc adjoint");
+    ck(B.grad.ensure(sizeof(double) * 6 * std::max<uint32_t>(1, total_chains)), "alloc adjoint");
+    ck(B.grad_sum.ensure(sizeof(double) * 6 * n), "alloc adjoint");
+    ck(cudaMemcpyAsync(B.adj_exps.p, pexp.data(), pexp.size(), cudaMemcpyHostToDevice, st), "upload adjoint");
+    ck(cudaMemcpyAsync(B.adj_aux.p, padj.data(), padj.size(), cudaMemcpyHostToDevice, st), "upload adjoint");
+    if (!aitems.empty())
+        ck(cudaMemcpyAsync(B.adj_items.p, aitems.data(), sizeof(uint2) * aitems.size(), cudaMemcpyHostToDevice, st),
+           "upload adjoint");
+    ck(cudaMemsetAsync(B.adj_counters.p, 0, sizeof(uint32_t) * std::max<size_t>(1, abk.size()), st), "memset");
+    ck(cudaMemsetAsync(B.grad.p, 0, sizeof(double) * 6 * std::max<uint32_t>(1, total_chains), st), "memset");
+    ck(cudaEventRecord(ctx->ev[2], st), "event");
+    for (size_t b = 0; b < abk.size(); ++b)
+        ck(launch_batch_adjoint(abk[b].shape, B.adj_exps.p, B.adj_aux.p, B.adj_items.as<uint2>() + abk[b].item_off,
+                                (uint32_t)abk[b].items.size(), B.adj_counters.as<uint32_t>() + b, B.grad.as<double>(),
+                                (int)bins, abk[b].grid, st),
+           "batched adjoint kernel");
+    ck(launch_grad_reduce_segments(B.grad.as<double>(), B.ranges.as<uint2>(), n, B.grad_sum.as<double>(), st),
+       "adjoint reduction");
+    ck(cudaEventRecord(ctx->ev[3], st), "event");
+    std::vector<double> gs(6 * (size_t)n);
+    ck(cudaMemcpyAsync(gs.data(), B.grad_sum.p, sizeof(double) * gs.size(), cudaMemcpyDeviceToHost, st), "read gradients");
+    ck(cudaStreamSynchronize(st), "batched adjoint");
+    float t_tab = 0.f, t_rep = 0.f;
+    ck(cudaEventElapsedTime(&t_tab, ctx->ev[0], ctx->ev[1]), "event time");
+    ck(cudaEventElapsedTime(&t_rep, ctx->ev[2], ctx->ev[3]), "event time");
+    ctx->kernels_per_launch = (uint32_t)abk.size() + 1;
+    // per experiment: the weight-averaged path gradients; d/d(sigma) = d/d(eps) 2 sigma
+    double m = -std::numeric_limits<double>::infinity();
+    for (uint32_t e = 0; e < n; ++e)
+        if (res[e].total_paths && std::isfinite(res[e].log10_weight)) m = std::max(m, res[e].log10_weight);
+    double wsum = 0.0, tmu = 0.0, tsig = 0.0;
+    for (uint32_t e = 0; e < n; ++e) {
+        const double *g = gs.data() + 6 * (size_t)e;
+        double *o = adj->grad + 5 * (size_t)e;
+        if (!(g[5] > 0.0)) {
+            for (int k = 0; k < 5; ++k) o[k] = std::numeric_limits<double>::quiet_NaN();
+            continue;
+        }
+        const double sigma = std::sqrt((double)ex[e].eps);
+        o[0] = g[0] / g[5];
+        o[1] = g[1] / g[5] * 2.0 * sigma;
+        o[2] = g[2] / g[5];
+        o[3] = g[3] / g[5];
+        o[4] = g[4] / g[5];
+        const double w = std::pow(10.0, res[e].log10_weight - m);
+        wsum += w;
+        tmu += w * o[0];
+        tsig += w * o[1];
+    }
+    if (adj->total) {
+        adj->total[0] = wsum > 0.0 ? m + std::log10(wsum) : -std::numeric_limits<double>::infinity();
+        adj->total[1] = wsum > 0.0 ? tmu / wsum : std::numeric_limits<double>::quiet_NaN();
+        adj->total[2] = wsum > 0.0 ? tsig / wsum : std::numeric_limits<double>::quiet_NaN();
+    }
+    if (adj->timing) {
+        adj->timing[0] = t_tab;
+        adj->timing[1] = t_rep;
+    }
 }
 
 }  // namespace
@@ -1550,6 +1725,18 @@ twisty_status twisty_run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uin
 {
     if (!ctx || (!ex && n) || (!res && n)) return TWISTY_ERR_INVALID_ARGUMENT;
     return guard(ctx, [&] { run_batch(ctx, ex, n, iterations ? iterations : 1, res); });
+}
+
+twisty_status twisty_adjoint_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, twisty_result *res,
+                                   double *grad, double total[3], double timing_ms[2])
+{
+    if (!ctx || (!ex && n) || (!res && n) || (!grad && n)) return TWISTY_ERR_INVALID_ARGUMENT;
+    return guard(ctx, [&] {
+        if (ctx->p.lut_mode != TWISTY_LUT_FP64 && ctx->p.lut_mode != TWISTY_LUT_MULTI_DS)
+            fail(TWISTY_ERR_UNSUPPORTED, "the batched adjoint builds its derivative tables in FP64 (lut_mode FP64 or MULTI_DS)");
+        const BatchAdjointOut out{grad, total, timing_ms};
+        run_batch(ctx, ex, n, 1, res, &out);
+    });
 }
 
 twisty_status twisty_export_paths(twisty_ctx *ctx, const twisty_bc *bc, const char *dir, uint64_t max_paths, float *pos,
@@ -1678,6 +1865,26 @@ twisty_status twisty_adjoint(twisty_ctx *ctx, const twisty_bc *bc, const twisty_
             throw;
         }
         dtab.release(); dg.release(); dout.release();
+    });
+}
+
+twisty_status twisty_chain_results(twisty_ctx *ctx, double *log10_sum, uint64_t *valid, uint32_t n_chains)
+{
+    if (!ctx || (!log10_sum && n_chains)) return TWISTY_ERR_INVALID_ARGUMENT;
+    return guard(ctx, [&] {
+        if (!ctx->launched) fail(TWISTY_ERR_INVALID_ARGUMENT, "no pass has run on this context");
+        if (n_chains != ctx->spec.n_chains) fail(TWISTY_ERR_INVALID_ARGUMENT, "n_chains must be the pass's chain count");
+        if (n_chains == 0) return;
+        set_device(ctx);
+        std::vector<ChainOut> h(n_chains);
+        ck(cudaEventSynchronize(ctx->ev[2]), "sync");
+        ck(cudaMemcpyAsync(h.data(), ctx->chain_out.p, sizeof(ChainOut) * n_chains, cudaMemcpyDeviceToHost, ctx->stream),
+           "read chain results");
+        ck(cudaStreamSynchronize(ctx->stream), "read chain results");
+        for (uint32_t i = 0; i < n_chains; ++i) {
+            log10_sum[i] = h[i].log10_sum + ctx->log10_norm;
+            if (valid) valid[i] = h[i].valid;
+        }
     });
 }
 

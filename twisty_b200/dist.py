@@ -1,10 +1,18 @@
-"""Sharding one experiment over ranks (one process per GPU) and combining the results.
+"""Sharding over ranks (one process per GPU) and combining the results.
 
-Every rank runs the same experiment with a disjoint range of chain ids
-(``chain_offset = rank * chains``), so the chains of all ranks are independent draws of the
-same Markov process and the estimate is their sum. The one exchange step combines the
-per-rank results: log10 sums by log-sum-exp, absolute standard errors in quadrature (the
-ranks' chains are independent), counts by addition. It moves 6 doubles per rank.
+One experiment (the single-run forms): every rank runs the same experiment with a disjoint
+range of chain ids (``chain_offset = rank * chains``), so the chains of all ranks are
+independent draws of the same Markov process and the estimate is their sum. The one exchange
+step combines the per-rank results: log10 sums by log-sum-exp, absolute standard errors in
+quadrature (the ranks' chains are independent), counts by addition. It moves 6 doubles per
+rank.
+
+A batch (the receiver / pixel grids): experiments are independent, so the ranks split the
+batch by experiment (``partition_experiments``: each rank takes a contiguous range holding its
+share of the work, balanced by paths x segments) and run their own sub-batch with the
+experiments' own Philox stream ids and bootstrap seeds (those of the full batch, so that the
+result of an experiment does not depend on the number of ranks); ``gather_partitioned`` then
+puts every experiment's result on every rank in one all-gather of n x 7 doubles.
 """
 from __future__ import annotations
 
@@ -62,3 +70,54 @@ def all_combine_batch(results, group=None, device=None) -> list:
     dist.all_gather(parts, t, group=group)
     rows = [p.tolist() for p in parts]
     return [combine([rows[r][i] for r in range(len(rows))]) for i in range(t.shape[0])]
+
+
+def partition_experiments(experiments, rank: int, world: int) -> list:
+    """Indices of the experiments rank `rank` of `world` runs: a contiguous range, cut where the
+    running cost (paths x segments) crosses rank / world of the total, so every rank's share is
+    within one experiment's cost of total / world. Contiguous, so that the sub-batch keeps the
+    full batch's stream ids and bootstrap seeds: run it with experiment_id and bootstrap_seed
+    raised by its first index (twisty_run_batch numbers experiments from those)."""
+    cost = [float(x.paths) * float(x.num_segments) for x in experiments]
+    total = sum(cost)
+
+    def cut(r):
+        if r <= 0:
+            return 0
+        if r >= world:
+            return len(cost)
+        target = total * r / world
+        acc = 0.0
+        for i, c in enumerate(cost):
+            if acc + 0.5 * c > target:
+                return i
+            acc += c
+        return len(cost)
+
+    return list(range(cut(rank), cut(rank + 1)))
+
+
+def gather_partitioned(results, indices, n: int, group=None, device=None) -> list:
+    """Every experiment's result tuple (FIELDS) on every rank: each rank passes the results of
+    the experiments it ran (`indices`, from partition_experiments) and receives a list of n
+    dicts, experiment i's from the rank that ran it."""
+    import torch
+    import torch.distributed as dist
+    t = torch.full((n, len(FIELDS) + 1), float("nan"), dtype=torch.float64, device=device)
+    for i, r in zip(indices, results):
+        t[i, :len(FIELDS)] = torch.tensor(local_tuple(r), dtype=torch.float64)
+        t[i, len(FIELDS)] = 1.0   # row present
+    parts = [torch.empty_like(t) for _ in range(dist.get_world_size(group))]
+    dist.all_gather(parts, t, group=group)
+    out = [None] * n
+    for p in parts:
+        rows = p.tolist()
+        for i in range(n):
+            if rows[i][len(FIELDS)] == 1.0:
+                if out[i] is not None:
+                    raise RuntimeError(f"experiment {i} ran on two ranks")
+                out[i] = combine([rows[i][:len(FIELDS)]])
+    missing = [i for i in range(n) if out[i] is None]
+    if missing:
+        raise RuntimeError(f"experiments {missing[:8]} ran on no rank")
+    return out
