@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define TWISTY_B200_ABI_VERSION 1
+#define TWISTY_B200_ABI_VERSION 2
 
 /* Status codes. The reference reports failures by std::nullopt
  * (FullExperimentRunnerOptimalPerturbOptimized_GPU.cu:153-157), std::runtime_error
@@ -137,6 +137,11 @@ typedef struct twisty_params {
        through L1), 1 = shared memory (fewer warps per CTA for large tables), 2 = through L1.
        Path export, the adjoint, receiver-shifted and incremental runs always stage it. */
     uint32_t comp_table_memory;
+    /* error against FP64, measured (no reference counterpart): K > 0 replays the pass's first K
+       chains (the same proposals) in the FP64 form after the pass and reports the relative
+       difference of their summed weights in twisty_result.fp64_rel_error. The FP64 form runs a
+       chain per thread, so the check costs about K / (all chains) of a pass of that form; 0 = off. */
+    uint32_t fp64_check_chains;
 } twisty_params;
 
 /* ExperimentRunner::ExperimentResults (Twisty/ExperimentRunner.h:73-82). */
@@ -163,6 +168,17 @@ typedef struct twisty_result {
        linear table. */
     uint32_t table_form;
     uint32_t steep_bins;
+    /* The result's error against FP64 (no reference counterpart). weight_error_bound: bound on
+       |log10 w - log10 w_FP64| of every path's weight for the path's own curvatures and table,
+       from the form's arithmetic -- fixed-point tables (N-1)(2^-s + secant error), exact-blend
+       tables (N-1) 4e-7, the plain form's float blend (N-1) 2.6e-8, 0 for the FP64 form; it does
+       not cover the FP32 trajectory's drift from the FP64 one, which fp64_rel_error measures:
+       |W_K / W_K,FP64 - 1| over the first fp64_check_chains chains replayed in the FP64 form
+       (NaN when the check is off). */
+    double weight_error_bound;
+    double fp64_rel_error;
+    uint32_t fp64_check_chains;
+    uint32_t reserved;
 } twisty_result;
 
 enum {

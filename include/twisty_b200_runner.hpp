@@ -116,6 +116,9 @@ class ExperimentRunner {
         long long setupExperimentMs = 0;
         long long perturbExperimentMs = 0;
         long long weightingExperimentMs = 0;
+        // error against FP64 (twisty_result.weight_error_bound, .fp64_rel_error)
+        double weightErrorBoundLog10 = 0.0;
+        double fp64RelError = NAN;
     };
 
     // ExperimentRunner::ParseExperimentParamsFromConfig (Twisty/ExperimentRunner.cpp:48-177).
@@ -212,6 +215,8 @@ class ExperimentRunner {
         out.setupExperimentMs = (long long)r.setup_ms;
         out.perturbExperimentMs = (long long)r.perturb_ms;
         out.weightingExperimentMs = (long long)r.weighting_ms;
+        out.weightErrorBoundLog10 = r.weight_error_bound;
+        out.fp64RelError = r.fp64_rel_error;
         return out;
     }
 

@@ -42,14 +42,16 @@ def test_struct_sizes_match_header(tmp_path):
     src = str(tmp_path / "abi_probe.c")
     with open(src, "w") as f:
         f.write('#include "twisty_b200.h"\n#include <stdio.h>\n#include <stddef.h>\n'
-                'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(twisty_params), sizeof(twisty_bc),'
+                'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(twisty_params), sizeof(twisty_bc),'
                 ' sizeof(twisty_result), sizeof(twisty_lut_info), sizeof(twisty_experiment),'
-                ' offsetof(twisty_params, eval_end_shift), offsetof(twisty_result, total_ms)); return 0;}\n')
+                ' offsetof(twisty_params, eval_end_shift), offsetof(twisty_result, total_ms),'
+                ' offsetof(twisty_params, fp64_check_chains), offsetof(twisty_result, fp64_rel_error)); return 0;}\n')
     exe = src[:-2]
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), src, "-o", exe], check=True)
     sizes = list(map(int, subprocess.run([exe], capture_output=True, text=True).stdout.split()))
     assert sizes == [C.sizeof(_abi.Params), C.sizeof(_abi.BC), C.sizeof(_abi.Result), C.sizeof(_abi.LutInfo),
-                     C.sizeof(_abi.Experiment), _abi.Params.eval_end_shift.offset, _abi.Result.total_ms.offset]
+                     C.sizeof(_abi.Experiment), _abi.Params.eval_end_shift.offset, _abi.Result.total_ms.offset,
+                     _abi.Params.fp64_check_chains.offset, _abi.Result.fp64_rel_error.offset]
 
 
 def test_params_init_reference_defaults():
@@ -229,3 +231,54 @@ def test_benchmark_curve_fixture_is_the_bootstrappers():
     pos = T.bootstrap_curve(T.default_params(num_segments=256, bootstrap_seed=7), bench.workload_bc(T))
     fix = np.load(bench.BENCH_CURVE)
     assert np.array_equal(pos.view(np.uint32), fix.view(np.uint32))
+
+
+CALLER = r'''
+// A caller of the reference's runner API, compiled against the drop-in header unchanged.
+#include "twisty_b200_runner.hpp"
+#include <cstdio>
+#include <fstream>
+#include <sstream>
+using namespace twisty::b200;
+int main(int, char **argv)
+{
+    std::ifstream f(argv[1]);
+    std::stringstream buf;
+    buf << f.rdbuf();
+    BoundaryConditions bc;
+    std::string err;
+    ExperimentRunner::ExperimentParameters params = ExperimentRunner::ParseExperimentParamsFromConfig(buf.str(), false, &bc, &err);
+    if (!err.empty()) { std::printf("parse error %s\n", err.c_str()); return 2; }
+    std::printf("segments %u paths %llu skip %llu scatter %g eps %g bins %u end %g %g %g arclength %g\n",
+                params.numSegmentsPerCurve, (unsigned long long)params.numPathsInExperiment,
+                (unsigned long long)params.numPathsToSkip, params.weightingParameters.scatter,
+                params.weightingParameters.eps, params.weightingParameters.numCurvatureSteps,
+                bc.m_endPos.x, bc.m_endPos.y, bc.m_endPos.z, bc.arclength);
+    FullExperimentRunnerOptimalPerturb runner(params);
+    std::optional<ExperimentRunner::ExperimentResults> r = runner.RunExperiment(bc);
+    if (!r) { std::printf("no results: %s\n", runner.lastError().c_str()); return 3; }
+    std::printf("log10 %.17g paths %llu\n", r->experimentWeightLog10, (unsigned long long)r->totalPathsGenerated);
+    return 0;
+}
+'''
+
+
+def test_cpp_runner_header_compiles_for_a_reference_style_caller(tmp_path):
+    """include/twisty_b200_runner.hpp, the C++ face of the drop-in: a caller written against the
+    reference's runner API (ParseExperimentParamsFromConfig, FullExperimentRunnerOptimalPerturb,
+    RunExperiment -> std::optional<ExperimentResults>) compiles warning-free and links against the
+    library; without a GPU, RunExperiment returns no result and says why (no CPU fallback)."""
+    src = tmp_path / "caller.cpp"
+    src.write_text(CALLER)
+    exe = tmp_path / "caller"
+    lib_dir = os.path.dirname(_abi.LIB_PATH)
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"), str(src),
+                    "-o", str(exe), "-L", lib_dir, "-ltwisty_b200", f"-Wl,-rpath,{lib_dir}"], check=True)
+    cfg = tmp_path / "cfg.json"
+    cfg.write_text(json.dumps(reference_config(pathsToGenerate=1000)))
+    r = subprocess.run([str(exe), str(cfg)], capture_output=True, text=True, env={**os.environ, "CUDA_VISIBLE_DEVICES": ""})
+    assert "segments 66 paths 1000 skip 1000 scatter 10 eps 0.01 bins 1024 end 8 0 0 arclength 10" in r.stdout, r.stdout
+    if r.returncode == 3:
+        assert "no CUDA device" in r.stdout
+    else:   # a GPU is visible after all
+        assert r.returncode == 0 and "paths 1000" in r.stdout

@@ -1,5 +1,7 @@
 """Parity of the CUDA library (through its C ABI) with the oracle and the reference's own
 golden outputs. Every test here needs a B200 (marker `gpu`)."""
+import math
+
 import numpy as np
 import pytest
 
@@ -283,6 +285,33 @@ def test_chain_sums_match_reference_runner_n258(form):
     pval = mannwhitneyu(mine, ref, alternative="two-sided").pvalue
     assert pval > 1e-3, (pval, np.median(mine), np.median(ref), ref.min(), ref.max())
     assert ref.min() <= np.median(mine) <= ref.max()
+
+
+def test_results_state_their_error_against_fp64():
+    """Every result carries a bound of its arithmetic against FP64 (per path, for the path's own
+    curvatures), and with fp64_check_chains the measured relative error of its first chains'
+    weight against the FP64 form replaying them: equal to what a separate FP64 run of the same
+    chains gives."""
+    chains, steps = 512, 200
+    kw = dict(perturb_seed=99, num_chains=chains, paths_to_generate=chains * steps, paths_to_skip=100,
+              max_sub_chain=32, max_angle=0.1, lut_mode=T.LUT_FP64)
+    p, N, S = lut_params("D", form=T.FORM_COMPENSATED, fp64_check_chains=chains, **kw)
+    with T.Context(p) as ctx:
+        ctx.set_initial_curve(np.load("tests/golden/boot_66.npy"))
+        a = ctx.run(geom_bc(N, S))
+        assert ctx.kernels_per_launch() == 3
+    p64, _, _ = lut_params("D", form=T.FORM_FP64, **kw)
+    with T.Context(p64) as ctx:
+        ctx.set_initial_curve(np.load("tests/golden/boot_66.npy"))
+        b = ctx.run(geom_bc(N, S))
+    assert a.fp64_check_chains == chains and math.isnan(b.fp64_rel_error) and b.weight_error_bound == 0.0
+    assert a.fp64_rel_error == pytest.approx(abs(10 ** (a.log10_weight - b.log10_weight) - 1), rel=1e-6, abs=1e-12)
+    assert a.fp64_rel_error < 1e-4
+    assert 0.0 < a.weight_error_bound < 1e-4
+    pp, _, _ = lut_params("D", form=T.FORM_PLAIN_FP32, **kw)
+    with T.Context(pp) as ctx:
+        c = ctx.run(geom_bc(N, S))
+    assert math.isnan(c.fp64_rel_error) and c.weight_error_bound == pytest.approx(65 * 2.6e-8)
 
 
 def test_runs_are_deterministic_and_split_api_matches():

@@ -355,6 +355,8 @@ class ExperimentResults:
     normalizerLog10: float = 0.0
     relStdError: float = float("nan")
     clampedCurvatures: int = 0
+    weightErrorBoundLog10: float = 0.0    # per-path log10 error bound of the arithmetic vs FP64
+    fp64RelError: float = float("nan")     # measured on the fp64_check_chains chains (NaN: off)
 
     @property
     def avgPathWeightLog10(self) -> float:
@@ -410,7 +412,7 @@ class FullExperimentRunnerOptimalPerturb:
         r = self._context().run(boundaryConditions.to_c())
         return ExperimentResults(r.log10_weight, r.total_paths, r.failed_paths, r.total_ms, r.setup_ms,
                                  r.perturb_ms, r.weighting_ms, r.log10_normalizer, r.rel_std_error,
-                                 r.clamped_curvatures)
+                                 r.clamped_curvatures, r.weight_error_bound, r.fp64_rel_error)
 
     run_experiment = RunExperiment
 

@@ -81,6 +81,7 @@ class Params(C.Structure):
         ("comp_warps", C.c_uint32),
         ("incremental_resync", C.c_uint32),
         ("comp_table_memory", C.c_uint32),
+        ("fp64_check_chains", C.c_uint32),
     ]
 
 
@@ -101,6 +102,10 @@ class Result(C.Structure):
         ("weighting_ms", C.c_double),
         ("table_form", C.c_uint32),
         ("steep_bins", C.c_uint32),
+        ("weight_error_bound", C.c_double),
+        ("fp64_rel_error", C.c_double),
+        ("fp64_check_chains", C.c_uint32),
+        ("reserved", C.c_uint32),
     ]
 
 

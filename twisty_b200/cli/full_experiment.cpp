@@ -105,6 +105,8 @@ int main(int argc, char **argv)
     ofs << "\tWeighting time (ms) " << format_duration(r.weightingExperimentMs) << std::endl;
     ofs << "\tTotal experiment weight log10: " << std::setprecision(15) << r.experimentWeightLog10 << std::endl;
     ofs << "\tRelative standard error: " << r.relStdError << std::endl;
+    ofs << "\tPer-path log10 error bound vs FP64: " << r.weightErrorBoundLog10 << std::endl;
+    ofs << "\tRelative error vs FP64 (checked chains): " << r.fp64RelError << std::endl;
     ofs << std::endl;
     return 0;
 }

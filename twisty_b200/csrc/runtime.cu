@@ -146,6 +146,9 @@ struct twisty_ctx {
     std::vector<float> user_curve;
     std::vector<float> init_pos_host;
     DevBuf init_pos, init_seg, state, chain_out, partials, reduce_out, norm_scratch;
+    DevBuf check_state, check_out;   // the FP64 replay of the first chains (fp64_check_chains)
+    uint32_t check_chains = 0;
+    double check_meta[3] = {0.0, 0.0, 0.0};   // min_k, max_k, step of the FP64 replay's table
     uint32_t kernels_per_launch = 0;
     bool launched = false;
     BatchBufs batch;
@@ -561,8 +564,24 @@ void prepare(twisty_ctx *ctx, const twisty_bc *bcp)
     } else {
         ck(ctx->partials.ensure(sizeof(double2) * comp_blocks(c, ctx->tuning)), "alloc block partials");
     }
+    // the FP64 replay of the first chains, on the double copy of the run's table
+    ctx->check_chains = (p.form != TWISTY_FORM_FP64) ? std::min<uint32_t>(p.fp64_check_chains, c.n_chains) : 0u;
+    if (ctx->check_chains) {
+        ck(ctx->check_state.ensure(sizeof(double) * 3 * (size_t)(N + 1) * ctx->check_chains), "alloc FP64 check");
+        ck(ctx->check_out.ensure(sizeof(ChainOut) * ctx->check_chains), "alloc FP64 check");
+        if (p.lut_mode == TWISTY_LUT_FP64) {
+            const double max_k = (2.0 / (double)ds) * 1.01;
+            ctx->check_meta[0] = 0.0;
+            ctx->check_meta[1] = max_k;
+            ctx->check_meta[2] = max_k / (double)(p.num_curvature_steps - 1);
+        } else {
+            ctx->check_meta[0] = ctx->meta.min_k;
+            ctx->check_meta[1] = ctx->meta.max_k;
+            ctx->check_meta[2] = ctx->meta.step;
+        }
+    }
     ck(cudaStreamSynchronize(st), "prepare");
-    ctx->kernels_per_launch = c.n_chains ? 2 : 0;
+    ctx->kernels_per_launch = c.n_chains ? 2 + (ctx->check_chains ? 1 : 0) : 0;
     ctx->bc = bc;
     ctx->prepared = true;
     ctx->launched = false;
@@ -596,6 +615,18 @@ void launch(twisty_ctx *ctx, cudaStream_t st)
     ck(cudaEventRecord(ctx->ev[1], st), "event");
     if (c.n_chains) ck(launch_reduce(ctx->chain_out.as<ChainOut>(), c.n_chains, ctx->reduce_out.as<ReduceOut>(), st), "reduction");
     ck(cudaEventRecord(ctx->ev[2], st), "event");
+    if (ctx->check_chains) {
+        // after the timed pass: the first chains again, in FP64, on the same proposals
+        ChainSpec ck64 = c;
+        ck64.n_chains = ctx->check_chains;
+        ck64.last_steps = (ctx->check_chains == c.n_chains) ? c.last_steps : c.steps;
+        ck64.incr_resync = 0;
+        ck(launch_fp64_chains(ck64, ctx->init_pos.as<float>(), ctx->check_state.as<double>(), ctx->lut64.as<double>(),
+                              ctx->check_meta[0], ctx->check_meta[1], ctx->check_meta[2],
+                              (int32_t)ctx->p.num_curvature_steps, ctx->check_out.as<ChainOut>(), st),
+           "FP64 check");
+    }
+    ck(cudaEventRecord(ctx->ev[3], st), "event");
     ctx->launched = true;
 }
 
@@ -629,10 +660,37 @@ void collect(twisty_ctx *ctx, twisty_result *res)
     res->perturb_ms = a;
     res->weighting_ms = b;
     res->table_form = TWISTY_TABLE_NONE;
+    const double segs = (double)(ctx->spec.n_segments - 1);
     if (ctx->p.form == TWISTY_FORM_COMPENSATED) {
         const bool exact = ctx->tuning.exact_blend || ctx->lf.inv_scale == 0.0 || ctx->spec.has_eval_shift;
         res->table_form = exact ? TWISTY_TABLE_EXACT_BLEND : ctx->lf.wide ? TWISTY_TABLE_FIXED_WIDE : TWISTY_TABLE_FIXED_NARROW;
         res->steep_bins = exact ? 0u : (uint32_t)ctx->lf.steep;
+        // per segment: entry and correction each rounded to 2^-(s+1), plus the secant's error;
+        // exact blend: the float blend and the hardware log2 (under 4e-7 in log10 together)
+        res->weight_error_bound = exact ? segs * 4e-7 : segs * (ctx->lf.inv_scale + ctx->secant_err);
+    } else if (ctx->p.form == TWISTY_FORM_PLAIN_FP32) {
+        res->weight_error_bound = segs * 2.6e-8;   // the blend rounded to float: 2^-24 relative
+    }
+    res->fp64_rel_error = std::numeric_limits<double>::quiet_NaN();
+    res->fp64_check_chains = ctx->check_chains;
+    if (ctx->check_chains) {
+        const uint32_t K = ctx->check_chains;
+        std::vector<ChainOut> a(K), b(K);
+        ck(cudaEventSynchronize(ctx->ev[3]), "sync");
+        ck(cudaMemcpyAsync(a.data(), ctx->chain_out.p, sizeof(ChainOut) * K, cudaMemcpyDeviceToHost, ctx->stream), "read");
+        ck(cudaMemcpyAsync(b.data(), ctx->check_out.p, sizeof(ChainOut) * K, cudaMemcpyDeviceToHost, ctx->stream), "read");
+        ck(cudaStreamSynchronize(ctx->stream), "read FP64 check");
+        auto lse = [](const std::vector<ChainOut> &v) {
+            double m = -std::numeric_limits<double>::infinity();
+            for (const ChainOut &o : v) m = std::max(m, o.log10_sum);
+            if (!std::isfinite(m)) return m;
+            double sum = 0.0;
+            for (const ChainOut &o : v)
+                if (std::isfinite(o.log10_sum)) sum += std::pow(10.0, o.log10_sum - m);
+            return m + std::log10(sum);
+        };
+        const double la = lse(a), lb = lse(b);
+        if (std::isfinite(la) && std::isfinite(lb)) res->fp64_rel_error = std::fabs(std::pow(10.0, la - lb) - 1.0);
     }
 }
 
@@ -869,7 +927,7 @@ void twisty_destroy(twisty_ctx *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     DevBuf *bufs[] = {&ctx->lut64, &ctx->lut32, &ctx->fixtab, &ctx->lintab, &ctx->dmus, &ctx->deps, &ctx->lutaux,
                       &ctx->init_pos, &ctx->init_seg, &ctx->state, &ctx->chain_out, &ctx->partials, &ctx->reduce_out,
-                      &ctx->norm_scratch, &ctx->multi.dev};
+                      &ctx->norm_scratch, &ctx->multi.dev, &ctx->check_state, &ctx->check_out};
     for (DevBuf *b : bufs) b->release();
     ctx->batch.release();
     for (auto &e : ctx->ev)
@@ -1039,6 +1097,9 @@ twisty_status twisty_run_msegment(twisty_ctx *ctx, const twisty_bc *bc, twisty_r
         const double log10_sum = sum > 0 ? m + std::log10(sum) : -std::numeric_limits<double>::infinity();
         res->log10_mean_weight = valid ? log10_sum - std::log10((double)valid) + log10_norm : -std::numeric_limits<double>::infinity();
         res->log10_weight = res->log10_mean_weight;   // the estimator is the mean (ExperimentBase.cpp:1378-1381)
+        res->fp64_rel_error = std::numeric_limits<double>::quiet_NaN();
+        res->weight_error_bound = (double)(N - 1) * (p.form == TWISTY_FORM_PLAIN_FP32 ? 2.6e-8
+                                                     : ctx->exact_blend ? 4e-7 : ctx->lf.inv_scale + ctx->secant_err);
         res->rel_std_error = sum > 0 ? std::sqrt(var) / sum : NAN;
         res->total_paths = valid;
         res->failed_paths = failed;
@@ -1554,6 +1615,9 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
         const bool fixed = bh[e].lf.inv_scale != 0.0;
         r.table_form = fixed ? (lf[e].wide ? TWISTY_TABLE_FIXED_WIDE : TWISTY_TABLE_FIXED_NARROW) : TWISTY_TABLE_EXACT_BLEND;
         r.steep_bins = fixed ? (uint32_t)lf[e].steep : 0u;
+        // the device-built tables keep every secant within 1e-7 (steeper bins are re-weighed exactly)
+        r.weight_error_bound = (double)(eh[e].N - 1) * (fixed ? bh[e].lf.inv_scale + 1e-7 : 4e-7);
+        r.fp64_rel_error = std::numeric_limits<double>::quiet_NaN();
         r.perturb_ms = sum_ms / iters;
         r.weighting_ms = 0.0;
         r.total_ms = total_ms;
