@@ -71,7 +71,7 @@ size_t batch_adj_bytes() { return sizeof(BatchAdjExp); }
 void batch_pack_adjoint(const BatchAdjHost *in, uint32_t n, void *dst)
 {
     BatchAdjExp *d = static_cast<BatchAdjExp *>(dst);
-    for (uint32_t i = 0; i < n; ++i) d[i] = BatchAdjExp{in[i].lut, in[i].dmu, in[i].deps, in[i].ref_log10, 0u};
+    for (uint32_t i = 0; i < n; ++i) d[i] = BatchAdjExp{in[i].dtab, in[i].ref_log10, 0u};
 }
 
 namespace {

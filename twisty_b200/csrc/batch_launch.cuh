@@ -24,12 +24,10 @@ struct BatchExp {
 };
 
 // Per-experiment inputs of the batched adjoint replay beyond BatchExp (whose table is then the
-// linear table, staged in shared memory): the float table and its derivatives with respect to
-// mu_s and eps, and the reference the path weights are scaled by.
+// linear table, staged in shared memory): the derivative tables with respect to mu_s and eps
+// (launch_deriv_tables layout) and the reference the path weights are scaled by.
 struct BatchAdjExp {
-    const float *lut;
-    const float *dmu;
-    const float *deps;
+    const float4 *dtab;
     float ref_log10;
     uint32_t pad;
 };
@@ -154,9 +152,7 @@ __global__ void __launch_bounds__(MAXT, 1) batch_adjoint_kernel(const BatchExp *
         ModeArgs ma{};
         ma.log10_abs = e.log10_abs;
         ma.lin = e.lin;
-        ma.lut = a.lut;
-        ma.dmu = a.dmu;
-        ma.deps = a.deps;
+        ma.dtab = a.dtab;
         ma.ref_log10 = a.ref_log10;
         ma.grad = grad + (size_t)e.out_offset * 6;
         const uint32_t chain = it.y + warp * CPW + q;

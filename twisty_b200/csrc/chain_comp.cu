@@ -116,10 +116,17 @@ __global__ void __launch_bounds__(256) grad_reduce_segments_kernel(const double 
     }
 }
 
-__global__ void f64_to_f32_kernel(const double *__restrict__ in, float *__restrict__ out, size_t n)
+// Derivative tables in the linear table's form: per bin (dmu_i, dmu_{i+1} - dmu_i, deps_i,
+// deps_{i+1} - deps_i), the last bin's changes 0; tables of `bins` entries back to back.
+__global__ void deriv_table_kernel(const double *__restrict__ dmu, const double *__restrict__ deps, uint32_t bins,
+                                   size_t n, float4 *__restrict__ out)
 {
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        out[i] = (float)in[i];
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const bool last = (i % bins) == bins - 1;
+        const float m0 = (float)dmu[i], e0 = (float)deps[i];
+        const float m1 = last ? m0 : (float)dmu[i + 1], e1 = last ? e0 : (float)deps[i + 1];
+        out[i] = make_float4(m0, m1 - m0, e0, e1 - e0);
+    }
 }
 
 }  // namespace
@@ -132,11 +139,13 @@ cudaError_t launch_grad_reduce_segments(const double *grad_chains, const uint2 *
     return cudaGetLastError();
 }
 
-cudaError_t launch_f64_to_f32(const double *in, float *out, size_t n, cudaStream_t st)
+cudaError_t launch_deriv_tables(const double *dmu, const double *deps, uint32_t bins, uint32_t n_tables, float4 *out,
+                                cudaStream_t st)
 {
+    const size_t n = (size_t)bins * n_tables;
     if (n == 0) return cudaSuccess;
     const size_t blocks = std::min<size_t>((n + 255) / 256, 148 * 16);
-    f64_to_f32_kernel<<<(unsigned)blocks, 256, 0, st>>>(in, out, n);
+    deriv_table_kernel<<<(unsigned)blocks, 256, 0, st>>>(dmu, deps, bins, n, out);
     return cudaGetLastError();
 }
 
@@ -289,14 +298,12 @@ cudaError_t launch_comp_export(const ChainSpec &c, const CompTuning &t, const fl
 }
 
 cudaError_t launch_comp_adjoint(const ChainSpec &c, const CompTuning &t, const float *init_seg, const float2 *lintab,
-                                LutMetaF m, const float *lut, const float *dmu, const float *deps, float ref_log10,
-                                double *grad_chains, double *grad_out, cudaStream_t st)
+                                LutMetaF m, const float4 *dtab, float ref_log10, double *grad_chains, double *grad_out,
+                                cudaStream_t st)
 {
     ModeArgs ma{};
     ma.log10_abs = log10(c.absorption_factor);
-    ma.lut = lut;
-    ma.dmu = dmu;
-    ma.deps = deps;
+    ma.dtab = dtab;
     ma.ref_log10 = ref_log10;
     ma.grad = grad_chains;
     cudaError_t e = launch_mode(kModeAdjoint, c, t, init_seg, lintab, lintab, m, nullptr, nullptr, ma,

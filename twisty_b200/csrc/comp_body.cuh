@@ -84,10 +84,9 @@ struct ModeArgs {
     float *exp_pos;      // [chains][steps][N+1][3]
     double *exp_w;       // [chains][steps] log10 weights (absorption included, normaliser not)
     float x0[3];
-    // adjoint
-    const float *lut;    // float table
-    const float *dmu;    // d table / d mu_s
-    const float *deps;   // d table / d eps
+    // adjoint: per bin (dL/dmu_s, its change to the next bin, dL/deps, its change to the next
+    // bin) -- the derivative tables in the linear table's form, one 16-byte load per segment
+    const float4 *dtab;
     float ref_log10;     // log10 of the forward sum of path weights (normaliser and absorption excluded)
     double *grad;        // [chains][6]: d/dmu_s, d/deps, d/dx, d/dy, d/dz (log10 units), sum of weights
 };
@@ -363,8 +362,7 @@ enum { kModeForward = 0, kModeExport = 1, kModeAdjoint = 2 };
 // the table's linear interpolant taken half a bin to the left, whose slope at fractional bin r
 // is (L_{J+1} - L_J) / step with J = floor(r - 1/2); divided by the weight itself.
 __device__ __forceinline__ void receiver_grad(const float t3[3], const float t2[3], const float t1[3], float len2,
-                                              const float *__restrict__ lut, const CompConsts &k, float inv_ds,
-                                              float g[3])
+                                              const float2 *lin, const CompConsts &k, float inv_ds, float g[3])
 {
     const float r2 = 1.0f / len2;  // d t2 / d v2 = (I - t2 t2^T) / |v2|
     g[0] = g[1] = g[2] = 0.f;
@@ -378,13 +376,13 @@ __device__ __forceinline__ void receiver_grad(const float t3[3], const float t2[
         float r = fmaf(dn, k.kscale, k.roff);
         if (r < 0.f) r = 0.f;
         if (r > k.rmax) continue;  // clamped: flat
+        // the linear table (L_i, L_{i+1} - L_i): the blend at r and the slope of bin J
         const int32_t L = min((int32_t)r, k.bins - 1);
-        const int32_t R = min(L + 1, k.bins - 1);
-        const float lv = __ldg(lut + L), rv = __ldg(lut + R);
+        const float2 e = lin[L];
         const float dd = (r - (float)L) * k.step;
-        const float blend = fmaf(dd, rv - lv, lv);
+        const float blend = fmaf(dd, e.y, e.x);
         const int32_t J = min(max((int32_t)floorf(r - 0.5f), 0), k.bins - 2);
-        const float sl = __ldg(lut + J + 1) - __ldg(lut + J);
+        const float sl = lin[J].y;
         const float dlog = sl / (k.step * blend) * kInvLn10;  // d log10 w / d kappa
         const float dk = dlog * inv_ds * sign / dn;                  // d kappa / d t = inv_ds d/|d|
         const float dt = d[0] * t2[0] + d[1] * t2[1] + d[2] * t2[2];
@@ -766,22 +764,22 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
 
             double w;
             if (MODE == kModeAdjoint) {
-                // log10 weight and d/d(mu_s), d/d(eps) of this lane's segments (exact blend)
+                // log10 weight and d/d(mu_s), d/d(eps) of this lane's segments (exact blend): the
+                // blend from the staged linear table, the derivative blends from one 16-byte load
                 float s = 0.f, cc = 0.f, gmu = 0.f, geps = 0.f;
                 for_curvatures<G, SPL, false>(j, N, tan_smem, next_smem, [&](uint32_t, float qq, bool valid) {
                     float r = sqrt_approx(qq) + kc.roff;   // scaled tangents: the root is the bin index
                     if (r < 0.f) r = 0.f;
                     if (r > kc.rmax) r = kc.rmax;
                     const int32_t L = min((int32_t)r, kc.bins - 1);
-                    const int32_t Rb = min(L + 1, kc.bins - 1);
                     const float d = (r - (float)L) * kc.step;
-                    const float lv = __ldg(ma.lut + L), rv = __ldg(ma.lut + Rb);
-                    const float v = fmaf(d, rv - lv, lv);
+                    const float2 e = s_tab[L];
+                    const float4 dv = __ldg(ma.dtab + L);
+                    const float v = fmaf(d, e.y, e.x);
                     kahan_add(s, cc, valid ? __log2f(v) * kLog10_2 : 0.0f);
-                    const float ml = __ldg(ma.dmu + L), mr = __ldg(ma.dmu + Rb);
-                    const float el = __ldg(ma.deps + L), er = __ldg(ma.deps + Rb);
-                    gmu += valid ? fmaf(d, mr - ml, ml) / v : 0.0f;
-                    geps += valid ? fmaf(d, er - el, el) / v : 0.0f;
+                    const float iv = __fdividef(1.0f, v);
+                    gmu += valid ? fmaf(d, dv.y, dv.x) * iv : 0.0f;
+                    geps += valid ? fmaf(d, dv.w, dv.z) * iv : 0.0f;
                 });
                 float hi = s, lo = -cc;
                 group_sum_pair<G>(hi, lo);
@@ -792,7 +790,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                     const float4 v2 = load_rec((N - 2) / SPL, (N - 2) % SPL);
                     const float4 v1 = load_rec((N - 1) / SPL, (N - 1) % SPL);
                     const float t3[3] = {v3.x, v3.y, v3.z}, t2[3] = {v2.x, v2.y, v2.z}, t1[3] = {v1.x, v1.y, v1.z};
-                    receiver_grad(t3, t2, t1, v2.w, ma.lut, kc, c.inv_ds, g3);
+                    receiver_grad(t3, t2, t1, v2.w, s_tab, kc, c.inv_ds, g3);
                 }
                 if (active && !isnan(w)) {
                     const float wt = exp2f((float)(w - (double)ma.ref_log10) * kLog2_10);

@@ -152,10 +152,10 @@ cudaError_t launch_comp_export(const ChainSpec &c, const CompTuning &t, const fl
                                ChainOut *out, cudaStream_t st, LogFixed lf = LogFixed{0.0, 0.0});
 // Adjoint replay: per chain the weight-averaged gradients of log10 w with respect to
 // (mu_s, eps, receiver x, y, z) and the sum of the weights w/10^ref_log10, reduced over
-// chains into grad_out[6].
+// chains into grad_out[6]. dtab: the derivative tables as launch_deriv_tables lays them out.
 cudaError_t launch_comp_adjoint(const ChainSpec &c, const CompTuning &t, const float *init_seg, const float2 *lintab,
-                                LutMetaF m, const float *lut, const float *dmu, const float *deps, float ref_log10,
-                                double *grad_chains, double *grad_out, cudaStream_t st);
+                                LutMetaF m, const float4 *dtab, float ref_log10, double *grad_chains, double *grad_out,
+                                cudaStream_t st);
 
 // Batched persistent form: one launch runs the chains of many experiments that share a
 // kernel shape. Work items (experiment, first chain) are taken from *d_counter (zeroed by
@@ -195,13 +195,13 @@ cudaError_t launch_batch(const BatchShape &s, const void *d_exps, const uint2 *d
                          uint32_t *d_counter, ChainOut *out, int bins, int grid, cudaStream_t st);
 
 // Batched adjoint replay: the experiments packed as for launch_batch (their table being the
-// linear one, staged in shared memory by every shape), plus per experiment the float table,
-// its derivatives d/d(mu_s) and d/d(eps) (device, float[bins] each) and the log10 reference
-// the path weights are scaled by (the experiment's forward log10 sum without absorption).
+// linear one, staged in shared memory by every shape), plus per experiment its derivative
+// tables (device, launch_deriv_tables layout) and the log10 reference the path weights are
+// scaled by (the experiment's forward log10 sum without absorption).
 // grad[(out_offset + chain) * 6 + k]: the chain's sums of 10^(w - ref) d log10 w / d (mu_s,
 // eps, receiver x, y, z) and of 10^(w - ref).
 struct BatchAdjHost {
-    const float *lut, *dmu, *deps;
+    const float4 *dtab;
     float ref_log10;
 };
 size_t batch_adj_bytes();
@@ -213,8 +213,10 @@ cudaError_t launch_batch_adjoint(const BatchShape &s, const void *d_exps, const 
 // Per range ranges[x] = (first chain, count): the sums over its chains of the 6 gradient entries.
 cudaError_t launch_grad_reduce_segments(const double *grad_chains, const uint2 *ranges, uint32_t n, double *out,
                                         cudaStream_t st);
-// Element-wise double -> float.
-cudaError_t launch_f64_to_f32(const double *in, float *out, size_t n, cudaStream_t st);
+// Derivative tables d/d(mu_s), d/d(eps) (double, n_tables x bins) in the form the adjoint reads:
+// per bin float4 (dmu_i, dmu_{i+1} - dmu_i, deps_i, deps_{i+1} - deps_i).
+cudaError_t launch_deriv_tables(const double *dmu, const double *deps, uint32_t bins, uint32_t n_tables, float4 *out,
+                                cudaStream_t st);
 
 // ----------------------------------------------------------- reduction (chain_plain.cu)
 cudaError_t launch_reduce(const ChainOut *chains, uint32_t n, ReduceOut *out, cudaStream_t st);

@@ -85,11 +85,11 @@ uint64_t seed_of(uint32_t s)
 // size allocate nothing (DevBuf::ensure only grows). The last row serves the batched adjoint.
 struct BatchBufs {
     DevBuf specs, lut64, lut32, fix, lin, steps, nsegs, lf, ok, init_seg, exps, items, counters, chain_out, ranges, red;
-    DevBuf dmu, deps, d64mu, d64eps, d64scratch, adj_exps, adj_aux, adj_items, adj_counters, grad, grad_sum;
+    DevBuf dtab, d64mu, d64eps, d64scratch, adj_exps, adj_aux, adj_items, adj_counters, grad, grad_sum;
     void release()
     {
         DevBuf *all[] = {&specs, &lut64, &lut32, &fix, &lin, &steps, &nsegs, &lf, &ok, &init_seg, &exps, &items,
-                         &counters, &chain_out, &ranges, &red, &dmu, &deps, &d64mu, &d64eps, &d64scratch,
+                         &counters, &chain_out, &ranges, &red, &dtab, &d64mu, &d64eps, &d64scratch,
                          &adj_exps, &adj_aux, &adj_items, &adj_counters, &grad, &grad_sum};
         for (DevBuf *b : all) b->release();
     }
@@ -1628,8 +1628,7 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
     // derivative tables d/d(mu_s), d/d(eps) in FP64 on the device: one per experiment, or one per
     // table of the multi-ds set the experiments take theirs from
     const uint32_t ntab = multi ? ctx->multi.n : n;
-    ck(B.dmu.ensure(sizeof(float) * (size_t)bins * ntab), "alloc derivative tables");
-    ck(B.deps.ensure(sizeof(float) * (size_t)bins * ntab), "alloc derivative tables");
+    ck(B.dtab.ensure(sizeof(float4) * (size_t)bins * ntab), "alloc derivative tables");
     ck(B.d64mu.ensure(sizeof(double) * (size_t)bins * ntab), "alloc derivative tables");
     ck(B.d64eps.ensure(sizeof(double) * (size_t)bins * ntab), "alloc derivative tables");
     ck(B.d64scratch.ensure(sizeof(double) * (size_t)bins), "alloc derivative tables");
@@ -1662,8 +1661,8 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
                             B.d64eps.as<double>() + (size_t)t * bins, st),
            "derivative tables");
     }
-    ck(launch_f64_to_f32(B.d64mu.as<double>(), B.dmu.as<float>(), (size_t)bins * ntab, st), "derivative tables");
-    ck(launch_f64_to_f32(B.d64eps.as<double>(), B.deps.as<float>(), (size_t)bins * ntab, st), "derivative tables");
+    ck(launch_deriv_tables(B.d64mu.as<double>(), B.d64eps.as<double>(), bins, ntab, B.dtab.as<float4>(), st),
+       "derivative tables");
     ck(cudaEventRecord(ctx->ev[1], st), "event");
 
     // experiments for the replay: the linear table staged in shared memory, the exact blend
@@ -1684,8 +1683,7 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
         const uint32_t t = multi ? h.multi_index : e;
         const double log10_abs = std::log10(h.spec.absorption_factor);
         const bool ok = red[e].valid > 0 && std::isfinite(red[e].log10_sum);
-        ax[e] = BatchAdjHost{B.lut32.as<float>() + (size_t)e * bins, B.dmu.as<float>() + (size_t)t * bins,
-                             B.deps.as<float>() + (size_t)t * bins,
+        ax[e] = BatchAdjHost{B.dtab.as<float4>() + (size_t)t * bins,
                              ok ? (float)(red[e].log10_sum - (double)(h.N - 1) * log10_abs) : 0.0f};
         if (h.spec.n_chains == 0) continue;
         BatchShape sh{h.t.group, h.t.spl, std::min(h.t.warps_per_block, batch_max_threads(h.t.group, h.t.spl) / 32), 1, 1,
@@ -1891,28 +1889,19 @@ twisty_status twisty_adjoint(twisty_ctx *ctx, const twisty_bc *bc, const twisty_
         const float ds = bc->arclength / (float)N;
         build_tables(ctx, ds, true);
         const uint32_t bins = ctx->p.num_curvature_steps;
-        std::vector<double> hmu(bins), heps(bins);
-        ck(cudaMemcpyAsync(hmu.data(), ctx->dmus.p, sizeof(double) * bins, cudaMemcpyDeviceToHost, ctx->stream), "read derivative table");
-        ck(cudaMemcpyAsync(heps.data(), ctx->deps.p, sizeof(double) * bins, cudaMemcpyDeviceToHost, ctx->stream), "read derivative table");
-        ck(cudaStreamSynchronize(ctx->stream), "read derivative table");
-        std::vector<float> f(2 * (size_t)bins);
-        for (uint32_t i = 0; i < bins; ++i) {
-            f[i] = (float)hmu[i];
-            f[bins + i] = (float)heps[i];
-        }
         const ChainSpec &c = ctx->spec;
         DevBuf dtab, dg, dout;
         try {
-            ck(dtab.ensure(sizeof(float) * f.size()), "alloc");
+            ck(dtab.ensure(sizeof(float4) * bins), "alloc");
             ck(dg.ensure(sizeof(double) * 6 * std::max<uint32_t>(c.n_chains, 1)), "alloc");
             ck(dout.ensure(sizeof(double) * 6), "alloc");
-            ck(cudaMemcpyAsync(dtab.p, f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice, ctx->stream), "upload");
+            ck(launch_deriv_tables(ctx->dmus.as<double>(), ctx->deps.as<double>(), bins, 1, dtab.as<float4>(), ctx->stream),
+               "derivative tables");
             const double ref = fwd->log10_weight - fwd->log10_normalizer - (double)(N - 1) * std::log10(c.absorption_factor);
             CompTuning t = staged_tuning(ctx);
             t.exact_blend = 1;
             ck(launch_comp_adjoint(c, t, ctx->init_seg.as<float>(), ctx->lintab.as<float2>(), ctx->meta,
-                                   ctx->lut32.as<float>(), dtab.as<float>(), dtab.as<float>() + bins, (float)ref,
-                                   dg.as<double>(), dout.as<double>(), ctx->stream),
+                                   dtab.as<float4>(), (float)ref, dg.as<double>(), dout.as<double>(), ctx->stream),
                "adjoint kernel");
             double g[6];
             ck(cudaMemcpyAsync(g, dout.p, sizeof(g), cudaMemcpyDeviceToHost, ctx->stream), "read gradient");
