@@ -472,11 +472,19 @@ def main():
                     help="precision: one N=256 experiment (the headline); batch: 4096 uneven experiments; "
                          "image: 64x64 receiver grid at N=512 from a multi-arclength table set")
     ap.add_argument("--experiments", type=int, default=0, help="batch workload: number of experiments (default 4096)")
+    ap.add_argument("--segments", type=int, default=0,
+                    help="precision workload with N segments instead of 256 (per-N figures and profiles; the CPU "
+                         "baseline and the reference arm keep N = 256)")
     args = ap.parse_args()
     if args.experiments:
         BATCH["n"] = args.experiments
     if args.paths and args.workload == "precision":
         W["paths"] = args.paths
+    if args.segments and args.impl == "b200":
+        global WORKLOAD_NAME
+        W["N"] = args.segments
+        WORKLOAD_NAME = WORKLOAD_NAME.replace("N=256", f"N={args.segments}")
+        args.no_cpu = True
     if args.impl == "reference":
         return run_reference_arm(args)
 

@@ -253,6 +253,16 @@ uint32_t twisty_launch_kernel_count(const twisty_ctx *ctx);
  * (FullExperimentRunnerOptimalPerturb.cpp:96-109,358-365); a chain here is a thread there. */
 twisty_status twisty_chain_results(twisty_ctx *ctx, double *log10_sum, uint64_t *valid, uint32_t n_chains);
 
+/* Histogram of the experiment's path weights, the reference's histogram.txt
+ * (FullExperimentRunnerOptimalPerturb.cpp:26-37,394-422,562-575): every weighted path's linear
+ * weight 10^(log10 w + log10 normaliser) counted into n_buckets equal buckets over
+ * [min_weight, max_weight] (the reference: 500 over [4.69653e-16, 1.17517e-13], the range of
+ * five-segment paths); weights below the range count in the first bucket, above it in the last.
+ * Replays the chains of twisty_run with the same parameters (plain or compensated form), keeping
+ * each weight: about the cost of one more pass. counts[n_buckets], n_buckets <= 12288. */
+twisty_status twisty_weight_histogram(twisty_ctx *ctx, const twisty_bc *bc, double min_weight, double max_weight,
+                                      uint32_t n_buckets, uint64_t *counts);
+
 /* Many experiments (uneven N, S, mu_s, eps) in one persistent launch fed by a device
  * work queue; the pass is captured once as a CUDA graph and replayed `iterations` times
  * (results of the last replay). res has n entries. */

@@ -102,6 +102,12 @@ class ExperimentRunner {
         uint32_t numChains = 0;
         int32_t device = 0;
         uint64_t maxExportedPaths = 1000000;
+        // histogram.txt of the path weights (the reference always writes it; here it costs one
+        // more pass, so it is asked for): 500 buckets over the reference's range
+        bool outputHistogram = false;
+        double histogramMinWeight = 4.69653e-16;
+        double histogramMaxWeight = 1.17517e-13;
+        uint32_t histogramBuckets = 500;
     };
 
     // ExperimentRunner::ExperimentResults (Twisty/ExperimentRunner.h:73-82)
@@ -217,6 +223,8 @@ class ExperimentRunner {
         out.weightingExperimentMs = (long long)r.weighting_ms;
         out.weightErrorBoundLog10 = r.weight_error_bound;
         out.fp64RelError = r.fp64_rel_error;
+        WriteConvergence(r);
+        if (m_experimentParams.outputHistogram && !WriteHistogram(bc)) return std::nullopt;
         return out;
     }
 
@@ -225,6 +233,56 @@ class ExperimentRunner {
 
    protected:
     virtual twisty_form formOfRunner() const { return m_experimentParams.form; }
+
+    // histogram.txt in the reference's layout (FullExperimentRunnerOptimalPerturb.cpp:394-422):
+    // a "Histogram" line, then "binMin binMax count" per bucket.
+    bool WriteHistogram(const twisty_bc &bc)
+    {
+        const ExperimentParameters &e = m_experimentParams;
+        std::vector<uint64_t> counts(e.histogramBuckets);
+        const twisty_status s = twisty_weight_histogram(m_ctx, &bc, e.histogramMinWeight, e.histogramMaxWeight,
+                                                        e.histogramBuckets, counts.data());
+        if (s != TWISTY_OK) {
+            m_lastError = std::string(twisty_status_string(s)) + ": " + twisty_last_error(m_ctx);
+            return false;
+        }
+        std::ofstream f(m_experimentDirPath / "histogram.txt");
+        f << "Histogram" << '\n';
+        const double lo = e.histogramMinWeight, hi = e.histogramMaxWeight;
+        for (uint32_t i = 0; i < e.histogramBuckets; ++i)
+            f << lo + (hi - lo) * i / e.histogramBuckets << " " << lo + (hi - lo) * (i + 1) / e.histogramBuckets << " "
+              << counts[i] << '\n';
+        return true;
+    }
+
+    // ConvergenceWeights/ConvergenceWeights.txt, as ExperimentRunner::UpdateConvergenceWeight
+    // writes it (Twisty/ExperimentRunner.cpp:399-422): "paths, running mean weight" each time
+    // numPathsPerBatch more paths have been added -- here the chains' sums in chain order (a chain
+    // is the reference's thread). Best effort: an unwritable directory leaves the result alone.
+    void WriteConvergence(const twisty_result &r)
+    {
+        if (r.num_chains == 0) return;
+        std::vector<double> lw(r.num_chains);
+        std::vector<uint64_t> valid(r.num_chains);
+        if (twisty_chain_results(m_ctx, lw.data(), valid.data(), r.num_chains) != TWISTY_OK) return;
+        std::error_code ec;
+        const std::filesystem::path dir = m_experimentDirPath / "ConvergenceWeights";
+        std::filesystem::create_directories(dir, ec);
+        std::ofstream f(dir / "ConvergenceWeights.txt");
+        if (!f) return;
+        const uint64_t batch = m_experimentParams.numPathsPerBatch ? m_experimentParams.numPathsPerBatch : 1000000;
+        uint64_t paths = 0, since = 0;
+        long double sum = 0.0L;
+        for (uint32_t c = 0; c < r.num_chains; ++c) {
+            if (std::isfinite(lw[c])) sum += std::pow(10.0L, (long double)lw[c]);
+            paths += valid[c];
+            since += valid[c];
+            if (since >= batch || c + 1 == r.num_chains) {
+                f << paths << ", " << (paths ? sum / (long double)paths : 0.0L) << std::endl;
+                since = 0;
+            }
+        }
+    }
 
     twisty_params to_c() const
     {

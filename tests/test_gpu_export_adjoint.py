@@ -174,3 +174,28 @@ def test_adjoint_matches_fp64_cpu_finite_differences_of_the_reference_weighters(
     assert abs(g[1] - fd[1]) < 1e-3 * abs(fd[1]), (g[1], fd[1])
     scale = np.abs(fd[2:]).max()
     assert np.all(np.abs(g[2:] - fd[2:]) < 1e-3 * scale), (g[2:], fd[2:])
+
+
+@pytest.mark.parametrize("form", [T.FORM_COMPENSATED, T.FORM_PLAIN_FP32])
+def test_weight_histogram_counts_the_exported_paths(form):
+    """twisty_weight_histogram (the reference's histogram.txt) against the same pass's exported
+    path weights binned on the host by the reference's rule (linear weight incl. normaliser,
+    equal buckets, out-of-range weights in the end buckets)."""
+    mu, eps, sc, ab, nst, bins, N, S = LUT_SETS["B"]
+    chains, steps = 128, 40
+    p = T.default_params(num_segments=N, form=form, perturb_seed=8, num_chains=chains, paths_to_generate=chains * steps,
+                         paths_to_skip=10, mu=mu, eps=eps, scatter=sc, absorption=ab, num_steps_int=nst,
+                         num_curvature_steps=bins, max_sub_chain=16, max_angle=0.3)
+    bc = bc_for(N, S)
+    with T.Context(p) as ctx:
+        pos, w, r = ctx.export_paths(bc, None, chains * steps)
+        lin = 10.0 ** (w + r.log10_normalizer)
+        lo, hi = np.quantile(lin, 0.05), np.quantile(lin, 0.9)
+        counts = ctx.weight_histogram(bc, lo, hi, 64)
+    expect = np.zeros(64, np.uint64)
+    for v in lin:
+        b = 0 if v < lo else 63 if v > hi else min(int((v - lo) / (hi - lo) * 64), 63)
+        expect[b] += 1
+    assert counts.sum() == r.total_paths == w.size
+    # bucket edges: a weight within rounding of an edge may land on either side of it
+    assert np.abs(counts.astype(np.int64) - expect.astype(np.int64)).sum() <= 2

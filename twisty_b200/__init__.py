@@ -138,6 +138,15 @@ class Context:
         _check(_lib().twisty_chain_results(self._h, _fptr(lw), _fptr(v), n_chains), self._h)
         return lw, v
 
+    def weight_histogram(self, bc: _abi.BC, min_weight: float = 4.69653e-16, max_weight: float = 1.17517e-13,
+                         n_buckets: int = 500) -> np.ndarray:
+        """The reference's path-weight histogram (its defaults: 500 buckets over the range of
+        five-segment paths); counts per bucket."""
+        c = np.zeros(n_buckets, np.uint64)
+        _check(_lib().twisty_weight_histogram(self._h, C.byref(bc), float(min_weight), float(max_weight), n_buckets,
+                                              _fptr(c)), self._h)
+        return c
+
     def run_msegment(self, bc: _abi.BC) -> _abi.Result:
         """Independent-sample M-segment MC: paths_to_generate fresh bootstrap curves, mean weight."""
         r = _abi.Result()

@@ -167,6 +167,7 @@ SIGNATURES = [
     ("twisty_collect", C.c_int, [_P, C.POINTER(Result)]),
     ("twisty_launch_kernel_count", C.c_uint32, [_P]),
     ("twisty_chain_results", C.c_int, [_P, _P, _P, C.c_uint32]),
+    ("twisty_weight_histogram", C.c_int, [_P, C.POINTER(BC), C.c_double, C.c_double, C.c_uint32, _P]),
     ("twisty_run_batch", C.c_int, [_P, C.POINTER(Experiment), C.c_uint32, C.c_uint32, C.POINTER(Result)]),
     ("twisty_run_msegment", C.c_int, [_P, C.POINTER(BC), C.POINTER(Result)]),
     ("twisty_weight_paths", C.c_int, [_P, C.POINTER(BC), _P, C.c_uint64, C.c_int32, _P, _P, _P]),

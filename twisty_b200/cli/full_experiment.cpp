@@ -1,6 +1,6 @@
 // twisty_full_experiment -- drop-in for the reference's CLI driver Experiments/FullExperiment.cpp.
 //
-//   twisty_full_experiment config.json|config.yaml
+//   twisty_full_experiment config.json|config.yaml [--histogram]
 //
 // Reads the reference's experiment config (JSON, or the same keys in YAML), creates
 // <experimentDir>/<name>/<timestamp>/ and copies the config there, runs the experiment on
@@ -46,6 +46,8 @@ int main(int argc, char **argv)
         std::cout << "Call as: " << argv[0] << " configFilename" << std::endl;
         return 1;
     }
+    // --histogram: also write histogram.txt (the reference's always-on path-weight histogram)
+    const bool histogram = argc > 2 && std::string(argv[2]) == "--histogram";
     std::ifstream f(argv[1]);
     if (!f.is_open()) {
         std::cout << "Failed to open: " << argv[1] << std::endl;
@@ -82,6 +84,7 @@ int main(int argc, char **argv)
     std::filesystem::copy_file(argv[1], params.experimentDirPath + "/" + params.experimentName + (yaml ? ".yaml" : ".json"),
                                std::filesystem::copy_options::overwrite_existing);
     params.perExperimentDirSubfolder = "main";
+    params.outputHistogram = histogram;
     std::cout << "Experiment Path Count: " << params.numPathsInExperiment << std::endl;
     FullExperimentRunnerOptimalPerturbOptimized_GPU runner(params);
     std::optional<ExperimentRunner::ExperimentResults> results = runner.RunExperiment(bc);

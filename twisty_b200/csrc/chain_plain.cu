@@ -12,6 +12,8 @@
 // spelled with round-to-nearest intrinsics in the reference's operation order, so a chain
 // here is bit-identical to the same chain run by the CPU oracle.
 #include "kernels.h"
+
+#include <algorithm>
 #include "device_common.cuh"
 
 #include <cfloat>
@@ -97,11 +99,14 @@ __global__ void __launch_bounds__(kPlainThreads) plain_chain_kernel(ChainSpec c,
         }
         if (ok && !isnan(running)) dev::cw_add(cw, running);
         else ++failed;
-        if (exp_pos) {
-            // export replay: every weighted path of this chain, in step order
+        if (exp_w) {
+            // export replay: every weighted path of this chain, in step order (a weights-only
+            // replay passes no position buffer)
             const size_t pidx = (size_t)chain * c.steps + (s - c.burn_in);
-            float *dst = exp_pos + pidx * 3 * (size_t)(N + 1);
-            for (uint32_t i = 0; i < 3 * (N + 1); ++i) dst[i] = pos[i];
+            if (exp_pos) {
+                float *dst = exp_pos + pidx * 3 * (size_t)(N + 1);
+                for (uint32_t i = 0; i < 3 * (N + 1); ++i) dst[i] = pos[i];
+            }
             exp_w[pidx] = (ok && !isnan(running)) ? running : NAN;
         }
     }
@@ -398,6 +403,45 @@ cudaError_t launch_weigh_plain(const float *pos, uint64_t n_paths, uint32_t n_se
     const uint64_t blocks = (n_paths + 127) / 128;
     weigh_plain_kernel<<<(unsigned)blocks, 128, 0, st>>>(pos, n_paths, n_segments, inv_ds, lut, m,
                                                          absorption_factor, log10w, valid, bins);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------ path histogram
+namespace {
+// Linear path weights 10^(w + log10_norm) counted into nbins equal buckets over [lo, hi]: below
+// lo into the first, above hi into the last (the reference's rule,
+// FullExperimentRunnerOptimalPerturb.cpp:562-575, whose index for a weight of exactly hi is one
+// past its last bucket: here the last); NaN (unwritten or invalid) weights are not counted.
+__global__ void __launch_bounds__(256) weight_histogram_kernel(const double *__restrict__ w, uint64_t n,
+                                                               double log10_norm, double lo, double hi,
+                                                               uint32_t nbins, unsigned long long *__restrict__ counts)
+{
+    extern __shared__ unsigned int h[];
+    for (uint32_t i = threadIdx.x; i < nbins; i += blockDim.x) h[i] = 0u;
+    __syncthreads();
+    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x) {
+        const double x = w[p];
+        if (isnan(x)) continue;
+        const double v = exp10(x + log10_norm);
+        uint32_t b;
+        if (v < lo) b = 0;
+        else if (v > hi) b = nbins - 1;
+        else b = min((uint32_t)((v - lo) / (hi - lo) * (double)nbins), nbins - 1);
+        atomicAdd(&h[b], 1u);
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < nbins; i += blockDim.x)
+        if (h[i]) atomicAdd(&counts[i], (unsigned long long)h[i]);
+}
+}  // namespace
+
+cudaError_t launch_weight_histogram(const double *w, uint64_t n, double log10_norm, double lo, double hi, uint32_t nbins,
+                                    unsigned long long *counts, cudaStream_t st)
+{
+    if (n == 0) return cudaSuccess;
+    const uint64_t blocks = std::min<uint64_t>((n + 255) / 256, 148 * 8);
+    weight_histogram_kernel<<<(unsigned)blocks, 256, sizeof(unsigned int) * nbins, st>>>(w, n, log10_norm, lo, hi, nbins,
+                                                                                         counts);
     return cudaGetLastError();
 }
 

@@ -696,9 +696,9 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                         if (j == 0) ma.exp_w[pidx] = isnan(w) ? NAN : w + (N - 1) * ma.log10_abs;
                     }
                 }
-                if (MODE == kModeExport) {
+                if (MODE == kModeExport && ma.exp_pos) {
                     // positions x_0 + prefix sums of l_s t_s, in double; every lane takes part in
-                    // the scan, only active chains write
+                    // the scan, only active chains write (a weights-only replay passes no buffer)
                     double px = 0.0, py = 0.0, pz = 0.0;
                     double lx[SPL], ly[SPL], lz[SPL];
 #pragma unroll
@@ -804,7 +804,9 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
             } else {
                 w = path_log10<G, SPL, true, CLAMP, TAB_GLOBAL>(j, N, s_tab, kc, tan_smem, next_smem, no_bins, clamped);
             }
-            if (MODE == kModeExport) {
+            if (MODE == kModeExport && !ma.exp_pos && active && j == 0)   // weights-only replay
+                ma.exp_w[(size_t)chain * c.steps + wstep] = isnan(w) ? NAN : w + (N - 1) * ma.log10_abs;
+            if (MODE == kModeExport && ma.exp_pos) {
                 double px = 0.0, py = 0.0, pz = 0.0;
                 double lx[SPL], ly[SPL], lz[SPL];
 #pragma unroll

@@ -218,6 +218,11 @@ cudaError_t launch_grad_reduce_segments(const double *grad_chains, const uint2 *
 cudaError_t launch_deriv_tables(const double *dmu, const double *deps, uint32_t bins, uint32_t n_tables, float4 *out,
                                 cudaStream_t st);
 
+// Path-weight histogram (chain_plain.cu): w[n] log10 path weights (NaN: not counted), counted as
+// 10^(w + log10_norm) into nbins <= 12288 equal buckets over [lo, hi] (outside: the end buckets).
+cudaError_t launch_weight_histogram(const double *w, uint64_t n, double log10_norm, double lo, double hi, uint32_t nbins,
+                                    unsigned long long *counts, cudaStream_t st);
+
 // ----------------------------------------------------------- reduction (chain_plain.cu)
 cudaError_t launch_reduce(const ChainOut *chains, uint32_t n, ReduceOut *out, cudaStream_t st);
 // One reduction per range: ranges[x] = (first chain, count) -> out[x].

@@ -1921,6 +1921,61 @@ twisty_status twisty_adjoint(twisty_ctx *ctx, const twisty_bc *bc, const twisty_
     });
 }
 
+twisty_status twisty_weight_histogram(twisty_ctx *ctx, const twisty_bc *bc, double min_weight, double max_weight,
+                                      uint32_t n_buckets, uint64_t *counts)
+{
+    if (!ctx || !bc || !counts || n_buckets == 0 || n_buckets > 12288 || !(max_weight > min_weight))
+        return TWISTY_ERR_INVALID_ARGUMENT;
+    return guard(ctx, [&] {
+        if (ctx->p.form == TWISTY_FORM_FP64) fail(TWISTY_ERR_UNSUPPORTED, "the histogram replays the plain or compensated form");
+        if (ctx->p.eval_end_shift.x != 0.f || ctx->p.eval_end_shift.y != 0.f || ctx->p.eval_end_shift.z != 0.f)
+            fail(TWISTY_ERR_UNSUPPORTED, "eval_end_shift applies to forward passes only");
+        prepare(ctx, bc);
+        const ChainSpec &c = ctx->spec;
+        cudaStream_t st = ctx->stream;
+        DevBuf dw, dout, dcnt;
+        struct Release {
+            DevBuf *b[3];
+            ~Release()
+            {
+                for (DevBuf *x : b) x->release();
+            }
+        } rel{{&dw, &dout, &dcnt}};
+        ck(dcnt.ensure(sizeof(unsigned long long) * n_buckets), "alloc histogram");
+        ck(cudaMemsetAsync(dcnt.p, 0, sizeof(unsigned long long) * n_buckets, st), "memset");
+        if (c.n_chains) {
+            // the chains replayed in slices of at most 2^24 weighted paths, every weight kept
+            const uint32_t per = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(c.n_chains, (1ull << 24) / std::max(1u, c.steps)));
+            ck(dw.ensure(sizeof(double) * (size_t)per * c.steps), "alloc histogram");
+            ck(dout.ensure(sizeof(ChainOut) * per), "alloc histogram");
+            const float x0[3] = {bc->start_pos.x, bc->start_pos.y, bc->start_pos.z};
+            for (uint32_t a = 0; a < c.n_chains; a += per) {
+                ChainSpec ce = c;
+                ce.chain0 = c.chain0 + a;
+                ce.n_chains = std::min(per, c.n_chains - a);
+                ce.last_steps = (a + ce.n_chains == c.n_chains) ? c.last_steps : c.steps;
+                ck(cudaMemsetAsync(dw.p, 0xff, sizeof(double) * (size_t)ce.n_chains * c.steps, st), "memset");  // NaN
+                if (ctx->p.form == TWISTY_FORM_PLAIN_FP32)
+                    ck(launch_plain_chains(ce, ctx->init_pos.as<float>(), ctx->state.as<float>(), ctx->lut32.as<float>(),
+                                           ctx->meta, dout.as<ChainOut>(), st, nullptr, dw.as<double>()),
+                       "histogram replay");
+                else
+                    ck(launch_comp_export(ce, staged_tuning(ctx), ctx->init_seg.as<float>(), ctx->fixtab.as<float2>(),
+                                          ctx->lintab.as<float2>(), ctx->meta, x0, nullptr, dw.as<double>(),
+                                          dout.as<ChainOut>(), st, ctx->lf),
+                       "histogram replay");
+                ck(launch_weight_histogram(dw.as<double>(), (uint64_t)ce.n_chains * c.steps, ctx->log10_norm, min_weight,
+                                           max_weight, n_buckets, dcnt.as<unsigned long long>(), st),
+                   "histogram");
+            }
+        }
+        std::vector<unsigned long long> h(n_buckets);
+        ck(cudaMemcpyAsync(h.data(), dcnt.p, sizeof(unsigned long long) * n_buckets, cudaMemcpyDeviceToHost, st), "read histogram");
+        ck(cudaStreamSynchronize(st), "histogram");
+        for (uint32_t i = 0; i < n_buckets; ++i) counts[i] = h[i];
+    });
+}
+
 twisty_status twisty_chain_results(twisty_ctx *ctx, double *log10_sum, uint64_t *valid, uint32_t n_chains)
 {
     if (!ctx || (!log10_sum && n_chains)) return TWISTY_ERR_INVALID_ARGUMENT;
