@@ -384,3 +384,48 @@ def test_error_statuses():
         assert e.value.status == _abi.ERR_UNSUPPORTED
         ctx.update(perturb_method=0)
         assert ctx.run(geom_bc(N, S)).total_paths == 1000   # the context stays usable
+
+
+@pytest.mark.parametrize("form", [T.FORM_PLAIN_FP32, T.FORM_COMPENSATED])
+def test_weighers_on_degenerate_and_clamped_paths(oracle, form):
+    """Edge cases of the weighers against the oracle (pinned to the reference): a path with a
+    zero-length segment, whose tangent is NaN and which the reference marks invalid
+    (PathWeighters.cpp:89-92), and curvatures beyond a truncated table's range, clamped to its
+    last bin (:45-65)."""
+    p, N, S = lut_params("A")
+    paths = golden_npz("paths_A.npz")
+    pos = paths["pos"].copy()
+    pos[5, 11] = pos[5, 10]          # zero-length segment 10 of path 5
+    pos[7, 40] = pos[7, 41]          # and segment 40 of path 7
+    lut, info = golden_lut_info("A")
+    keep = lut.size // 8             # a table covering the lowest eighth of the curvature range
+    step = F32(info.curvature_step)
+    lut_t = np.ascontiguousarray(lut[:keep])
+    max_k = float(F32(step * F32(keep - 1)))
+    info_t = _abi.LutInfo(0.0, max_k, float(step), float(lut_t.min()), float(lut_t.max()), info.ds, keep)
+    meta = oracle.LutMeta(0.0, max_k, float(step), float(lut_t.min()), float(lut_t.max()), info.ds, keep, 0)
+    ow, ov, ob, oc = oracle.weigh_f32(pos, N, S, lut_t, meta, want_bins=True, want_curv=True)
+    assert ov[5] == 0 and ov[7] == 0 and ov.sum() == ov.size - 2
+    assert np.any(oc[ov == 1] > max_k)   # some curvatures beyond the table, clamped
+    with T.Context(p) as ctx:
+        ctx.set_lut(lut_t, info_t)
+        w, v, b = ctx.weight_paths(geom_bc(N, S), pos, form=form, want_bins=True)
+    assert np.array_equal(v, ov)
+    ok = ov == 1
+    if form == T.FORM_PLAIN_FP32:
+        assert np.array_equal(b[ok], ob[ok]) and np.max(np.abs(w[ok] - ow[ok])) < 1e-12
+    else:
+        assert np.all(np.abs(w[ok] - ow[ok]) < 1e-5 * np.abs(ow[ok]) + edge_jumps_log10(lut_t, step)[
+            np.clip(np.maximum(b[ok], ob[ok]), 0, keep - 1)].sum(axis=1) * (b[ok] != ob[ok]).any(axis=1))
+
+
+def test_empty_passes_and_batches():
+    """Zero paths: a run reports no paths and a weight of zero (log10 -inf), weighing no paths
+    is a no-op, and an empty batch returns nothing."""
+    p, N, S = lut_params("A", paths_to_generate=0)
+    with T.Context(p) as ctx:
+        r = ctx.run(geom_bc(N, S))
+        assert r.total_paths == 0 and r.num_chains == 0 and r.log10_weight == -math.inf
+        w, v, b = ctx.weight_paths(geom_bc(N, S), np.zeros((0, N + 1, 3), np.float32), form=T.FORM_PLAIN_FP32)
+        assert w.size == 0
+        assert ctx.run_batch([]) == []
