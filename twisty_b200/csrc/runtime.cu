@@ -102,6 +102,31 @@ struct BatchAdjointOut {
     double *timing;   // [2]
 };
 
+// Streams, events and the graph of one batched pass, kept by the context: a batch whose buckets,
+// grids and device buffers are those of the previous call replays the same graph (the
+// experiments' tables, curves and work items are uploaded afresh; the graph reads them from the
+// same buffers), so that a loop over the same grid (new mu_s or sigma per iteration, say) pays
+// no capture and no instantiation.
+struct BatchGraph {
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> events;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<uint64_t> key;   // what the graph was captured for
+    void release()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (cudaEvent_t e : events) cudaEventDestroy(e);
+        for (cudaStream_t st : streams) cudaStreamDestroy(st);
+        exec = nullptr;
+        graph = nullptr;
+        events.clear();
+        streams.clear();
+        key.clear();
+    }
+};
+
 struct twisty_ctx {
     twisty_params p{};
     int device = 0;
@@ -152,6 +177,7 @@ struct twisty_ctx {
     uint32_t kernels_per_launch = 0;
     bool launched = false;
     BatchBufs batch;
+    BatchGraph batch_graph;
 };
 
 namespace {
@@ -929,6 +955,7 @@ void twisty_destroy(twisty_ctx *ctx)
                       &ctx->init_pos, &ctx->init_seg, &ctx->state, &ctx->chain_out, &ctx->partials, &ctx->reduce_out,
                       &ctx->norm_scratch, &ctx->multi.dev, &ctx->check_state, &ctx->check_out};
     for (DevBuf *b : bufs) b->release();
+    ctx->batch_graph.release();
     ctx->batch.release();
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
@@ -1227,20 +1254,6 @@ float twisty_min_arclength(const twisty_bc *bc, uint32_t n) { return bc ? twisty
 
 namespace {
 
-// Streams, events and the graph of one batched pass.
-struct BatchGraph {
-    std::vector<cudaStream_t> streams;
-    std::vector<cudaEvent_t> events;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    ~BatchGraph()
-    {
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        for (cudaEvent_t e : events) cudaEventDestroy(e);
-        for (cudaStream_t st : streams) cudaStreamDestroy(st);
-    }
-};
 
 std::string exp_msg(uint32_t e, const std::string &m)
 {
@@ -1553,34 +1566,52 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
     ck(cudaMemcpyAsync(B.ranges.p, ranges.data(), sizeof(uint2) * n, cudaMemcpyHostToDevice, st), "upload batch");
     ck(cudaStreamSynchronize(st), "batch upload");
 
-    // ---- the pass as a graph: counters reset, one launch per bucket on forked streams, reduction
-    BatchGraph G;
-    G.streams.resize(buckets.size(), nullptr);
-    G.events.resize(buckets.size() + 3, nullptr);
-    for (auto &x : G.streams) ck(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking), "stream");
-    for (auto &x : G.events) ck(cudaEventCreateWithFlags(&x, cudaEventDisableTiming), "event");
-    cudaEvent_t fork = G.events[buckets.size()];
-    ck(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed), "capture");
-    {
-        cudaError_t ce = cudaMemsetAsync(B.counters.p, 0, sizeof(uint32_t) * buckets.size(), st);
-        if (ce == cudaSuccess) ce = cudaEventRecord(fork, st);
-        for (size_t b = 0; b < buckets.size() && ce == cudaSuccess; ++b) {
-            const Bucket &bk = buckets[b];
-            ce = cudaStreamWaitEvent(G.streams[b], fork, 0);
-            if (ce == cudaSuccess)
-                ce = launch_batch(bk.shape, B.exps.p, B.items.as<uint2>() + bk.item_off, (uint32_t)bk.items.size(),
-                                  B.counters.as<uint32_t>() + b, B.chain_out.as<ChainOut>(), (int)bins, bk.grid,
-                                  G.streams[b]);
-            if (ce == cudaSuccess) ce = cudaEventRecord(G.events[b], G.streams[b]);
-            if (ce == cudaSuccess) ce = cudaStreamWaitEvent(st, G.events[b], 0);
-        }
-        if (ce == cudaSuccess) ce = launch_reduce_segments(B.chain_out.as<ChainOut>(), B.ranges.as<uint2>(), n,
-                                                           B.red.as<ReduceOut>(), st);
-        const cudaError_t ee = cudaStreamEndCapture(st, &G.graph);
-        ck(ce, "batched pass capture");
-        ck(ee, "end capture");
+    // ---- the pass as a graph: counters reset, one launch per bucket on forked streams, reduction;
+    // captured again only when the buckets, grids or buffers differ from the previous call's
+    std::vector<uint64_t> key = {(uint64_t)n, (uint64_t)bins, (uint64_t)(uintptr_t)B.exps.p, (uint64_t)(uintptr_t)B.items.p,
+                                 (uint64_t)(uintptr_t)B.counters.p, (uint64_t)(uintptr_t)B.chain_out.p,
+                                 (uint64_t)(uintptr_t)B.ranges.p, (uint64_t)(uintptr_t)B.red.p};
+    for (const Bucket &bk : buckets) {
+        key.push_back(((uint64_t)bk.shape.group << 48) | ((uint64_t)bk.shape.spl << 40) | ((uint64_t)bk.shape.warps << 32) |
+                      ((uint64_t)bk.shape.exact << 4) | ((uint64_t)bk.shape.lut_smem << 3) |
+                      ((uint64_t)bk.shape.clamp << 2) | ((uint64_t)bk.shape.steep << 1));
+        key.push_back(((uint64_t)bk.grid << 32) | bk.item_off);
+        key.push_back(bk.items.size());
     }
-    ck(cudaGraphInstantiate(&G.exec, G.graph, 0), "graph instantiate");
+    BatchGraph &G = ctx->batch_graph;
+    if (!G.exec || G.key != key) {
+        G.release();
+        G.streams.resize(buckets.size(), nullptr);
+        G.events.resize(buckets.size() + 3, nullptr);
+        for (auto &x : G.streams) ck(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking), "stream");
+        for (auto &x : G.events) ck(cudaEventCreateWithFlags(&x, cudaEventDisableTiming), "event");
+        cudaEvent_t fork = G.events[buckets.size()];
+        ck(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed), "capture");
+        {
+            cudaError_t ce = cudaMemsetAsync(B.counters.p, 0, sizeof(uint32_t) * buckets.size(), st);
+            if (ce == cudaSuccess) ce = cudaEventRecord(fork, st);
+            for (size_t b = 0; b < buckets.size() && ce == cudaSuccess; ++b) {
+                const Bucket &bk = buckets[b];
+                ce = cudaStreamWaitEvent(G.streams[b], fork, 0);
+                if (ce == cudaSuccess)
+                    ce = launch_batch(bk.shape, B.exps.p, B.items.as<uint2>() + bk.item_off, (uint32_t)bk.items.size(),
+                                      B.counters.as<uint32_t>() + b, B.chain_out.as<ChainOut>(), (int)bins, bk.grid,
+                                      G.streams[b]);
+                if (ce == cudaSuccess) ce = cudaEventRecord(G.events[b], G.streams[b]);
+                if (ce == cudaSuccess) ce = cudaStreamWaitEvent(st, G.events[b], 0);
+            }
+            if (ce == cudaSuccess) ce = launch_reduce_segments(B.chain_out.as<ChainOut>(), B.ranges.as<uint2>(), n,
+                                                               B.red.as<ReduceOut>(), st);
+            const cudaError_t ee = cudaStreamEndCapture(st, &G.graph);
+            if (ce != cudaSuccess || ee != cudaSuccess) G.release();
+            ck(ce, "batched pass capture");
+            ck(ee, "end capture");
+        }
+        const cudaError_t ie = cudaGraphInstantiate(&G.exec, G.graph, 0);
+        if (ie != cudaSuccess) G.release();
+        ck(ie, "graph instantiate");
+        G.key = key;
+    }
     const double setup_ms = now_ms() - t0;
     ctx->kernels_per_launch = (uint32_t)buckets.size() + 1;   // one persistent launch per bucket + the reduction
 
