@@ -72,11 +72,26 @@ def test_compensated_export_geometry_and_weights(oracle, tmp_path):
     assert np.allclose(seg, seg0[None, :], rtol=2e-6)
     assert np.allclose(seg0, float(F32(S) / F32(N)), rtol=1e-3)
     assert np.allclose(pos64[:, 0], (0, 0, 0)) and np.allclose(pos64[:, -1], (0, 0, 7), atol=2e-5)
-    # the reference weigher on the exported geometry agrees to 1e-5 (edge flips aside)
+    # the reference weigher on the exported geometry: every path within 1e-5 relative, plus the
+    # weight jumps at the bin edges its curvatures lie near. The exported positions are the
+    # chain's tangents times lengths summed in double and rounded to float (2^-24 of |x| <= 7
+    # each), so the reference's curvatures from them differ from the chain's by up to ~5e-3 of a
+    # bin here (a segment's two rounded ends move its unit tangent by up to 2 x 7 x 2^-24 / ds =
+    # 2.4e-6, a curvature takes two tangents, and kscale = (bins - 1) / 2.02 ~ 1000 bins per
+    # unit): an edge within 1e-2 bins of a curvature may flip.
     olut, meta = oracle.lut_f32(oracle.wparams(mu, eps, sc, ab, nst, bins), F32(S) / F32(N))
-    ow, ov, _, _ = oracle.weigh_f32(pos, N, S, olut, meta, absorption=ab, want_bins=False)
-    rel = np.abs(ow - w) / np.abs(ow)
-    assert np.median(rel) < 1e-6 and np.mean(rel < 1e-5) > 0.95
+    ow, ov, ob, oc = oracle.weigh_f32(pos, N, S, olut, meta, absorption=ab, want_bins=True, want_curv=True)
+    assert np.all(ov == 1)
+    r_ = oc.astype(np.float64) / float(meta.step)
+    near = np.abs(r_ - np.round(r_)) < 1e-2
+    Lr = olut.astype(np.float64)
+    below = Lr[:-1] + float(meta.step) * (Lr[1:] - Lr[:-1])
+    jumps = np.concatenate([[0.0], np.abs(np.log10(Lr[1:]) - np.log10(below))])
+    edge = np.clip(np.round(r_).astype(np.int64), 0, bins - 1)
+    allowed = np.where(near, jumps[edge], 0.0).sum(axis=1)
+    dev = np.abs(ow - w)
+    assert np.all(dev <= 1e-5 * np.abs(ow) + allowed * (1 + 1e-6)), (dev - 1e-5 * np.abs(ow) - allowed).max()
+    assert np.median(dev / np.abs(ow)) < 1e-6
 
 
 # The differentiation configuration: N = 128 (and 130, the N the reference's bootstrapper
