@@ -55,6 +55,34 @@ SMS = 148
 LANES_PER_SM = 128
 
 
+_FP32_PEAK = {}
+
+
+def fp32_roof(T, device):
+    """The FP32 roof in T lane-instructions/s: the device's FMA issue rate measured by the library
+    (twisty_measure_fp32_peak, ~100 ms, once per process), and the nominal 148 SMs x 128 lanes x the
+    max SM clock of MEASURED_PEAKS.json beside it. MEASURED_PEAKS.json has no FP32 figure."""
+    if device not in _FP32_PEAK:
+        sm_max = load_peaks().get("sm_max_mhz", 1965.0)
+        nominal = SMS * LANES_PER_SM * sm_max * 1e6 / 1e12
+        try:
+            measured = T.measure_fp32_peak(device) / 1e12
+        except Exception:   # reported as unmeasured, never silently replaced by the nominal figure
+            measured = None
+        _FP32_PEAK[device] = (measured, nominal, sm_max)
+    return _FP32_PEAK[device]
+
+
+def roofline_fields(T, device, achieved_ti):
+    measured, nominal, sm_max = fp32_roof(T, device)
+    peak = measured if measured else nominal
+    return {"achieved": achieved_ti, "peak": peak, "unit": "Tinstr/s", "frac": achieved_ti / peak,
+            "peak_kind": ("measured: FMA issue rate of this B200 (twisty_measure_fp32_peak)" if measured else
+                          "nominal (the FMA-rate measurement failed)"),
+            "peak_nominal": nominal, "frac_of_nominal": achieved_ti / nominal,
+            "peak_nominal_basis": f"{SMS} SMs x {LANES_PER_SM} lanes x {sm_max:g} MHz (max SM clock of MEASURED_PEAKS.json)"}
+
+
 def load_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -336,9 +364,6 @@ def run_image_workload(args, T, torch, device, ws, rank, pg):
     ctx.close()
     done = sum(r.total_paths * I["N"] for r in res)
     value = done * ws / (per_step / 1e3)
-    peaks = load_peaks()
-    sm_max = peaks.get("sm_max_mhz", 1965.0)
-    peak_ti = SMS * LANES_PER_SM * sm_max * 1e6 / 1e12
     achieved_ti = INSTR_PER_SEGMENT * done / (per_step / 1e3) / 1e12
     if rank == 0:
         import ctypes
@@ -352,9 +377,8 @@ def run_image_workload(args, T, torch, device, ws, rank, pg):
                 "e2e": {"value": done * ws / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms,
                         "h2d_bytes_per_step": ctypes.sizeof(T._abi.Experiment) * len(exps),
                         "d2h_bytes_per_step": ctypes.sizeof(T._abi.Result) * len(exps)},
-                "roofline": {"bound": "fp32", "kernel": "batch_kernel", "achieved": achieved_ti, "peak": peak_ti,
-                             "unit": "Tinstr/s", "frac": achieved_ti / peak_ti, "traffic": None,
-                             "basis": f"{INSTR_PER_SEGMENT:g} FP32 instructions per path-segment"},
+                "roofline": {"bound": "fp32", "kernel": "batch_kernel", **roofline_fields(T, device, achieved_ti),
+                             "traffic": None, "basis": f"{INSTR_PER_SEGMENT:g} FP32 instructions per path-segment"},
                 "cpu_baseline": None, "clocks": clk.summary(), "gpu_launches": launches * args.steps}
         if adjoint:
             line["adjoint"] = adjoint
@@ -394,15 +418,10 @@ def measure_batch(T, device, steps, warmup, exps=None, first=0, chain_offset=0):
                 launches=launches, clocks=clk.summary())
 
 
-def batch_roofline(done, per_step):
-    peaks = load_peaks()
-    sm_max = peaks.get("sm_max_mhz", 1965.0)
-    peak_ti = SMS * LANES_PER_SM * sm_max * 1e6 / 1e12
+def batch_roofline(T, device, done, per_step):
     achieved_ti = INSTR_PER_SEGMENT * done / (per_step / 1e3) / 1e12
-    return {"bound": "fp32", "kernel": "batch_kernel", "achieved": achieved_ti, "peak": peak_ti, "unit": "Tinstr/s",
-            "frac": achieved_ti / peak_ti, "traffic": None,
-            "basis": f"{INSTR_PER_SEGMENT:g} FP32 instructions per path-segment; peak = {SMS} SMs x {LANES_PER_SM} "
-                     f"lanes x {sm_max:g} MHz"}
+    return {"bound": "fp32", "kernel": "batch_kernel", **roofline_fields(T, device, achieved_ti), "traffic": None,
+            "basis": f"{INSTR_PER_SEGMENT:g} FP32 instructions per path-segment"}
 
 
 def run_batch_workload(args, T, torch, device, ws, rank, pg):
@@ -445,7 +464,7 @@ def run_batch_workload(args, T, torch, device, ws, rank, pg):
                            "parallelism": f"experiments split over {ws} ranks" if ws > 1 else "one GPU"},
                 "e2e": {"value": done_all / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms,
                         "setup_ms": m["setup_ms"], "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-                "roofline": batch_roofline(m["done"], m["per_step"]),
+                "roofline": batch_roofline(T, device, m["done"], m["per_step"]),
                 "cpu_baseline": None, "clocks": m["clocks"], "gpu_launches": m["launches"] * args.steps}
         if combined:
             line["combined"] = combined
@@ -609,7 +628,7 @@ def main():
                     "setup_ms": bm["setup_ms"],
                     "h2d_bytes_per_step": ctypes.sizeof(T._abi.Experiment) * len(bm["exps"]),
                     "d2h_bytes_per_step": ctypes.sizeof(T._abi.Result) * len(bm["exps"])},
-            "roofline": batch_roofline(bm["done"], bm["per_step"]), "gpu_launches_per_step": bm["launches"],
+            "roofline": batch_roofline(T, device, bm["done"], bm["per_step"]), "gpu_launches_per_step": bm["launches"],
             "failed_paths": sum(r.failed_paths for r in bm["res"]), "clocks": bm["clocks"]}
 
     combined = None
@@ -618,17 +637,13 @@ def main():
         from twisty_b200 import dist as D
         combined = D.all_combine(res, device=f"cuda:{device}")
 
-    peaks = load_peaks()
     clocks = clk.summary()
-    sm_max = peaks.get("sm_max_mhz", 1965.0)
-    peak_ti = SMS * LANES_PER_SM * sm_max * 1e6 / 1e12
     achieved_ti = INSTR_PER_SEGMENT * segs / (kernel_ms / 1e3) / 1e12
     roofline = {"bound": "fp32", "kernel": "comp_chain_kernel" if form == T.FORM_COMPENSATED else args.form,
-                "achieved": achieved_ti, "peak": peak_ti, "unit": "Tinstr/s", "frac": achieved_ti / peak_ti,
+                **roofline_fields(T, device, achieved_ti),
                 "traffic": TRAFFIC_PER_LAUNCH if form == T.FORM_COMPENSATED else None,
-                "basis": f"{INSTR_PER_SEGMENT:g} FP32 instructions per path-segment; peak = "
-                f"{SMS} SMs x {LANES_PER_SM} lanes x {sm_max:g} MHz (max SM clock of MEASURED_PEAKS.json); "
-                "traffic = DRAM bytes per launch from ncu (per chain, not per path)",
+                "basis": f"{INSTR_PER_SEGMENT:g} FP32 instructions per path-segment; traffic = DRAM bytes per launch "
+                         "from ncu (per chain, not per path)",
                 "segments_per_s_kernel_only": segs / (kernel_ms / 1e3)}
 
     cpu = None

@@ -394,6 +394,11 @@ typedef struct twisty_shape {
 } twisty_shape;
 twisty_status twisty_default_shape(uint32_t num_segments, uint32_t bins, twisty_shape *out);
 
+/* No counterpart in the reference. The FP32 issue rate of the device (lane-level FMA
+ * instructions per second, independent FMA chains in every lane of every SM), measured in
+ * about 100 ms: the denominator of the chain kernels' roofline. */
+twisty_status twisty_measure_fp32_peak(int device, double *lane_instr_per_s);
+
 /* ------------------------------------------------------- allocation-free pass */
 /* No counterpart in the reference. For callers that cannot allocate device memory when
  * they run a pass: an application whose own caching allocator holds nearly all of the

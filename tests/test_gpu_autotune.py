@@ -56,3 +56,10 @@ def test_batch_keeps_the_default_for_a_tuned_shape_it_has_no_kernel_for(tmp_path
     assert len(res) == 1 and res[0].total_paths == paths and res[0].failed_paths == 0
     assert math.isfinite(res[0].log10_weight)
     assert r.total_paths == paths and r.failed_paths == 0 and math.isfinite(r.log10_weight)
+
+
+def test_measured_fp32_peak_is_near_the_nominal_rate():
+    """twisty_measure_fp32_peak, the roofline's denominator: independent FMA chains in every lane
+    reach the FP32 pipe's rate, 128 lanes x SMs x the SM clock (at most the 1965 MHz maximum)."""
+    v = T.measure_fp32_peak(0)
+    assert 0.5 * 148 * 128 * 1965e6 < v < 1.05 * 148 * 128 * 1965e6, v

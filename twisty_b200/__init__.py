@@ -428,3 +428,11 @@ class FullExperimentRunnerOptimalPerturb:
 
 class FullExperimentRunnerOptimalPerturbOptimized_GPU(FullExperimentRunnerOptimalPerturb):
     """The reference's CUDA runner name; the same B200 runner."""
+
+
+def measure_fp32_peak(device: int = 0) -> float:
+    """The device's FP32 issue rate, lane-level FMA instructions per second
+    (twisty_measure_fp32_peak): the denominator of the chain kernels' roofline."""
+    v = C.c_double()
+    _check(_lib().twisty_measure_fp32_peak(int(device), C.byref(v)))
+    return float(v.value)

@@ -188,6 +188,7 @@ SIGNATURES = [
     ("twisty_tuning_cache_save", C.c_int, [C.c_char_p]),
     ("twisty_tuning_cache_load", C.c_int, [C.c_char_p]),
     ("twisty_default_shape", C.c_int, [C.c_uint32, C.c_uint32, C.POINTER(Shape)]),
+    ("twisty_measure_fp32_peak", C.c_int, [C.c_int, C.POINTER(C.c_double)]),
 ]
 
 _lib = None
