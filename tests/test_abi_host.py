@@ -6,6 +6,7 @@ import json
 import os
 import re
 import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -282,3 +283,17 @@ def test_cpp_runner_header_compiles_for_a_reference_style_caller(tmp_path):
         assert "no CUDA device" in r.stdout
     else:   # a GPU is visible after all
         assert r.returncode == 0 and "paths 1000" in r.stdout
+
+
+def test_reference_arm_loads_nothing_of_this_library():
+    """bench.py's reference arm runs the reference's own loop (compiled from its sources into
+    oracle/_ref) and must not load this library: a small run in a fresh process."""
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    if not os.path.exists(harness):
+        pytest.skip("the reference build (make -C oracle ref) is absent")
+    code = ("import sys; sys.path.insert(0, %r); import bench; "
+            "v, ms, rec = bench.cpu_reference_run(20000, 2); "
+            "assert rec['paths'] == 20000 and v > 0; "
+            "assert 'twisty_b200' not in sys.modules, sorted(m for m in sys.modules if 'twisty' in m); print('ok')") % ROOT
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
