@@ -485,7 +485,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP32 drop-in")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-batch", action="store_true", help="skip timing the batching workload")
-    ap.add_argument("--no-adjoint", action="store_true", help="image workload: skip the batched adjoint")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the adjoint (precision line: the differentiation form; image workload: its batched adjoint)")
     ap.add_argument("--paths", type=int, default=0, help="paths per pass (default 2^26; smaller for profiling)")
     ap.add_argument("--workload", default="precision", choices=["precision", "batch", "image"],
                     help="precision: one N=256 experiment (the headline); batch: 4096 uneven experiments; "
@@ -630,6 +631,33 @@ def main():
                     "d2h_bytes_per_step": ctypes.sizeof(T._abi.Result) * len(bm["exps"])},
             "roofline": batch_roofline(T, device, bm["done"], bm["per_step"]), "gpu_launches_per_step": bm["launches"],
             "failed_paths": sum(r.failed_paths for r in bm["res"]), "clocks": bm["clocks"]}
+
+    if rank == 0 and form == T.FORM_COMPENSATED and not args.no_adjoint:
+        # the differentiation form at its own configuration (N = 128, S = 16, receiver (8,0,0)
+        # along x, 4096-bin tables and derivative tables, 2^22 paths): forward pass, then the
+        # adjoint replay of its chains (derivative tables built, curvatures recomputed)
+        ap_ = T.default_params(num_segments=128, mu=1.0, eps=0.01, scatter=10.0, num_steps_int=4000,
+                               num_curvature_steps=4096, form=T.FORM_COMPENSATED, lut_mode=T.LUT_FP64,
+                               perturb_seed=31, num_chains=4096, paths_to_generate=1 << 22, paths_to_skip=2000,
+                               max_sub_chain=32, max_angle=0.1, device=device)
+        abc = T.make_bc((0, 0, 0), (1, 0, 0), (8, 0, 0), (1, 0, 0), 16.0)
+        with T.Context(ap_) as ca:
+            f0 = ca.run(abc)
+            ca.adjoint(abc, f0)   # warm
+            t0 = time.perf_counter()
+            f1 = ca.run(abc)
+            t1 = time.perf_counter()
+            g = ca.adjoint(abc, f1)
+            t2 = time.perf_counter()
+        segs_a = f1.total_paths * 128
+        extra["adjoint"] = {"workload": "differentiation form: N=128 S=16 x1=(8,0,0) tangents (1,0,0), sigma=0.1 "
+                                        "mu_s=10, 4096-bin tables and derivative tables, 2^22 paths (4096 chains, "
+                                        "2000 burn-in steps), k~U{2..32}, angle~U(-0.1,0.1)",
+                            "forward_ms": (t1 - t0) * 1e3, "adjoint_ms": (t2 - t1) * 1e3,
+                            "adjoint_path_segments_per_s": segs_a / (t2 - t1),
+                            "gradient": {"d_mu_s": g[0], "d_sigma": g[1], "d_receiver": list(g[2:5])},
+                            "note": "host wall time of twisty_run and of twisty_adjoint (derivative tables, replay, "
+                                    "reduction); the replay runs the burn-in steps again"}
 
     combined = None
     if pg:
