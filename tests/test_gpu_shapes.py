@@ -79,3 +79,24 @@ def test_explicit_shape_matches_fp64(N, shape):
     assert a.total_paths == b.total_paths == 512 * 64
     assert a.failed_paths == 0
     assert abs(a.log10_weight - b.log10_weight) < 1.5e-7 * abs(b.log10_weight) + 1e-5, (a.log10_weight, b.log10_weight)
+
+
+@pytest.mark.parametrize("N,angle", [(10, 0.05), (12, 0.05), (24, 0.05), (32, 0.05), (36, 0.05), (24, 0.3), (36, 0.3)])
+def test_long_chains_turning_the_shorter_side_match_fp64(N, angle):
+    """Below N = 37 the forward kernels turn the complement of a sub-chain that is longer than
+    half the path (by -theta about the same chord: the moved path up to one rotation of the
+    whole path) and carry the path's end-to-end chord d through those moves, re-summed every
+    16 steps. The FP64 form always turns the sub-chain itself. Few chains with many steps each
+    (16384) would show a drift of d as a drift of the weights; they agree as short chains do.
+    (At N <= 12 with 0.3 rad moves the FP32 and FP64 trajectories of such long chains part by
+    3e-5 to 2e-3 in log10 whichever side is turned, as they did before complements were turned;
+    0.05 rad keeps them together there.)"""
+    kw = dict(num_chains=64, paths_to_generate=64 * 16384, max_angle=angle)
+    res = {}
+    for form in (T.FORM_COMPENSATED, T.FORM_FP64):
+        with T.Context(_params(N, form, **kw)) as ctx:
+            res[form] = ctx.run(_bc(N))
+    a, b = res[T.FORM_COMPENSATED], res[T.FORM_FP64]
+    assert a.total_paths == b.total_paths == 64 * 16384
+    assert a.failed_paths == 0
+    assert abs(a.log10_weight - b.log10_weight) < 1.5e-7 * abs(b.log10_weight) + 1e-5, (a.log10_weight, b.log10_weight)

@@ -164,6 +164,11 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float x)
 // pipe with the square root): r + 2^23 rounded toward -infinity carries floor(r) in its low
 // mantissa bits for 0 <= r < 2^23. NaN and infinity, which only a degenerate zero-length
 // chord can produce, land past the last bin, are bounded to it and get a NaN fraction.
+template <bool B>
+struct BoolTag {
+    static constexpr bool value = B;
+};
+
 template <bool CLAMP>
 __device__ __forceinline__ float bin_of(float qq, const CompConsts &k, bool valid, uint32_t &clamped, int32_t &L)
 {
@@ -487,6 +492,22 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
     const uint32_t gchain = c.chain0 + (real_chain ? chain : 0);
     // rotation rounds: sub-chains have at most k_eff segments (a step takes the warp's longest)
     const uint32_t max_rounds = (c.k_eff + G - 1) / G;
+    // Shorter side (forward passes of shapes that hold at most 36 segments, where a sub-chain
+    // can be longer than half the path): turning the complement of the sub-chain, [right, N)
+    // and [0, left), by -theta about the same chord gives the moved path up to one rotation of
+    // the whole path, and the weights see only curvatures, which that rotation leaves alone.
+    // The chain then lives in a frame that turns with it. The sub-chain's chord is d minus the
+    // complement's, d = the sum of l_s t_s over the whole path in that frame: carried through
+    // every complement move (d <- R(-theta) d) and re-summed from the state every 16 steps, so
+    // that its rounding cannot build up over a long chain. (The 4 x 16 shape, N = 37..64, is
+    // left out: it gained 2 % at N = 48 and its code lost 5 % at N = 64, where no sub-chain is
+    // longer than half the path.) The incremental form turns the same side, so that it follows
+    // the full recompute's trajectory. Shapes of 4 or fewer segments per lane on more than one
+    // lane are left out too: at their 64-register budget the second code path spilled (4 x 4,
+    // N = 13..16, measured 5-25 % slower).
+    constexpr bool CMPL = MODE == kModeForward && !SHIFT && G < 32 && G * SPL <= 36 && (G == 1 || SPL > 4);
+    const bool cmpl_on = CMPL && N < 2 * c.k_eff;
+    float dX = 0.f, dY = 0.f, dZ = 0.f;
     float lse_m = 0.f, lse_s = 0.f, lse_c = 0.f;  // exact form: running max (float) and Kahan sum
     unsigned long long lse_t = 0;                   // fixed form: running max as a path total
     uint32_t valid = 0, failed = 0, clamped = 0;
@@ -546,10 +567,39 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
             const float sn = __shfl_sync(FULL, psn, jj, G);
             const float cs = __shfl_sync(FULL, pcs, jj, G);
             const uint32_t right = left + k;
-            // rounds this step needs: the longest sub-chain among the warp's chains
-            uint32_t kmax = k;
+            // the segments this chain turns: the sub-chain, or its complement where that is
+            // shorter, on the steps where that takes two or more rounds off the warp's rotation
+            // (a step that turns complements pays for the wrap and for carrying d: saving one
+            // round of three, as at N = 13 and 14 on 4 x 4, measured slower)
+            bool cm = false, use_c = false;
+            uint32_t kmax;   // the longest turned side among the warp's chains
+            if constexpr (CMPL) {
+                if (cmpl_on && ((base + jj) & 15u) == 0u) {
+                    dX = 0.f; dY = 0.f; dZ = 0.f;
 #pragma unroll
-            for (int o = G; o < 32; o <<= 1) kmax = max(kmax, __shfl_xor_sync(FULL, kmax, o));
+                    for (int m = 0; m < SPL; ++m) {   // padding slots hold zero tangents
+                        const float2 a = st.xy[Lay::xy(own, m)];
+                        const float l = st.l[j * SPL + m];
+                        dX = fmaf(l, a.x, dX);
+                        dY = fmaf(l, a.y, dY);
+                        dZ = fmaf(l, st.z[Lay::z(own, m)], dZ);
+                    }
+                    group_sum3<G>(dX, dY, dZ);
+                }
+                kmax = __reduce_max_sync(FULL, k);
+                if (cmpl_on) {
+                    const uint32_t kc = __reduce_max_sync(FULL, min(k, N - k));
+                    use_c = (kc + G - 1) / G + 2 <= (kmax + G - 1) / G;   // the same for the whole warp
+                    if (use_c) {
+                        cm = N - k < k;
+                        kmax = kc;
+                    }
+                }
+            } else {
+                kmax = k;
+#pragma unroll
+                for (int o = G; o < 32; o <<= 1) kmax = max(kmax, __shfl_xor_sync(FULL, kmax, o));
+            }
             const uint32_t rounds = min((kmax + G - 1) / G, max_rounds);
             // incremental form: the two end curvatures before the rotation (kappa_{left-1} and
             // kappa_{right-1}; left >= 1 and right <= N-1, so all four tangents exist)
@@ -568,80 +618,115 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                 }
             }
             // chord x_right - x_left = sum of l_s t_s over the k segments left .. right-1
-            // (k <= N - 2 < G * SPL, so a sub-chain never needs more than SPL rounds)
+            // (k <= N - 2 < G * SPL, so a sub-chain never needs more than SPL rounds; a
+            // complement turned instead is shorter than its sub-chain)
             constexpr int R = (kMaxSubChain + G - 1) / G < SPL ? (kMaxSubChain + G - 1) / G : SPL;
             // more than 4 rounds (8-lane groups) under the 64-register budget of 1024-thread
             // CTAs (SPL < 16): the rotation pass reloads its tangents instead of keeping every
             // round's in registers (measured: no spills, N <= 64 up to 27 % faster)
             constexpr bool RELOAD = R > 4 && (SPL < 16 || G < 8);
             constexpr int RK = RELOAD ? 1 : R;
-            float vx[RK], vy[RK], vz[RK];
-            uint32_t va[RK], vb[RK];
-            float cx = 0.f, cy = 0.f, cz = 0.f;
+            // The move: the chord of the turned segments, the axis, the rotation. WRAP: the warp
+            // turns complements this step (the chains with cm), which wrap past segment N-1 to 0,
+            // turn by -theta and carry d; a step that turns none runs the plain code.
+            auto turn = [&](auto wrap_tag) {
+                constexpr bool WRAP = decltype(wrap_tag)::value;
+                const bool cmw = WRAP && cm;
+                const uint32_t first = cmw ? right : left;
+                const uint32_t cnt = cmw ? N - k : k;
+                auto seg_of = [&](uint32_t idx) {
+                    uint32_t s = first + idx;
+                    if (WRAP && s >= N) s -= N;
+                    return s;
+                };
+                float vx[RK], vy[RK], vz[RK];
+                uint32_t va[RK], vb[RK];
+                float cx = 0.f, cy = 0.f, cz = 0.f;
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                if (r > 0 && (uint32_t)r >= rounds) break;
-                const uint32_t s = left + j + r * G;
-                const int ri = RELOAD ? 0 : r;
-                va[ri] = Lay::xy(gbase + s / SPL, s % SPL);
-                vb[ri] = Lay::z(gbase + s / SPL, s % SPL);
-                if (s < right) {
-                    const float2 a = st.xy[va[ri]];
-                    vx[ri] = a.x;
-                    vy[ri] = a.y;
-                    vz[ri] = st.z[vb[ri]];
-                    const float l = st.l[s];
-                    cx = fmaf(l, vx[ri], cx);
-                    cy = fmaf(l, vy[ri], cy);
-                    cz = fmaf(l, vz[ri], cz);
-                }
-            }
-            if constexpr (G == 32) {
-                int ix = __float2int_rn(cx * chord_scale);
-                int iy = __float2int_rn(cy * chord_scale);
-                int iz = __float2int_rn(cz * chord_scale);
-                ix = __reduce_add_sync(FULL, ix);
-                iy = __reduce_add_sync(FULL, iy);
-                iz = __reduce_add_sync(FULL, iz);
-                cx = (float)ix;
-                cy = (float)iy;
-                cz = (float)iz;
-            } else {
-                group_sum3<G>(cx, cy, cz);
-            }
-            // Rodrigues by +theta about the unit chord a -- the rotation the reference's
-            // quaternion sandwich q^-1 p q applies with its product convention:
-            // v cos + (a x v) sin + a (a.v)(1 - cos), sin = 2 s c, 1 - cos = 2 s^2 (half angle s, c)
-            const float inv = rsqrtf(fmaf(cx, cx, fmaf(cy, cy, cz * cz)));
-            const float ax = cx * inv, ay = cy * inv, az = cz * inv;
-            const float sth = 2.f * sn * cs, omc = 2.f * sn * sn;
-            __syncwarp();
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                if (r > 0 && (uint32_t)r >= rounds) break;
-                const uint32_t s = left + j + r * G;
-                const int ri = RELOAD ? 0 : r;
-                if (RELOAD) {
-                    va[0] = Lay::xy(gbase + s / SPL, s % SPL);
-                    vb[0] = Lay::z(gbase + s / SPL, s % SPL);
-                }
-                if (s < right) {
-                    if (RELOAD) {
-                        const float2 a = st.xy[va[0]];
-                        vx[0] = a.x;
-                        vy[0] = a.y;
-                        vz[0] = st.z[vb[0]];
+                for (int r = 0; r < R; ++r) {
+                    if (r > 0 && (uint32_t)r >= rounds) break;
+                    const uint32_t idx = j + r * G;
+                    const uint32_t s = seg_of(idx);
+                    const int ri = RELOAD ? 0 : r;
+                    va[ri] = Lay::xy(gbase + s / SPL, s % SPL);
+                    vb[ri] = Lay::z(gbase + s / SPL, s % SPL);
+                    if (WRAP ? idx < cnt : s < right) {
+                        const float2 a = st.xy[va[ri]];
+                        vx[ri] = a.x;
+                        vy[ri] = a.y;
+                        vz[ri] = st.z[vb[ri]];
+                        const float l = st.l[s];
+                        cx = fmaf(l, vx[ri], cx);
+                        cy = fmaf(l, vy[ri], cy);
+                        cz = fmaf(l, vz[ri], cz);
                     }
-                    const float x = vx[ri], y = vy[ri], z = vz[ri];
-                    const float crx = ay * z - az * y, cry = az * x - ax * z, crz = ax * y - ay * x;
-                    const float ad = (ax * x + ay * y + az * z) * omc;
-                    const float nx = fmaf(ax, ad, fmaf(sth, crx, fmaf(-omc, x, x)));
-                    const float ny = fmaf(ay, ad, fmaf(sth, cry, fmaf(-omc, y, y)));
-                    const float nz = fmaf(az, ad, fmaf(sth, crz, fmaf(-omc, z, z)));
-                    const float h = fmaf(renorm, fmaf(nx, nx, fmaf(ny, ny, nz * nz)), 1.5f);
-                    st.xy[va[ri]] = make_float2(nx * h, ny * h);
-                    st.z[vb[ri]] = nz * h;
                 }
+                if constexpr (G == 32) {
+                    int ix = __float2int_rn(cx * chord_scale);
+                    int iy = __float2int_rn(cy * chord_scale);
+                    int iz = __float2int_rn(cz * chord_scale);
+                    ix = __reduce_add_sync(FULL, ix);
+                    iy = __reduce_add_sync(FULL, iy);
+                    iz = __reduce_add_sync(FULL, iz);
+                    cx = (float)ix;
+                    cy = (float)iy;
+                    cz = (float)iz;
+                } else {
+                    group_sum3<G>(cx, cy, cz);
+                }
+                if (cmw) { cx = dX - cx; cy = dY - cy; cz = dZ - cz; }   // the sub-chain's chord
+                // Rodrigues by +theta about the unit chord a -- the rotation the reference's
+                // quaternion sandwich q^-1 p q applies with its product convention:
+                // v cos + (a x v) sin + a (a.v)(1 - cos), sin = 2 s c, 1 - cos = 2 s^2 (half angle s, c)
+                const float inv = rsqrtf(fmaf(cx, cx, fmaf(cy, cy, cz * cz)));
+                const float ax = cx * inv, ay = cy * inv, az = cz * inv;
+                const float sth = (cmw ? -2.f : 2.f) * sn * cs, omc = 2.f * sn * sn;
+                __syncwarp();
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    if (r > 0 && (uint32_t)r >= rounds) break;
+                    const uint32_t idx = j + r * G;
+                    const uint32_t s = seg_of(idx);
+                    const int ri = RELOAD ? 0 : r;
+                    if (RELOAD) {
+                        va[0] = Lay::xy(gbase + s / SPL, s % SPL);
+                        vb[0] = Lay::z(gbase + s / SPL, s % SPL);
+                    }
+                    if (WRAP ? idx < cnt : s < right) {
+                        if (RELOAD) {
+                            const float2 a = st.xy[va[0]];
+                            vx[0] = a.x;
+                            vy[0] = a.y;
+                            vz[0] = st.z[vb[0]];
+                        }
+                        const float x = vx[ri], y = vy[ri], z = vz[ri];
+                        const float crx = ay * z - az * y, cry = az * x - ax * z, crz = ax * y - ay * x;
+                        const float ad = (ax * x + ay * y + az * z) * omc;
+                        const float nx = fmaf(ax, ad, fmaf(sth, crx, fmaf(-omc, x, x)));
+                        const float ny = fmaf(ay, ad, fmaf(sth, cry, fmaf(-omc, y, y)));
+                        const float nz = fmaf(az, ad, fmaf(sth, crz, fmaf(-omc, z, z)));
+                        const float h = fmaf(renorm, fmaf(nx, nx, fmaf(ny, ny, nz * nz)), 1.5f);
+                        st.xy[va[ri]] = make_float2(nx * h, ny * h);
+                        st.z[vb[ri]] = nz * h;
+                    }
+                }
+                if constexpr (WRAP) {
+                    // the whole path's chord turns with the complement (selected, not branched)
+                    const float crx = ay * dZ - az * dY, cry = az * dX - ax * dZ, crz = ax * dY - ay * dX;
+                    const float ad = (ax * dX + ay * dY + az * dZ) * omc;
+                    const float nX = fmaf(ax, ad, fmaf(sth, crx, fmaf(-omc, dX, dX)));
+                    const float nY = fmaf(ay, ad, fmaf(sth, cry, fmaf(-omc, dY, dY)));
+                    const float nZ = fmaf(az, ad, fmaf(sth, crz, fmaf(-omc, dZ, dZ)));
+                    dX = cm ? nX : dX;
+                    dY = cm ? nY : dY;
+                    dZ = cm ? nZ : dZ;
+                }
+            };
+            if constexpr (CMPL) {
+                if (use_c) turn(BoolTag<true>{});
+                else turn(BoolTag<false>{});
+            } else {
+                turn(BoolTag<false>{});
             }
             __syncwarp();
             const uint32_t step = base + jj;
@@ -656,7 +741,12 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                 if constexpr (INCR) {
                     if (incr_now) {
                         // the two end curvatures after the rotation; the interior ones keep their terms
+                        // (a turned complement moved the outer tangents of the two joints instead)
                         float a1x, a1y, a1z, b0x, b0y, b0z;
+                        if (cm) {
+                            tan_at(left - 1, e0x, e0y, e0z);
+                            tan_at(right, e3x, e3y, e3z);
+                        }
                         tan_at(left, a1x, a1y, a1z);
                         tan_at(right - 1, b0x, b0y, b0z);
                         const uint32_t t_new =
