@@ -165,6 +165,8 @@ BATCH_NAME = ("batching: 4096 experiments, N log-uniform [16,1024], receivers on
 TRAFFIC_PER_LAUNCH = 106496
 # the incremental variant's full-recompute period (weighted steps)
 INCR_RESYNC = 32
+# N of the small-N figures reported beside the headline (same geometry and table, 2^24 paths)
+SMALL_N = (12, 16, 24, 32, 48, 64)
 
 
 def batch_experiments(T, n=None, seed=None):
@@ -487,6 +489,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip timing the batching workload")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint (precision line: the differentiation form; image workload: its batched adjoint)")
+    ap.add_argument("--no-small-n", action="store_true", help="skip the small-N figures")
     ap.add_argument("--paths", type=int, default=0, help="paths per pass (default 2^26; smaller for profiling)")
     ap.add_argument("--workload", default="precision", choices=["precision", "batch", "image"],
                     help="precision: one N=256 experiment (the headline); batch: 4096 uneven experiments; "
@@ -617,6 +620,25 @@ def main():
                                 "resync_every": INCR_RESYNC, "error_vs_fp64": ie, "speedup_over_value": iv / (value / ws),
                                 "note": "weights updated from the two curvatures each rotation changes, full "
                                         "recompute every resync_every-th weighted step; not the headline"}
+
+    if rank == 0 and form == T.FORM_COMPENSATED and not args.no_small_n and not args.segments:
+        # the same geometry and table at small N (2^24 paths each), where per-step work that does
+        # not scale with N bounds the kernel: events around each pass, L2 flushed between
+        small = {}
+        for n_small in SMALL_N:
+            sp = workload_params(T, form, device=device)
+            sp.num_segments = n_small
+            sp.paths_to_generate = 1 << 24
+            with T.Context(sp) as cs:
+                cs.prepare(bc)
+                sms = time_passes(T, torch, cs, max(3, min(args.steps, 5)), 1, device)
+                rs = cs.collect()
+            small[str(n_small)] = {"value": rs.total_paths * n_small / (sum(sms) / len(sms) / 1e3),
+                                   "ms_per_step": sum(sms) / len(sms), "chains": rs.num_chains,
+                                   "shape": T.default_shape(n_small, W["bins"])}
+        extra["small_n"] = {"unit": UNIT, "paths": 1 << 24, "per_n": small,
+                            "note": "the precision workload's geometry and 8192-bin table at N segments; N <= 36 "
+                                    "(except 13..16) turns the shorter side of each move"}
 
     if rank == 0 and form == T.FORM_COMPENSATED and not args.no_batch:
         # the batching form on its own workload (4096 uneven experiments), timed in this run
