@@ -165,7 +165,7 @@ BATCH_NAME = ("batching: 4096 experiments, N log-uniform [16,1024], receivers on
 TRAFFIC_PER_LAUNCH = 106496
 # the incremental variant's full-recompute period (weighted steps)
 INCR_RESYNC = 32
-# N of the small-N figures reported beside the headline (same geometry and table, 2^24 paths)
+# N of the small-N figures reported beside the headline (same geometry and table, 2^32 / N paths)
 SMALL_N = (12, 16, 24, 32, 48, 64)
 
 
@@ -622,13 +622,14 @@ def main():
                                         "recompute every resync_every-th weighted step; not the headline"}
 
     if rank == 0 and form == T.FORM_COMPENSATED and not args.no_small_n and not args.segments:
-        # the same geometry and table at small N (2^24 paths each), where per-step work that does
-        # not scale with N bounds the kernel: events around each pass, L2 flushed between
+        # the same geometry and table at small N, where per-step work that does not scale with N
+        # bounds the kernel: 2^32 path-segments per pass (2^32 / N paths, so that the 256 burn-in
+        # steps per chain stay a small share), events around each pass, L2 flushed between
         small = {}
         for n_small in SMALL_N:
             sp = workload_params(T, form, device=device)
             sp.num_segments = n_small
-            sp.paths_to_generate = 1 << 24
+            sp.paths_to_generate = (1 << 32) // n_small
             with T.Context(sp) as cs:
                 cs.prepare(bc)
                 sms = time_passes(T, torch, cs, max(3, min(args.steps, 5)), 1, device)
@@ -636,7 +637,7 @@ def main():
             small[str(n_small)] = {"value": rs.total_paths * n_small / (sum(sms) / len(sms) / 1e3),
                                    "ms_per_step": sum(sms) / len(sms), "chains": rs.num_chains,
                                    "shape": T.default_shape(n_small, W["bins"])}
-        extra["small_n"] = {"unit": UNIT, "paths": 1 << 24, "per_n": small,
+        extra["small_n"] = {"unit": UNIT, "paths": "2^32 / N", "per_n": small,
                             "note": "the precision workload's geometry and 8192-bin table at N segments; N <= 36 "
                                     "(except 13..16) turns the shorter side of each move"}
 

@@ -121,9 +121,9 @@ typedef struct twisty_params {
                                     the chain itself unchanged (finite-difference checks) */
     /* compensated-form kernel shape; 0 = chosen from N. comp_group lanes per chain (1, 4, 8, 16,
        32) x comp_spl segments per lane (>= N in total), comp_warps warps per CTA. Shapes:
-       1 x {8, 12}; 4 x {2, 3, 4, 5, 8, 9, 16, 17, 20, 24, 28, 32}; 8 x {2, 4, 8, 9, 12, 16, 17, 20,
-       24, 32}; 16 x {4, 8, 12, 16, 17, 20, 24, 28, 32}; 32 x {4, 8, 12, 16, 17, 20, 24, 28, 32}
-       (batched runs: all but 8 x 32). */
+       1 x {8, 12, 16, 24}; 4 x {2, 3, 4, 5, 8, 9, 16, 17, 20, 24, 28, 32}; 8 x {2, 4, 8, 9, 12, 16,
+       17, 20, 24, 32}; 16 x {4, 8, 12, 16, 17, 20, 24, 28, 32}; 32 x {4, 8, 12, 16, 17, 20, 24, 28,
+       32} (batched runs: all but 8 x 32, 1 x 16 and 1 x 24). */
     uint32_t comp_group;
     uint32_t comp_spl;
     uint32_t comp_warps;
@@ -382,6 +382,9 @@ twisty_status twisty_tuning_cache_load(const char *path);
  * forward pass of num_segments segments with a bins-bin weight table takes when the shape
  * knobs are zero, comp_table_memory is 0 and the tuning cache has no entry for them
  * (comp_default_tuning and the placement rule of twisty_run). Host-only: needs no device.
+ * For N = 13..24 the shape also depends on the pass: a pass takes the one-lane 1 x 16 (N <= 16)
+ * or 1 x 24 only when its paths_to_generate reaches 60000 or 130000 times its paths_to_skip
+ * (shorter passes take 4 x 4, 4 x 5 or 4 x 8); this reports the long pass's shape.
  * TWISTY_ERR_INVALID_ARGUMENT for a null out, N < 4 or bins < 2; TWISTY_ERR_UNSUPPORTED
  * when no shape covers N (N > 1024). */
 typedef struct twisty_shape {
@@ -390,7 +393,9 @@ typedef struct twisty_shape {
     uint32_t warps;         /* warps per CTA */
     uint32_t table_in_l1;   /* 1: the table is gathered through L1; 0: staged in shared memory */
     uint32_t smem_bytes;    /* dynamic shared memory per CTA */
-    uint32_t batched;       /* 1: twisty_run_batch has a kernel of this shape */
+    uint32_t batched;       /* 1: twisty_run_batch has a kernel of this shape (0 for the one-lane
+                               1 x 16 and 1 x 24 of N = 13..24: batched runs of such N take 4 x 4,
+                               4 x 5 or 4 x 8) */
 } twisty_shape;
 twisty_status twisty_default_shape(uint32_t num_segments, uint32_t bins, twisty_shape *out);
 
@@ -420,7 +425,7 @@ twisty_status twisty_measure_fp32_peak(int device, double *lane_instr_per_s);
  * as the device's context: do not call this entry point again after cudaDeviceReset in the
  * same process.
  *
- * The kernel shape and table placement are twisty_run's defaults for N and bins
+ * The kernel shape and table placement are twisty_run's defaults for N, bins and the pass
  * (twisty_default_shape): the table is staged in shared memory when it fits beside the
  * chain state, else gathered through L1. bins is at most TWISTY_NOALLOC_MAX_BINS. */
 #define TWISTY_NOALLOC_MAX_CHAINS 16384u

@@ -16,7 +16,7 @@ import twisty_b200 as T
 
 pytestmark = pytest.mark.gpu
 
-NS = [4, 5, 6, 7, 8, 9, 10, 12, 16, 17, 18, 20, 31, 32, 33, 34, 36, 48, 64, 65, 66, 72, 76, 80, 96, 100, 128, 129, 130,
+NS = [4, 5, 6, 7, 8, 9, 10, 12, 13, 14, 16, 17, 18, 20, 31, 32, 33, 34, 36, 48, 64, 65, 66, 72, 76, 80, 96, 100, 128, 129, 130,
       136, 150, 160, 170, 192, 200, 256, 257, 258, 272, 300, 320, 350, 384, 400, 420, 448, 512, 513, 514, 544, 600, 640, 768, 800, 850, 896,
       1000, 1024]
 
@@ -67,10 +67,13 @@ def test_shapes_agree_on_the_same_chains(N, shapes):
 
 
 @pytest.mark.parametrize("N,shape", [(80, (4, 20, 24)), (90, (4, 24, 20)), (96, (4, 24, 24)), (112, (4, 28, 16)),
-                                     (100, (4, 28, 20)), (128, (4, 32, 12)), (120, (4, 32, 16))])
+                                     (100, (4, 28, 20)), (128, (4, 32, 12)), (120, (4, 32, 16)),
+                                     (16, (4, 4, 32)), (16, (1, 16, 16)), (13, (1, 16, 24)), (24, (1, 24, 16)),
+                                     (20, (1, 24, 12)), (18, (1, 24, 16))])
 def test_explicit_shape_matches_fp64(N, shape):
-    """Shapes the defaults do not pick at these N (the autotuner's candidates), full and padded,
-    with the table staged and through L1, against the FP64 form on the same proposals."""
+    """Shapes the defaults do not pick at these N (the autotuner's candidates, among them the
+    one-lane 1 x 16 and 1 x 24 that long passes take at N = 13..24), full and padded, with the
+    table staged and through L1, against the FP64 form on the same proposals."""
     g, spl, w = shape
     with T.Context(_params(N, T.FORM_COMPENSATED, comp_group=g, comp_spl=spl, comp_warps=w)) as ctx:
         a = ctx.run(_bc(N))

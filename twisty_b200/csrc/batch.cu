@@ -26,7 +26,8 @@ void batch_pack_experiments(const BatchExpHost *in, uint32_t n, void *dst)
 
 bool batch_shape_supported(const BatchShape &s, uint32_t n_max, uint32_t k_eff)
 {
-    if (s.group == 8 && s.spl == 32) return false;   // a single-run shape only: no batched variant
+    // single-run shapes only: no batched variant
+    if ((s.group == 8 && s.spl == 32) || (s.group == 1 && (s.spl == 16 || s.spl == 24))) return false;
     CompTuning t{s.group, s.spl, s.warps, s.exact};
     const int maxt = batch_max_threads(s.group, s.spl);
     return comp_tuning_supported(t, n_max, k_eff) && s.warps * 32 <= maxt;

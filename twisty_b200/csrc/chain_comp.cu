@@ -69,7 +69,8 @@ cudaError_t launch_mode(int mode, const ChainSpec &c, const CompTuning &t, const
     cudaError_t e = cudaSuccess;
     if (launch_comp_shapes_a(a, e) || launch_comp_shapes_b(a, e) || launch_comp_shapes_c(a, e) ||
         launch_comp_shapes_d(a, e) || launch_comp_shapes_e(a, e) || launch_comp_shapes_f(a, e) ||
-        launch_comp_shapes_g(a, e) || launch_comp_shapes_h(a, e))
+        launch_comp_shapes_g(a, e) || launch_comp_shapes_h(a, e) ||
+        launch_comp_shapes_i(a, e))
         return e;
     return cudaErrorInvalidValue;
 }
@@ -176,13 +177,25 @@ bool comp_table_needs_clamp(float inv_ds, const LutMetaF &m)
 // segment per lane more than a power of two (3, 5, 9, 17)
 // serve N = 2^k + 2, the N of the reference's own configurations (10, 18, 34, 66, 130, 258,
 // 514), which would otherwise pad to the next power of two.
-CompTuning comp_default_tuning(uint32_t n)
+// Since chains of up to 36 segments turn the shorter side of each move, one lane per chain
+// also wins at N = 13..24 on long passes: 1 x 16 (N = 13..16) and 1 x 24 (17..24) at 16 warps
+// measured +35-42 % and +15-19 % over 4 x {4, 5, 8} on passes of 2^32 path-segments. They run
+// twice as many chains, each of which pays the burn-in, at 0.72 (1 x 16) and 0.81 (1 x 24) of
+// the cost per weighted step (both fitted to those runs), so they win once a pass's paths reach
+// about 58000 and 125000 times its burn-in steps per chain; the thresholds below round those up.
+// (At 2^24 paths and 256 burn-in steps: 1 x 16 +5 % at N = 16, 1 x 24 4-10 % slower.) The
+// batched kernels have neither one-lane shape.
+CompTuning comp_default_tuning(uint32_t n, bool batched, uint64_t paths, uint64_t burn_in)
 {
     CompTuning t;
     t.exact_blend = 0;
+    const bool lane16 = !batched && paths / 60000u >= burn_in;
+    const bool lane24 = !batched && paths / 130000u >= burn_in;
     if (n <= 8) { t.group = 1; t.spl = 8; t.warps_per_block = 32; }
     else if (n <= 12) { t.group = 1; t.spl = 12; t.warps_per_block = 24; }
+    else if (n <= 16 && lane16) { t.group = 1; t.spl = 16; t.warps_per_block = 16; }
     else if (n <= 16) { t.group = 4; t.spl = 4; t.warps_per_block = 32; }
+    else if (n <= 24 && lane24) { t.group = 1; t.spl = 24; t.warps_per_block = 16; }
     else if (n <= 20) { t.group = 4; t.spl = 5; t.warps_per_block = 32; }
     else if (n <= 32) { t.group = 4; t.spl = 8; t.warps_per_block = 32; }
     else if (n <= 36) { t.group = 4; t.spl = 9; t.warps_per_block = 32; }
@@ -225,7 +238,7 @@ int comp_stage_min_warps(const CompTuning &t)
 bool comp_tuning_supported(const CompTuning &t, uint32_t n, uint32_t k_eff)
 {
     const int s = t.spl;
-    const bool shape = (t.group == 1 && (s == 8 || s == 12)) ||
+    const bool shape = (t.group == 1 && (s == 8 || s == 12 || s == 16 || s == 24)) ||
                        (t.group == 4 && (s == 2 || s == 3 || s == 4 || s == 5 || s == 8 || s == 9 || s == 16 || s == 17 || s == 20 ||
                                          s == 24 || s == 28 || s == 32)) ||
                        (t.group == 8 && (s == 2 || s == 4 || s == 8 || s == 9 || s == 12 || s == 16 || s == 17 || s == 20 ||
@@ -236,12 +249,6 @@ bool comp_tuning_supported(const CompTuning &t, uint32_t n, uint32_t k_eff)
                                           s == 28 || s == 32));
     return shape && (uint32_t)(t.group * t.spl) >= n && n >= 4 && k_eff <= (uint32_t)kMaxSubChain &&
            t.warps_per_block >= 1 && t.warps_per_block * 32 <= comp_max_threads(t.group, t.spl);
-}
-
-uint32_t comp_default_chains(uint32_t n, int sm_count)
-{
-    const CompTuning t = comp_default_tuning(n);
-    return (uint32_t)sm_count * t.warps_per_block * (32 / t.group);
 }
 
 size_t comp_smem_bytes(const CompTuning &t, uint32_t bins)

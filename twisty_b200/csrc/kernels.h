@@ -125,10 +125,12 @@ struct CompTuning {
     int lut_global = 0;      // 1: gather the table through L1 instead of staging it in shared memory
                              // (forward passes only; the chain state keeps the shared memory)
 };
-CompTuning comp_default_tuning(uint32_t n_segments);
+// The default shape of N segments for a pass of `paths` weighted paths with `burn_in` steps per
+// chain (the defaults: a long pass); batched: among the shapes the batched kernels have.
+CompTuning comp_default_tuning(uint32_t n_segments, bool batched = false, uint64_t paths = ~0ull,
+                               uint64_t burn_in = 0);
 int comp_stage_min_warps(const CompTuning &t);
 bool comp_tuning_supported(const CompTuning &t, uint32_t n_segments, uint32_t k_eff);
-uint32_t comp_default_chains(uint32_t n_segments, int sm_count);
 size_t comp_smem_bytes(const CompTuning &t, uint32_t bins);
 // Shared memory a CTA may use (B200: 227 KB).
 constexpr size_t kCompSmemCap = 227 * 1024;

@@ -103,7 +103,7 @@ extern "C" twisty_status twisty_run_noalloc(const twisty_noalloc_args *a, void *
 
     // the default shape and table placement of twisty_run's forward pass (shared memory when the
     // table fits beside the shape's chain state, else gathered through L1)
-    CompTuning t = comp_default_tuning(N);
+    CompTuning t = comp_default_tuning(N, false, a->paths, a->burn_in);
     t.exact_blend = 1;  // the table is the linear (L_i, L_{i+1} - L_i) form
     if (!comp_tuning_supported(t, N, c.k_eff)) return bad("no compensated kernel shape for this N");
     t.lut_global = comp_table_through_l1(t, a->bins, true) ? 1 : 0;

@@ -538,7 +538,7 @@ void prepare(twisty_ctx *ctx, const twisty_bc *bcp)
         // one CombinedWeightValues_C per chain holds at most 1e6 paths (CombinedWeightUtils.h:22-24)
         max_steps = std::min<uint32_t>(max_steps, 1000000u);
     } else if (p.form == TWISTY_FORM_COMPENSATED) {
-        ctx->tuning = comp_default_tuning(N);
+        ctx->tuning = comp_default_tuning(N, false, p.paths_to_generate, p.paths_to_skip);
         if (!p.comp_group && !p.comp_spl && !p.comp_warps) tune_lookup(ctx->device_name, N, p.num_curvature_steps, ctx->tuning);
         if (p.comp_group || p.comp_spl) {
             if (!p.comp_group || !p.comp_spl) fail(TWISTY_ERR_INVALID_CONFIG, "comp_group and comp_spl are set together");
@@ -1363,7 +1363,7 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
         h.seg_off = n_seg_floats;
         n_seg_floats += 3 * N;
         // kernel shape and chain layout: whole CTAs of chains, ~2048 steps per chain
-        h.t = comp_default_tuning(N);
+        h.t = comp_default_tuning(N, true);
         {
             // a tuned shape the batched kernel does not have keeps the default
             CompTuning tuned = h.t;
