@@ -6,7 +6,9 @@ result live in torch tensors the test allocates, and the entry point itself only
 scratch array compiled into the library. Its result must match the context-based
 twisty_run on the same table, initial curve and proposals, on two calls in a row (the
 second call reuses the shared scratch the first one filled). The cases cover the kernel
-shapes 4 x 16, 4 x 17, 8 x 24, 16 x 24 and 32 x 24 (N = 64, 66, 192, 384, 768) and both table placements:
+shapes 1 x 16, 1 x 24 (N = 16, 24, whose passes here are long against their 2 burn-in steps,
+so both entry points take the one-lane shapes, which also turn the shorter side of each move),
+4 x 16, 4 x 17, 8 x 24, 16 x 24 and 32 x 24 (N = 64, 66, 192, 384, 768) and both table placements:
 a 4096-bin table staged in shared memory and a 20000-bin table gathered through L1 where
 staging it would cost the shape warps.
 
@@ -25,12 +27,12 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("bins", [4096, 20000])
-@pytest.mark.parametrize("N", [64, 66, 192, 384, 768])
+@pytest.mark.parametrize("N", [16, 24, 64, 66, 192, 384, 768])
 def test_noalloc_pass_matches_twisty_run_twice(N, bins):
     import torch
 
     S = 0.16 * N
-    chains, steps, burn = 4096, 100 if N <= 192 else 40, 50
+    chains, steps, burn = 4096, 100 if N <= 192 else 40, 2 if N <= 24 else 50
     p = T.default_params(num_segments=N, mu=1.0, eps=0.01, scatter=10.0, num_steps_int=4000,
                          num_curvature_steps=bins, form=T.FORM_COMPENSATED, lut_mode=T.LUT_FP64,
                          perturb_seed=77, num_chains=chains, paths_to_generate=chains * steps,
