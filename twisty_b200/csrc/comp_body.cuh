@@ -586,6 +586,8 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                     }
                     group_sum3<G>(dX, dY, dZ);
                 }
+                // whole-warp reductions: every chain of a warp belongs to one experiment (a CTA
+                // runs one experiment's work item at a time), so cmpl_on is the same in every lane
                 kmax = __reduce_max_sync(FULL, k);
                 if (cmpl_on) {
                     const uint32_t kc = __reduce_max_sync(FULL, min(k, N - k));
