@@ -178,7 +178,9 @@ typedef struct twisty_result {
     double weight_error_bound;
     double fp64_rel_error;
     uint32_t fp64_check_chains;
-    uint32_t reserved;
+    /* The compensated form's kernel shape that ran: lanes per chain << 8 | segments per lane
+       (0x0110 = 1 x 16); 0 for the other forms. No reference counterpart. */
+    uint32_t kernel_shape;
 } twisty_result;
 
 enum {

@@ -105,7 +105,7 @@ class Result(C.Structure):
         ("weight_error_bound", C.c_double),
         ("fp64_rel_error", C.c_double),
         ("fp64_check_chains", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("kernel_shape", C.c_uint32),
     ]
 
 

@@ -691,6 +691,7 @@ void collect(twisty_ctx *ctx, twisty_result *res)
         const bool exact = ctx->tuning.exact_blend || ctx->lf.inv_scale == 0.0 || ctx->spec.has_eval_shift;
         res->table_form = exact ? TWISTY_TABLE_EXACT_BLEND : ctx->lf.wide ? TWISTY_TABLE_FIXED_WIDE : TWISTY_TABLE_FIXED_NARROW;
         res->steep_bins = exact ? 0u : (uint32_t)ctx->lf.steep;
+        res->kernel_shape = ((uint32_t)ctx->tuning.group << 8) | (uint32_t)ctx->tuning.spl;
         // per segment: entry and correction each rounded to 2^-(s+1), plus the secant's error;
         // exact blend: the float blend and the hardware log2 (under 4e-7 in log10 together)
         res->weight_error_bound = exact ? segs * 4e-7 : segs * (ctx->lf.inv_scale + ctx->secant_err);
@@ -1646,6 +1647,7 @@ void run_batch(twisty_ctx *ctx, const twisty_experiment *ex, uint32_t n, uint32_
         const bool fixed = bh[e].lf.inv_scale != 0.0;
         r.table_form = fixed ? (lf[e].wide ? TWISTY_TABLE_FIXED_WIDE : TWISTY_TABLE_FIXED_NARROW) : TWISTY_TABLE_EXACT_BLEND;
         r.steep_bins = fixed ? (uint32_t)lf[e].steep : 0u;
+        r.kernel_shape = ((uint32_t)eh[e].t.group << 8) | (uint32_t)eh[e].t.spl;
         // the device-built tables keep every secant within 1e-7 (steeper bins are re-weighed exactly)
         r.weight_error_bound = (double)(eh[e].N - 1) * (fixed ? bh[e].lf.inv_scale + 1e-7 : 4e-7);
         r.fp64_rel_error = std::numeric_limits<double>::quiet_NaN();
