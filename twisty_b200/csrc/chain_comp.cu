@@ -1,6 +1,6 @@
 // chain_comp.cu -- single-run entry points of the compensated form: the weigher of given
 // paths, the launchers and the kernel-shape table. The chain kernel (comp_launch.cuh, body in
-// comp_body.cuh) is instantiated per shape in comp_shapes_{a..h}.cu, compiled in parallel.
+// comp_body.cuh) is instantiated per shape in comp_shapes_{a..i}.cu, compiled in parallel.
 #include "comp_launch.cuh"
 
 namespace twisty {

@@ -1,5 +1,5 @@
 // comp_launch.cuh -- the compensated chain kernel and its per-shape launcher, included by the
-// translation units that instantiate it (comp_shapes_{a..h}.cu, a few shapes each, so that the
+// translation units that instantiate it (comp_shapes_{a..i}.cu, a few shapes each, so that the
 // many template variants compile in parallel) and by chain_comp.cu, which dispatches to them.
 #pragma once
 #include "comp_body.cuh"
