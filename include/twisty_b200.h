@@ -121,9 +121,9 @@ typedef struct twisty_params {
                                     the chain itself unchanged (finite-difference checks) */
     /* compensated-form kernel shape; 0 = chosen from N. comp_group lanes per chain (1, 4, 8, 16,
        32) x comp_spl segments per lane (>= N in total), comp_warps warps per CTA. Shapes:
-       1 x {8, 12, 16, 24}; 4 x {2, 3, 4, 5, 8, 9, 16, 17, 20, 24, 28, 32}; 8 x {2, 4, 8, 9, 12, 16,
-       17, 20, 24, 32}; 16 x {4, 8, 12, 16, 17, 20, 24, 28, 32}; 32 x {4, 8, 12, 16, 17, 20, 24, 28,
-       32} (batched runs: all but 8 x 32, 1 x 16 and 1 x 24). */
+       1 x {8, 12, 16, 24}; 4 x {2, 3, 4, 5, 8, 9, 12, 16, 17, 20, 24, 28, 32}; 8 x {2, 4, 8, 9, 12,
+       16, 17, 20, 24, 32}; 16 x {4, 8, 12, 16, 17, 20, 24, 28, 32}; 32 x {4, 8, 12, 16, 17, 20, 24,
+       28, 32} (batched runs: all but 8 x 32, 1 x 16, 1 x 24 and 4 x 12). */
     uint32_t comp_group;
     uint32_t comp_spl;
     uint32_t comp_warps;
@@ -396,8 +396,8 @@ typedef struct twisty_shape {
     uint32_t table_in_l1;   /* 1: the table is gathered through L1; 0: staged in shared memory */
     uint32_t smem_bytes;    /* dynamic shared memory per CTA */
     uint32_t batched;       /* 1: twisty_run_batch has a kernel of this shape (0 for the one-lane
-                               1 x 16 and 1 x 24 of N = 13..24: batched runs of such N take 4 x 4,
-                               4 x 5 or 4 x 8) */
+                               1 x 16 and 1 x 24 of N = 13..24 and for 4 x 12 of N = 37..48:
+                               batched runs of such N take 4 x 4, 4 x 5, 4 x 8 or 4 x 16) */
 } twisty_shape;
 twisty_status twisty_default_shape(uint32_t num_segments, uint32_t bins, twisty_shape *out);
 

@@ -201,8 +201,8 @@ def test_reference_bootstrapper_refuses_other_n():
 def test_default_shape_covers_every_n_and_table_size():
     """twisty_default_shape (host-only): every N from 4 to 1024 has a shape that covers it, fits
     in shared memory with its table staged or through L1, and has a batched kernel except the
-    one-lane 1 x 16 and 1 x 24 of long passes at N = 13..24 (batched runs take 4-lane shapes
-    there); tables of up to 4096 bins are staged, 100000-bin tables go through L1."""
+    one-lane 1 x 16 and 1 x 24 of long passes at N = 13..24 and 4 x 12 at N = 37..48 (batched
+    runs take other 4-lane shapes there); tables of up to 4096 bins are staged, 100000-bin tables go through L1."""
     import twisty_b200 as T
     for bins in (256, 2048, 4096, 8192, 20000, 100000):
         for n in range(4, 1025):
@@ -212,6 +212,8 @@ def test_default_shape_covers_every_n_and_table_size():
             assert s["smem_bytes"] <= 227 * 1024, (n, bins, s)
             if 13 <= n <= 24:
                 assert (s["group"], s["spl"], s["batched"]) == (1, 16 if n <= 16 else 24, 0), (n, bins, s)
+            elif 37 <= n <= 48:
+                assert (s["group"], s["spl"], s["batched"]) == (4, 12, 0), (n, bins, s)
             else:
                 assert s["batched"] == 1, (n, bins, s)
             if bins <= 4096:

@@ -16,7 +16,7 @@ import twisty_b200 as T
 
 pytestmark = pytest.mark.gpu
 
-NS = [4, 5, 6, 7, 8, 9, 10, 12, 13, 14, 16, 17, 18, 20, 31, 32, 33, 34, 36, 48, 64, 65, 66, 72, 76, 80, 96, 100, 128, 129, 130,
+NS = [4, 5, 6, 7, 8, 9, 10, 12, 13, 14, 16, 17, 18, 20, 31, 32, 33, 34, 36, 40, 48, 64, 65, 66, 72, 76, 80, 96, 100, 128, 129, 130,
       136, 150, 160, 170, 192, 200, 256, 257, 258, 272, 300, 320, 350, 384, 400, 420, 448, 512, 513, 514, 544, 600, 640, 768, 800, 850, 896,
       1000, 1024]
 

@@ -1,14 +1,15 @@
 """Small N against the oracle's FP64 twin chains, through the C ABI. Needs a B200.
 
-Below N = 37 the compensated form runs code paths of its own: forward passes turn the
+Below N = 49 the compensated form runs code paths of its own: forward passes turn the
 complement of a sub-chain longer than half the path (the moved path up to one rotation of the
 whole path, with the path's end-to-end chord carried through those moves); groups of 1 and 4
 lanes apply each rotation as v + (R - I) v; long passes at N = 13..24 take the one-lane shapes
-1 x 16 and 1 x 24. Every chain here is compared, as a whole run, with the oracle's FP64 chains
-(oracle/twisty_oracle.c, which turns the sub-chain itself by the reference's quaternion
-rotation) on the same proposals (Philox stream, chain ids, burn-in), initial curve and FP64
-table. Small rotation angles keep the FP32 and FP64 trajectories together, so the estimates
-agree to the FP32 trajectory's rounding: 1.5e-7 of |log10 W| plus 1e-5.
+1 x 16 and 1 x 24; N = 37..48 take 4 x 12, which turns the shorter side as well. Every chain
+here is compared, as a whole run, with the oracle's FP64 chains (oracle/twisty_oracle.c,
+which turns the sub-chain itself by the reference's quaternion rotation) on the same
+proposals (Philox stream, chain ids, burn-in), initial curve and FP64 table. Small rotation
+angles keep the FP32 and FP64 trajectories together, so the estimates agree to the FP32
+trajectory's rounding: 1.5e-7 of |log10 W| plus 1e-5.
 """
 import numpy as np
 import pytest
@@ -38,6 +39,8 @@ CASES = [
     (24, 8, None, (4, 8)),
     (32, 4, None, (4, 8)),
     (36, 4, None, (4, 9)),
+    (40, 4, None, (4, 12)),
+    (48, 4, None, (4, 12)),
     (20, 4, (4, 5, 32), (4, 5)),
 ]
 

@@ -27,7 +27,8 @@ void batch_pack_experiments(const BatchExpHost *in, uint32_t n, void *dst)
 bool batch_shape_supported(const BatchShape &s, uint32_t n_max, uint32_t k_eff)
 {
     // single-run shapes only: no batched variant
-    if ((s.group == 8 && s.spl == 32) || (s.group == 1 && (s.spl == 16 || s.spl == 24))) return false;
+    if ((s.group == 8 && s.spl == 32) || (s.group == 1 && (s.spl == 16 || s.spl == 24)) ||
+        (s.group == 4 && s.spl == 12)) return false;
     CompTuning t{s.group, s.spl, s.warps, s.exact};
     const int maxt = batch_max_threads(s.group, s.spl);
     return comp_tuning_supported(t, n_max, k_eff) && s.warps * 32 <= maxt;

@@ -183,8 +183,11 @@ bool comp_table_needs_clamp(float inv_ds, const LutMetaF &m)
 // twice as many chains, each of which pays the burn-in, at 0.72 (1 x 16) and 0.81 (1 x 24) of
 // the cost per weighted step (both fitted to those runs), so they win once a pass's paths reach
 // about 58000 and 125000 times its burn-in steps per chain; the thresholds below round those up.
-// (At 2^24 paths and 256 burn-in steps: 1 x 16 +5 % at N = 16, 1 x 24 4-10 % slower.) The
-// batched kernels have neither one-lane shape.
+// (At 2^24 paths and 256 burn-in steps: 1 x 16 +5 % at N = 16, 1 x 24 4-10 % slower.)
+// 4 x 12, which also turns the shorter side, serves N = 37..48 with less padding than 4 x 16:
+// +16-19 % at N = 37, 40 and +8-13 % at 44, 48, on passes of 2^24 paths and of 2^32
+// path-segments alike (+3-8 % without the shorter side). The batched kernels have neither
+// one-lane shape nor 4 x 12.
 CompTuning comp_default_tuning(uint32_t n, bool batched, uint64_t paths, uint64_t burn_in)
 {
     CompTuning t;
@@ -199,6 +202,7 @@ CompTuning comp_default_tuning(uint32_t n, bool batched, uint64_t paths, uint64_
     else if (n <= 20) { t.group = 4; t.spl = 5; t.warps_per_block = 32; }
     else if (n <= 32) { t.group = 4; t.spl = 8; t.warps_per_block = 32; }
     else if (n <= 36) { t.group = 4; t.spl = 9; t.warps_per_block = 32; }
+    else if (n <= 48 && !batched) { t.group = 4; t.spl = 12; t.warps_per_block = 24; }
     else if (n <= 64) { t.group = 4; t.spl = 16; t.warps_per_block = 24; }
     else if (n <= 68) { t.group = 4; t.spl = 17; t.warps_per_block = 24; }
     else if (n <= 72) { t.group = 8; t.spl = 9; t.warps_per_block = 32; }
@@ -239,7 +243,7 @@ bool comp_tuning_supported(const CompTuning &t, uint32_t n, uint32_t k_eff)
 {
     const int s = t.spl;
     const bool shape = (t.group == 1 && (s == 8 || s == 12 || s == 16 || s == 24)) ||
-                       (t.group == 4 && (s == 2 || s == 3 || s == 4 || s == 5 || s == 8 || s == 9 || s == 16 || s == 17 || s == 20 ||
+                       (t.group == 4 && (s == 2 || s == 3 || s == 4 || s == 5 || s == 8 || s == 9 || s == 12 || s == 16 || s == 17 || s == 20 ||
                                          s == 24 || s == 28 || s == 32)) ||
                        (t.group == 8 && (s == 2 || s == 4 || s == 8 || s == 9 || s == 12 || s == 16 || s == 17 || s == 20 ||
                                          s == 24 || s == 32)) ||

@@ -8,7 +8,7 @@
 // weights, and accumulate the path weight into the experiment's running sum.
 //
 // B200 layout and arithmetic:
-//  * G lanes cooperate on one chain (G = 8, 16 or 32); lane j owns the SPL contiguous
+//  * G lanes cooperate on one chain (G = 1, 4, 8, 16 or 32); lane j owns the SPL contiguous
 //    segments j*SPL .. j*SPL+SPL-1. The chain lives in shared memory as its unit tangents
 //    t_i and segment lengths l_i. Rotating the points between left and right about the
 //    chord x_right - x_left turns every tangent t_left .. t_{right-1} by the same rotation
@@ -26,8 +26,10 @@
 //  * Rotation: the chord is summed across the group (for full-warp groups as 32-bit fixed
 //    point with the warp reduction instruction, scaled by the chain's longest segment so
 //    that 64 segments cannot overflow; otherwise by float shuffles), normalised, and each
-//    tangent in the sub-chain is turned by Rodrigues' formula with the angle's sin and
-//    1 - cos taken from the proposal's half-angle sine and cosine.
+//    tangent in the sub-chain is turned by Rodrigues' formula (groups of 1 and 4 lanes: by
+//    v + (R - I) v, the matrix built once per step) with the angle's sin and 1 - cos taken
+//    from the proposal's half-angle sine and cosine. Forward passes of short chains turn the
+//    complement of a sub-chain longer than half the path instead (chain_body).
 //  * The table is staged once per CTA in shared memory as float2. In the fixed-point form
 //    entry i holds round((log10 L_i - c0) 2^s) as uint32 bits and the change of log10 of
 //    the blend across the bin (secant): a segment costs one 8-byte LDS, one integer add
@@ -492,8 +494,8 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
     const uint32_t gchain = c.chain0 + (real_chain ? chain : 0);
     // rotation rounds: sub-chains have at most k_eff segments (a step takes the warp's longest)
     const uint32_t max_rounds = (c.k_eff + G - 1) / G;
-    // Shorter side (forward passes of shapes that hold at most 36 segments, where a sub-chain
-    // can be longer than half the path): turning the complement of the sub-chain, [right, N)
+    // Shorter side (forward passes of shapes that hold at most 36 segments, and 4 x 12, where a
+    // sub-chain can be longer than half the path): turning the complement of the sub-chain, [right, N)
     // and [0, left), by -theta about the same chord gives the moved path up to one rotation of
     // the whole path, and the weights see only curvatures, which that rotation leaves alone.
     // The chain then lives in a frame that turns with it. The sub-chain's chord is d minus the
@@ -501,11 +503,13 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
     // every complement move (d <- R(-theta) d) and re-summed from the state every 16 steps, so
     // that its rounding cannot build up over a long chain. (The 4 x 16 shape, N = 37..64, is
     // left out: it gained 2 % at N = 48 and its code lost 5 % at N = 64, where no sub-chain is
-    // longer than half the path.) The incremental form turns the same side, so that it follows
+    // longer than half the path; 4 x 12 took N = 37..48 from it, +5-10 % with the shorter side
+    // over without.) The incremental form turns the same side, so that it follows
     // the full recompute's trajectory. Shapes of 4 or fewer segments per lane on more than one
     // lane are left out too: at their 64-register budget the second code path spilled (4 x 4,
     // N = 13..16, measured 5-25 % slower).
-    constexpr bool CMPL = MODE == kModeForward && !SHIFT && G < 32 && G * SPL <= 36 && (G == 1 || SPL > 4);
+    constexpr bool CMPL = MODE == kModeForward && !SHIFT && G < 32 && (G * SPL <= 36 || (G == 4 && SPL == 12)) &&
+                          (G == 1 || SPL > 4);
     const bool cmpl_on = CMPL && N < 2 * c.k_eff;
     float dX = 0.f, dY = 0.f, dZ = 0.f;
     float lse_m = 0.f, lse_s = 0.f, lse_c = 0.f;  // exact form: running max (float) and Kahan sum

@@ -32,7 +32,7 @@ bool launch_comp_shapes_e(const CompLaunch &a, cudaError_t &e);   // 32 x {16, 2
 bool launch_comp_shapes_f(const CompLaunch &a, cudaError_t &e);   // 16 x 20, 32 x {20, 28}
 bool launch_comp_shapes_g(const CompLaunch &a, cudaError_t &e);   // 8 x {20, 24}, 16 x {24, 28, 32}
 bool launch_comp_shapes_h(const CompLaunch &a, cudaError_t &e);   // 4 x {20, 24, 28, 32}
-bool launch_comp_shapes_i(const CompLaunch &a, cudaError_t &e);   // 1 x {16, 24}
+bool launch_comp_shapes_i(const CompLaunch &a, cudaError_t &e);   // 1 x {16, 24}, 4 x 12
 
 namespace {
 
