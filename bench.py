@@ -638,8 +638,8 @@ def main():
                                    "ms_per_step": sum(sms) / len(sms), "chains": rs.num_chains,
                                    "shape": T.default_shape(n_small, W["bins"])}
         extra["small_n"] = {"unit": UNIT, "paths": "2^32 / N", "per_n": small,
-                            "note": "the precision workload's geometry and 8192-bin table at N segments; N <= 36 "
-                                    "(except 13..16) turns the shorter side of each move"}
+                            "note": "the precision workload's geometry and 8192-bin table at N segments; up to "
+                                    "N = 48 the kernels (all shapes but 4 x 4) turn the shorter side of each move"}
 
     if rank == 0 and form == T.FORM_COMPENSATED and not args.no_batch:
         # the batching form on its own workload (4096 uneven experiments), timed in this run
