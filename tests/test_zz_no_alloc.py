@@ -8,7 +8,7 @@ twisty_run on the same table, initial curve and proposals, on two calls in a row
 second call reuses the shared scratch the first one filled). The cases cover the kernel
 shapes 1 x 16, 1 x 24 (N = 16, 24, whose passes here are long against their 2 burn-in steps,
 so both entry points take the one-lane shapes, which also turn the shorter side of each move),
-4 x 16, 4 x 17, 8 x 24, 16 x 24 and 32 x 24 (N = 64, 66, 192, 384, 768) and both table placements:
+4 x 12 (N = 40, which turns the shorter side too), 4 x 16, 4 x 17, 8 x 24, 16 x 24 and 32 x 24 (N = 64, 66, 192, 384, 768) and both table placements:
 a 4096-bin table staged in shared memory and a 20000-bin table gathered through L1 where
 staging it would cost the shape warps.
 
@@ -27,7 +27,7 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("bins", [4096, 20000])
-@pytest.mark.parametrize("N", [16, 24, 64, 66, 192, 384, 768])
+@pytest.mark.parametrize("N", [16, 24, 40, 64, 66, 192, 384, 768])
 def test_noalloc_pass_matches_twisty_run_twice(N, bins):
     import torch
 
