@@ -22,7 +22,8 @@
 //    full recompute reads consecutive columns of one row: conflict-free). Row pitches
 //    (32 + 16/SPL float2, 32 + G/SPL floats) shift successive rows by distinct banks so
 //    the k consecutive segments of a rotation fall in distinct banks (at most 2-way
-//    conflicts). The next lane's first tangent comes by shuffle.
+//    conflicts); one-lane shapes keep rows of 32 (comp_pitch_xy). The next lane's first
+//    tangent comes by shuffle.
 //  * Rotation: the chord is summed across the group (for full-warp groups as 32-bit fixed
 //    point with the warp reduction instruction, scaled by the chain's longest segment so
 //    that 64 segments cannot overflow; otherwise by float shuffles), normalised, and each
@@ -316,10 +317,19 @@ __device__ __forceinline__ unsigned long long path_fixed(uint32_t j, uint32_t gb
     return (unsigned long long)group_sum<G>(isum);
 }
 
+// Row pitches of a warp's planes (float2 and float elements). With several lanes per chain
+// the rows are padded so that the consecutive segments of one rotation, spread over lanes and
+// rows, fall in distinct banks. With one lane per chain every lane is its own chain: a rotation
+// has the lanes at unrelated rows, and an unpadded row of 32 puts lane i in bank (pair) i mod
+// 16 (32) whatever its row, so no access conflicts (the padded pitch measured the one-lane
+// kernel bound by shared-memory wavefronts at 92 % of their peak).
+__host__ __device__ constexpr int comp_pitch_xy(int G, int SPL) { return G == 1 ? 32 : 32 + ((16 / SPL) > 1 ? (16 / SPL) : 1); }
+__host__ __device__ constexpr int comp_pitch_z(int G, int SPL) { return G == 1 ? 32 : 32 + ((G / SPL) > 1 ? (G / SPL) : 1); }
+
 template <int G, int SPL>
 struct Layout {
-    static constexpr int PXY = 32 + ((16 / SPL) > 1 ? (16 / SPL) : 1);  // float2 plane pitch
-    static constexpr int PZ = 32 + ((G / SPL) > 1 ? (G / SPL) : 1);     // float plane pitch
+    static constexpr int PXY = comp_pitch_xy(G, SPL);  // float2 plane pitch
+    static constexpr int PZ = comp_pitch_z(G, SPL);    // float plane pitch
     static constexpr int XY_BYTES = SPL * PXY * 8;
     static constexpr int Z_BYTES = SPL * PZ * 4;
     // xy, z planes; rounded to 16 bytes so that every warp's float2 plane (and what follows the
@@ -331,8 +341,7 @@ struct Layout {
 
 constexpr size_t warp_state_bytes(int G, int SPL)
 {
-    return ((size_t)SPL * (32 + ((16 / SPL) > 1 ? (16 / SPL) : 1)) * 8 +
-            (size_t)SPL * (32 + ((G / SPL) > 1 ? (G / SPL) : 1)) * 4 + 15) / 16 * 16;
+    return ((size_t)SPL * comp_pitch_xy(G, SPL) * 8 + (size_t)SPL * comp_pitch_z(G, SPL) * 4 + 15) / 16 * 16;
 }
 
 // Threads per CTA the chain kernel of a shape is compiled for (its register budget: 65536 /
