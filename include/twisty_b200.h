@@ -386,7 +386,8 @@ twisty_status twisty_tuning_cache_load(const char *path);
  * (comp_default_tuning and the placement rule of twisty_run). Host-only: needs no device.
  * For N = 13..24 the shape also depends on the pass: a pass takes the one-lane 1 x 16 (N <= 16)
  * or 1 x 24 only when its paths_to_generate reaches 60000 or 130000 times its paths_to_skip
- * (shorter passes take 4 x 4, 4 x 5 or 4 x 8); this reports the long pass's shape.
+ * (shorter passes take 4 x 4, 4 x 5 or 4 x 8), and 1 x 16 runs 24 warps instead of 16 from
+ * 210000 times; this reports the longest pass's shape.
  * TWISTY_ERR_INVALID_ARGUMENT for a null out, N < 4 or bins < 2; TWISTY_ERR_UNSUPPORTED
  * when no shape covers N (N > 1024). */
 typedef struct twisty_shape {

@@ -33,6 +33,7 @@ CASES = [
     (10, 4, None, (1, 12)),
     (12, 4, None, (1, 12)),
     (16, 4, None, (1, 16)),        # 512000 paths >= 60000 x 4 burn-in steps: one lane
+    (16, 2, None, (1, 16)),        # >= 210000 x 2: one lane at 24 warps
     (16, 16, None, (4, 4)),        # a short pass against its burn-in: 4 lanes
     (20, 2, None, (1, 24)),        # 512000 >= 130000 x 2
     (24, 2, None, (1, 24)),

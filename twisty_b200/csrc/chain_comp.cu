@@ -184,6 +184,9 @@ bool comp_table_needs_clamp(float inv_ds, const LutMetaF &m)
 // the cost per weighted step (both fitted to those runs), so they win once a pass's paths reach
 // about 58000 and 125000 times its burn-in steps per chain; the thresholds below round those up.
 // (At 2^24 paths and 256 burn-in steps: 1 x 16 +5 % at N = 16, 1 x 24 4-10 % slower.)
+// With unpadded one-lane rows (comp_pitch_xy), 1 x 16 at 24 warps carries 1.5x the chains of
+// 16 warps at 0.883 of the cost per step: +9.6 % at N = 16 on passes of 2^32 path-segments,
+// +4 % at 2^26 paths, 7 % slower at 2^24; it takes over at paths >= 210000 x burn-in.
 // 4 x 12, which also turns the shorter side, serves N = 37..48 with less padding than 4 x 16:
 // +16-19 % at N = 37, 40 and +8-13 % at 44, 48, on passes of 2^24 paths and of 2^32
 // path-segments alike (+3-8 % without the shorter side). The batched kernels have neither
@@ -193,9 +196,11 @@ CompTuning comp_default_tuning(uint32_t n, bool batched, uint64_t paths, uint64_
     CompTuning t;
     t.exact_blend = 0;
     const bool lane16 = !batched && paths / 60000u >= burn_in;
+    const bool lane16_24w = !batched && paths / 210000u >= burn_in;
     const bool lane24 = !batched && paths / 130000u >= burn_in;
     if (n <= 8) { t.group = 1; t.spl = 8; t.warps_per_block = 32; }
     else if (n <= 12) { t.group = 1; t.spl = 12; t.warps_per_block = 24; }
+    else if (n <= 16 && lane16_24w) { t.group = 1; t.spl = 16; t.warps_per_block = 24; }
     else if (n <= 16 && lane16) { t.group = 1; t.spl = 16; t.warps_per_block = 16; }
     else if (n <= 16) { t.group = 4; t.spl = 4; t.warps_per_block = 32; }
     else if (n <= 24 && lane24) { t.group = 1; t.spl = 24; t.warps_per_block = 16; }
