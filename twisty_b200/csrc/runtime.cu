@@ -547,6 +547,16 @@ void prepare(twisty_ctx *ctx, const twisty_bc *bcp)
             if (!p.comp_warps) ctx->tuning.warps_per_block = (p.comp_spl >= 12) ? 24 : 32;
         }
         if (p.comp_warps) ctx->tuning.warps_per_block = (int)p.comp_warps;
+        // A pass of fewer chains than a full grid of the shape holds (num_chains set by the
+        // caller) takes fewer warps per CTA, so that its chains spread over every SM: 4096
+        // chains of the 8 x 16 shape would fill 43 CTAs of 24 warps on 43 of 148 SMs, and fill
+        // 147 CTAs of 7 warps instead. Chain ids and proposals do not depend on the layout.
+        if (requested && !p.comp_warps) {
+            const uint64_t chains = std::min<uint64_t>(requested, std::max<uint64_t>(p.paths_to_generate, 1));
+            const uint64_t per_warp_grid = (uint64_t)ctx->sm_count * (32u / (uint32_t)ctx->tuning.group);
+            const uint64_t need = (chains + per_warp_grid - 1) / per_warp_grid;
+            if (need < (uint64_t)ctx->tuning.warps_per_block) ctx->tuning.warps_per_block = (int)std::max<uint64_t>(need, 1);
+        }
         ctx->tuning.exact_blend = ctx->exact_blend;
         if (!comp_tuning_supported(ctx->tuning, N, c.k_eff)) fail(TWISTY_ERR_UNSUPPORTED, "no compensated kernel shape for this N / max_sub_chain");
         // the table's placement (table_through_l1); comp_table_memory 1 / 2 force the choice
