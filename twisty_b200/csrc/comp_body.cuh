@@ -904,8 +904,12 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                     float r = sqrt_approx(qq) + kc.roff;   // scaled tangents: the root is the bin index
                     if (r < 0.f) r = 0.f;
                     if (r > kc.rmax) r = kc.rmax;
-                    const int32_t L = min((int32_t)r, kc.bins - 1);
-                    const float d = (r - (float)L) * kc.step;
+                    // floor(r) by a round-down add, as bin_of takes it (no float/int conversions
+                    // on the MUFU pipe, which the blend's log2 and reciprocal already load;
+                    // measured 1.8 % off the differentiation configuration's adjoint call)
+                    const float fl = __fadd_rd(r, 8388608.0f);
+                    const int32_t L = (int32_t)min(__float_as_uint(fl) - 0x4B000000u, (uint32_t)kc.bins - 1u);
+                    const float d = (r - (fl - 8388608.0f)) * kc.step;
                     const float2 e = s_tab[L];
                     const float4 dv = __ldg(ma.dtab + L);
                     const float v = fmaf(d, e.y, e.x);
