@@ -539,7 +539,8 @@ void prepare(twisty_ctx *ctx, const twisty_bc *bcp)
         max_steps = std::min<uint32_t>(max_steps, 1000000u);
     } else if (p.form == TWISTY_FORM_COMPENSATED) {
         ctx->tuning = comp_default_tuning(N, false, p.paths_to_generate, p.paths_to_skip);
-        if (!p.comp_group && !p.comp_spl && !p.comp_warps) tune_lookup(ctx->device_name, N, p.num_curvature_steps, ctx->tuning);
+        bool default_shape = !p.comp_group && !p.comp_spl && !p.comp_warps;
+        if (default_shape && tune_lookup(ctx->device_name, N, p.num_curvature_steps, ctx->tuning)) default_shape = false;
         if (p.comp_group || p.comp_spl) {
             if (!p.comp_group || !p.comp_spl) fail(TWISTY_ERR_INVALID_CONFIG, "comp_group and comp_spl are set together");
             ctx->tuning.group = (int)p.comp_group;
@@ -551,11 +552,32 @@ void prepare(twisty_ctx *ctx, const twisty_bc *bcp)
         // caller) takes fewer warps per CTA, so that its chains spread over every SM: 4096
         // chains of the 8 x 16 shape would fill 43 CTAs of 24 warps on 43 of 148 SMs, and fill
         // 147 CTAs of 7 warps instead. Chain ids and proposals do not depend on the layout.
+        // When that leaves fewer than 12 warps per CTA, a default shape of 8 or more lanes per
+        // chain doubles its lanes per chain and halves its segments per lane (the same slots)
+        // while the kernels have such a shape: more warps to hide latency with (shapes of 1 and
+        // 4 lanes pack chains into warps on purpose, and keep their shorter-side moves). The differentiation configuration (N = 128,
+        // 4096 chains) takes 16 x 8 at 14 warps over 8 x 16 at 7: forward 2.61 -> 2.20 ms,
+        // adjoint call 6.19 -> 4.57 ms.
         if (requested && !p.comp_warps) {
             const uint64_t chains = std::min<uint64_t>(requested, std::max<uint64_t>(p.paths_to_generate, 1));
-            const uint64_t per_warp_grid = (uint64_t)ctx->sm_count * (32u / (uint32_t)ctx->tuning.group);
-            const uint64_t need = (chains + per_warp_grid - 1) / per_warp_grid;
-            if (need < (uint64_t)ctx->tuning.warps_per_block) ctx->tuning.warps_per_block = (int)std::max<uint64_t>(need, 1);
+            auto need_warps = [&](const CompTuning &t) {
+                const uint64_t per_warp_grid = (uint64_t)ctx->sm_count * (32u / (uint32_t)t.group);
+                return std::max<uint64_t>((chains + per_warp_grid - 1) / per_warp_grid, 1);
+            };
+            uint64_t need = need_warps(ctx->tuning);
+            if (need < (uint64_t)ctx->tuning.warps_per_block) {
+                ctx->tuning.warps_per_block = (int)need;
+                while (default_shape && need < 12 && ctx->tuning.group >= 8 && ctx->tuning.group < 32 &&
+                       ctx->tuning.spl % 2 == 0) {
+                    CompTuning w = ctx->tuning;
+                    w.group *= 2;
+                    w.spl /= 2;
+                    if (!comp_tuning_supported(w, N, c.k_eff)) break;
+                    need = std::min<uint64_t>(need_warps(w), 24);   // 24 warps: within every shape's thread limit
+                    w.warps_per_block = (int)need;
+                    ctx->tuning = w;
+                }
+            }
         }
         ctx->tuning.exact_blend = ctx->exact_blend;
         if (!comp_tuning_supported(ctx->tuning, N, c.k_eff)) fail(TWISTY_ERR_UNSUPPORTED, "no compensated kernel shape for this N / max_sub_chain");
