@@ -900,7 +900,7 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                 // log10 weight and d/d(mu_s), d/d(eps) of this lane's segments (exact blend): the
                 // blend from the staged linear table, the derivative blends from one 16-byte load
                 float s = 0.f, cc = 0.f, gmu = 0.f, geps = 0.f;
-                for_curvatures<G, SPL, false>(j, N, tan_smem, next_smem, [&](uint32_t, float qq, bool valid) {
+                auto adj_seg = [&](uint32_t, float qq, bool valid) {
                     float r = sqrt_approx(qq) + kc.roff;   // scaled tangents: the root is the bin index
                     if (r < 0.f) r = 0.f;
                     if (r > kc.rmax) r = kc.rmax;
@@ -917,7 +917,13 @@ __device__ __forceinline__ double chain_body(const ChainSpec &c, const CompConst
                     const float iv = __fdividef(1.0f, v);
                     gmu += valid ? fmaf(d, dv.y, dv.x) * iv : 0.0f;
                     geps += valid ? fmaf(d, dv.w, dv.z) * iv : 0.0f;
-                });
+                };
+                // a chain that fills its group's slots walks them with validity known at compile
+                // time (every curvature but the group's last boundary), as the forward recompute does
+                if (N == (uint32_t)(G * SPL))
+                    for_curvatures<G, SPL, true>(j, N, tan_smem, next_smem, adj_seg);
+                else
+                    for_curvatures<G, SPL, false>(j, N, tan_smem, next_smem, adj_seg);
                 float hi = s, lo = -cc;
                 group_sum_pair<G>(hi, lo);
                 w = (double)hi + (double)lo;
