@@ -495,12 +495,18 @@ def main():
                     help="precision: one N=256 experiment (the headline); batch: 4096 uneven experiments; "
                          "image: 64x64 receiver grid at N=512 from a multi-arclength table set")
     ap.add_argument("--experiments", type=int, default=0, help="batch workload: number of experiments (default 4096)")
+    ap.add_argument("--image-pixels", type=int, default=0,
+                    help="image workload: pixels per side (default 64; smaller grids for profiling)")
     ap.add_argument("--segments", type=int, default=0,
                     help="precision workload with N segments instead of 256 (per-N figures and profiles; the CPU "
                          "baseline and the reference arm keep N = 256)")
     args = ap.parse_args()
     if args.experiments:
         BATCH["n"] = args.experiments
+    if args.image_pixels:
+        global IMAGE_NAME
+        IMAGE["nx"] = IMAGE["ny"] = args.image_pixels
+        IMAGE_NAME = IMAGE_NAME.replace("64x64", f"{args.image_pixels}x{args.image_pixels}")
     if args.paths and args.workload == "precision":
         W["paths"] = args.paths
     if args.segments and args.impl == "b200":
