@@ -260,7 +260,7 @@ __device__ __forceinline__ double path_log10(uint32_t j, uint32_t N, const float
 {
     unsigned long long isum = 0;
     float csum = 0.f, ks = 0.f, kc = 0.f;
-    for_curvatures<G, SPL, false>(j, N, tan, next, [&](uint32_t i, float qq, bool valid) {
+    auto seg = [&](uint32_t i, float qq, bool valid) {
         int32_t L;
         const float frac = bin_of<CLAMP>(qq, k, valid, clamped, L);
         if (valid) bin_sink(i, isnan(frac) ? -1 : L);
@@ -273,7 +273,12 @@ __device__ __forceinline__ double path_log10(uint32_t j, uint32_t N, const float
             const float c2 = fmaf(frac, e.y, csum);
             csum = valid ? c2 : csum;
         }
-    });
+    };
+    // a chain that fills its group's slots: slot validity known at compile time
+    if (N == (uint32_t)(G * SPL))
+        for_curvatures<G, SPL, true>(j, N, tan, next, seg);
+    else
+        for_curvatures<G, SPL, false>(j, N, tan, next, seg);
     if (EXACT) {
         float hi = ks, lo = -kc;
         group_sum_pair<G>(hi, lo);
