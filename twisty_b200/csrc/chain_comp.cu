@@ -248,8 +248,8 @@ bool comp_tuning_supported(const CompTuning &t, uint32_t n, uint32_t k_eff)
 {
     const int s = t.spl;
     const bool shape = (t.group == 1 && (s == 8 || s == 12 || s == 16 || s == 24)) ||
-                       (t.group == 4 && (s == 2 || s == 3 || s == 4 || s == 5 || s == 8 || s == 9 || s == 12 || s == 16 || s == 17 || s == 20 ||
-                                         s == 24 || s == 28 || s == 32)) ||
+                       (t.group == 4 && (s == 2 || s == 3 || s == 4 || s == 5 || s == 8 || s == 9 || s == 12 || s == 16 ||
+                                         s == 17 || s == 20 || s == 24 || s == 28 || s == 32)) ||
                        (t.group == 8 && (s == 2 || s == 4 || s == 8 || s == 9 || s == 12 || s == 16 || s == 17 || s == 20 ||
                                          s == 24 || s == 32)) ||
                        (t.group == 16 && (s == 4 || s == 8 || s == 12 || s == 16 || s == 17 || s == 20 || s == 24 ||

@@ -328,8 +328,14 @@ __device__ __forceinline__ unsigned long long path_fixed(uint32_t j, uint32_t gb
 // has the lanes at unrelated rows, and an unpadded row of 32 puts lane i in bank (pair) i mod
 // 16 (32) whatever its row, so no access conflicts (the padded pitch measured the one-lane
 // kernel bound by shared-memory wavefronts at 92 % of their peak).
-__host__ __device__ constexpr int comp_pitch_xy(int G, int SPL) { return G == 1 ? 32 : 32 + ((16 / SPL) > 1 ? (16 / SPL) : 1); }
-__host__ __device__ constexpr int comp_pitch_z(int G, int SPL) { return G == 1 ? 32 : 32 + ((G / SPL) > 1 ? (G / SPL) : 1); }
+__host__ __device__ constexpr int comp_pitch_xy(int G, int SPL)
+{
+    return G == 1 ? 32 : 32 + ((16 / SPL) > 1 ? (16 / SPL) : 1);
+}
+__host__ __device__ constexpr int comp_pitch_z(int G, int SPL)
+{
+    return G == 1 ? 32 : 32 + ((G / SPL) > 1 ? (G / SPL) : 1);
+}
 
 template <int G, int SPL>
 struct Layout {

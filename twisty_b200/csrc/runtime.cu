@@ -555,9 +555,9 @@ void prepare(twisty_ctx *ctx, const twisty_bc *bcp)
         // When that leaves fewer than 12 warps per CTA, a default shape of 8 or more lanes per
         // chain doubles its lanes per chain and halves its segments per lane (the same slots)
         // while the kernels have such a shape: more warps to hide latency with (shapes of 1 and
-        // 4 lanes pack chains into warps on purpose, and keep their shorter-side moves). The differentiation configuration (N = 128,
-        // 4096 chains) takes 16 x 8 at 14 warps over 8 x 16 at 7: forward 2.61 -> 2.20 ms,
-        // adjoint call 6.19 -> 4.57 ms.
+        // 4 lanes pack chains into warps on purpose, and keep their shorter-side moves). The
+        // differentiation configuration (N = 128, 4096 chains) takes 16 x 8 at 14 warps over
+        // 8 x 16 at 7: forward 2.61 -> 2.20 ms, adjoint call 6.19 -> 4.57 ms.
         if (requested && !p.comp_warps) {
             const uint64_t chains = std::min<uint64_t>(requested, std::max<uint64_t>(p.paths_to_generate, 1));
             auto need_warps = [&](const CompTuning &t) {
