@@ -84,9 +84,10 @@ def test_explicit_shape_matches_fp64(N, shape):
     assert abs(a.log10_weight - b.log10_weight) < 1.5e-7 * abs(b.log10_weight) + 1e-5, (a.log10_weight, b.log10_weight)
 
 
-@pytest.mark.parametrize("N,angle", [(10, 0.05), (12, 0.05), (24, 0.05), (32, 0.05), (36, 0.05), (24, 0.3), (36, 0.3)])
+@pytest.mark.parametrize("N,angle", [(10, 0.05), (12, 0.05), (24, 0.05), (32, 0.05), (36, 0.05), (48, 0.05), (24, 0.3),
+                                     (36, 0.3), (48, 0.3)])
 def test_long_chains_turning_the_shorter_side_match_fp64(N, angle):
-    """Below N = 37 the forward kernels turn the complement of a sub-chain that is longer than
+    """Below N = 49 the forward kernels turn the complement of a sub-chain that is longer than
     half the path (by -theta about the same chord: the moved path up to one rotation of the
     whole path) and carry the path's end-to-end chord d through those moves, re-summed every
     16 steps. The FP64 form always turns the sub-chain itself. Few chains with many steps each
