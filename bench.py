@@ -167,6 +167,8 @@ TRAFFIC_PER_LAUNCH = 106496
 INCR_RESYNC = 32
 # N of the small-N figures reported beside the headline (same geometry and table, 2^32 / N paths)
 SMALL_N = (12, 16, 24, 32, 48, 64)
+# paths of the export and re-weighing figures (N = 256: 50 MB of positions)
+REWEIGH_PATHS = 1 << 14
 
 
 def batch_experiments(T, n=None, seed=None):
@@ -490,6 +492,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint (precision line: the differentiation form; image workload: its batched adjoint)")
     ap.add_argument("--no-small-n", action="store_true", help="skip the small-N figures")
+    ap.add_argument("--no-reweigh", action="store_true", help="skip the export and re-weighing figures")
     ap.add_argument("--paths", type=int, default=0, help="paths per pass (default 2^26; smaller for profiling)")
     ap.add_argument("--workload", default="precision", choices=["precision", "batch", "image"],
                     help="precision: one N=256 experiment (the headline); batch: 4096 uneven experiments; "
@@ -660,6 +663,33 @@ def main():
                     "d2h_bytes_per_step": ctypes.sizeof(T._abi.Result) * len(bm["exps"])},
             "roofline": batch_roofline(T, device, bm["done"], bm["per_step"]), "gpu_launches_per_step": bm["launches"],
             "failed_paths": sum(r.failed_paths for r in bm["res"]), "clocks": bm["clocks"]}
+
+    if rank == 0 and form == T.FORM_COMPENSATED and not args.no_reweigh:
+        # the export and re-weighing pipeline (the reference's path-batch output and its batch
+        # re-weigher): the workload's first REWEIGH_PATHS weighted paths exported, then weighed
+        # again through the C ABI by both weighers (host positions in, weights out, each call
+        # uploading the positions), end to end on the host clock
+        with T.Context(workload_params(T, form, device=device)) as cx:
+            t0 = time.perf_counter()
+            pos, w_exp, _ = cx.export_paths(bc, None, REWEIGH_PATHS)
+            export_ms = (time.perf_counter() - t0) * 1e3
+            cx.weight_paths(bc, pos[:64], T.FORM_COMPENSATED)   # tables and buffers, outside the timing
+            rw = {}
+            for name, f in (("compensated", T.FORM_COMPENSATED), ("plain_fp32", T.FORM_PLAIN_FP32)):
+                ts = []
+                for _ in range(3):
+                    t0 = time.perf_counter()
+                    wr, vr, _ = cx.weight_paths(bc, pos, f)
+                    ts.append((time.perf_counter() - t0) * 1e3)
+                ok = (vr == 1) & np.isfinite(w_exp)
+                rel = np.abs(wr[ok] - w_exp[ok]) / np.abs(w_exp[ok])
+                rw[name] = {"value": pos.shape[0] * W["N"] / (min(ts) / 1e3), "ms": min(ts),
+                            "median_rel_diff_vs_export": float(np.median(rel)) if rel.size else None}
+        extra["reweigh"] = {"unit": UNIT, "paths": int(pos.shape[0]), "export_ms": export_ms,
+                            "h2d_bytes_per_call": int(pos.nbytes), "d2h_bytes_per_call": int(pos.shape[0] * 9),
+                            **rw, "note": "twisty_export_paths of the workload's first weighted paths, then "
+                                          "twisty_weight_paths on them (host clock, positions uploaded per call); "
+                                          "the weights compared with the export's own"}
 
     if rank == 0 and form == T.FORM_COMPENSATED and not args.no_adjoint:
         # the differentiation form at its own configuration (N = 128, S = 16, receiver (8,0,0)
