@@ -169,6 +169,8 @@ INCR_RESYNC = 32
 SMALL_N = (12, 16, 24, 32, 48, 64)
 # paths of the export and re-weighing figures (N = 256: 50 MB of positions)
 REWEIGH_PATHS = 1 << 14
+# (N, paths) of the M-segment estimator figures (the bootstrapper resolves N - 2 in {64, 256})
+MSEGMENT = ((66, 1 << 24), (258, 1 << 22))
 
 
 def batch_experiments(T, n=None, seed=None):
@@ -493,6 +495,7 @@ def main():
                     help="skip the adjoint (precision line: the differentiation form; image workload: its batched adjoint)")
     ap.add_argument("--no-small-n", action="store_true", help="skip the small-N figures")
     ap.add_argument("--no-reweigh", action="store_true", help="skip the export and re-weighing figures")
+    ap.add_argument("--no-msegment", action="store_true", help="skip the M-segment estimator figures")
     ap.add_argument("--paths", type=int, default=0, help="paths per pass (default 2^26; smaller for profiling)")
     ap.add_argument("--workload", default="precision", choices=["precision", "batch", "image"],
                     help="precision: one N=256 experiment (the headline); batch: 4096 uneven experiments; "
@@ -690,6 +693,25 @@ def main():
                             **rw, "note": "twisty_export_paths of the workload's first weighted paths, then "
                                           "twisty_weight_paths on them (host clock, positions uploaded per call); "
                                           "the weights compared with the export's own"}
+
+    if rank == 0 and form == T.FORM_COMPENSATED and not args.no_msegment:
+        # the independent-sample M-segment estimator on the workload's geometry: every path a
+        # fresh bootstrapped curve, weighed by the compensated weigher (device time of the pass)
+        msr = {}
+        for n_ms, p_ms in MSEGMENT:
+            mp = workload_params(T, form, device=device)
+            mp.num_segments = n_ms
+            mp.paths_to_generate = p_ms
+            with T.Context(mp) as cm:
+                cm.run_msegment(bc)   # tables and buffers
+                rm = cm.run_msegment(bc)
+            msr[str(n_ms)] = {"paths": int(rm.total_paths), "failed_paths": int(rm.failed_paths), "ms": rm.perturb_ms,
+                              "paths_per_s": rm.total_paths / (rm.perturb_ms / 1e3),
+                              "value": rm.total_paths * n_ms / (rm.perturb_ms / 1e3),
+                              "log10_weight": rm.log10_weight, "rel_std_error": rm.rel_std_error}
+        extra["msegment"] = {"unit": UNIT, "per_n": msr,
+                             "note": "twisty_run_msegment: paths generated by the recursive bootstrapper on the device "
+                                     "and weighed in the compensated form; the estimate is the mean weight"}
 
     if rank == 0 and form == T.FORM_COMPENSATED and not args.no_adjoint:
         # the differentiation form at its own configuration (N = 128, S = 16, receiver (8,0,0)
