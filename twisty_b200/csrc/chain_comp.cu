@@ -177,7 +177,7 @@ bool comp_table_needs_clamp(float inv_ds, const LutMetaF &m)
 // segment per lane more than a power of two (3, 5, 9, 17)
 // serve N = 2^k + 2, the N of the reference's own configurations (10, 18, 34, 66, 130, 258,
 // 514), which would otherwise pad to the next power of two.
-// Since chains of up to 36 segments turn the shorter side of each move, one lane per chain
+// Since short chains turn the shorter side of each move (comp_body), one lane per chain
 // also wins at N = 13..24 on long passes: 1 x 16 (N = 13..16) and 1 x 24 (17..24) at 16 warps
 // measured +35-42 % and +15-19 % over 4 x {4, 5, 8} on passes of 2^32 path-segments. They run
 // twice as many chains, each of which pays the burn-in, at 0.72 (1 x 16) and 0.81 (1 x 24) of
