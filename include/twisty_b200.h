@@ -133,8 +133,9 @@ typedef struct twisty_params {
        (an algorithmic shortcut, reported separately; fixed-point tables without clamping) */
     uint32_t incremental_resync;
     /* where the compensated form keeps the weight table (no reference counterpart): 0 = chosen
-       from its size (shared memory when it fits beside a full CTA of chain state, else read
-       through L1), 1 = shared memory (fewer warps per CTA for large tables), 2 = through L1.
+       from its size (shared memory when it fits beside a full CTA of chain state, or beside
+       20 of the 24 warps of the 20- and 24-segment shapes, else read through L1), 1 = shared
+       memory (fewer warps per CTA for large tables), 2 = through L1.
        Path export, the adjoint, receiver-shifted and incremental runs always stage it. */
     uint32_t comp_table_memory;
     /* error against FP64, measured (no reference counterpart): K > 0 replays the pass's first K

@@ -3,8 +3,10 @@ the C ABI. Needs a B200.
 
 The reference's own configurations mostly use 20000-bin tables (160 KB): staged in shared
 memory beside the chain state they would leave a CTA a quarter of its warps, so forward passes
-read them through L1 instead. Both placements run the same arithmetic on the same table
-values, so with the same chain layout their results are identical.
+read them through L1 instead. The 20- and 24-segment shapes, whose 24 warps leave little room
+beside the chain state, stage a table at 20 warps where it fits there (8192 bins in the
+20-segment shapes). Both placements run the same arithmetic on the same table values, so with
+the same chain layout their results are identical.
 """
 import pytest
 
@@ -60,3 +62,24 @@ def test_invalid_table_memory_is_rejected():
         with pytest.raises(T.TwistyError) as ei:
             ctx.run(_bc(64))
     assert ei.value.status == _abi.ERR_INVALID_CONFIG and "comp_table_memory" in str(ei.value)
+
+
+@pytest.mark.parametrize("N,group", [(80, 4), (160, 8), (320, 16), (640, 32)])
+def test_twenty_segment_shapes_stage_8192_bin_tables_at_20_warps(N, group):
+    """An 8192-bin table (64 KB) does not fit beside 24 warps of a 20-segment shape's chain
+    state; the default placement stages it at 20 warps instead of reading it through L1 at 24.
+    Same chains as the L1 placement at 20 warps (identical result) and as the FP64 form."""
+    s = T.default_shape(N, 8192)
+    assert (s["group"], s["spl"], s["warps"], s["table_in_l1"]) == (group, 20, 20, 0), s
+    chains = 148 * 20 * (32 // group)
+    kw = dict(num_chains=chains, paths_to_generate=chains * 40)
+    res = {}
+    for key, extra in (("staged", {}), ("l1", dict(comp_warps=20, comp_table_memory=2)),
+                       ("fp64", dict(form=T.FORM_FP64))):
+        with T.Context(_params(N, 8192, **kw, **extra)) as ctx:
+            res[key] = ctx.run(_bc(N))
+    a, b, c = res["staged"], res["l1"], res["fp64"]
+    assert a.kernel_shape == b.kernel_shape == (group << 8) | 20
+    assert a.total_paths == b.total_paths == c.total_paths == chains * 40 and a.failed_paths == 0
+    assert a.log10_weight == b.log10_weight
+    assert abs(a.log10_weight - c.log10_weight) < 1.5e-7 * abs(c.log10_weight) + 1e-5, (a.log10_weight, c.log10_weight)

@@ -167,8 +167,9 @@ bool comp_table_needs_clamp(float inv_ds, const LutMetaF &m)
 // measured only 2 % above 32 x 16
 // and would drop to 12 warps through L1 for large tables, so 32 x 16 stays. The 24-segment
 // shapes run 24 warps, which leave no room to stage a table: they stage one at 20 warps when
-// that fits (comp_stage_min_warps) and gather it through L1 at 24 otherwise; 16 x 28 likewise
-// stages at 16 and gathers at 20. 32 x 32 stays at 12 warps: 16 warps through L1 measured even
+// that fits (comp_stage_min_warps) and gather it through L1 at 24 otherwise; the 20-segment
+// shapes do the same with tables too large to stage at 24 warps; 16 x 28 stages at 16 and
+// gathers at 20. 32 x 32 stays at 12 warps: 16 warps through L1 measured even
 // with it at N = 1024.
 // Up to N = 32, 4-lane groups put 8 chains in a warp, which share the per-step work of the
 // proposal broadcast, the group reductions and the log-sum-exp (N = 16: +23 %, 32: +12 %
@@ -235,11 +236,14 @@ CompTuning comp_default_tuning(uint32_t n, bool batched, uint64_t paths, uint64_
 // it through L1 at the shape's full warps. The 24-segment shapes at 24 warps have no room for a
 // table; at 20 warps a staged table measured above L1 at 24 (32 x 24: 1-5 % at N = 640, 768;
 // 16 x 24: 3 % at N = 384; 8 x 24: 4 % at N = 192, 4096 bins) and L1 at 24 3-13 % above 16
-// staged warps (32 x 24, N = 600-768, 4096 to 20000 bins). 16 x 28 staged at 16 warps measured
-// 5 % above L1 at 20 (N = 448). Other shapes stage only at full warps.
+// staged warps (32 x 24, N = 600-768, 4096 to 20000 bins). The 20-segment shapes at 24 warps
+// stage tables of up to ~4096 bins; an 8192-bin table staged at 20 warps measured above L1 at 24
+// (8 x 20: 3.0 % at N = 144, 3.9 % at 160; 16 x 20: 1.3 % at 320, 0.1 % at 300; 32 x 20: 0.7 %
+// at 640, 0.0 % at 600; 4 x 20: 0.4 % at 80; passes of 2^32 path-segments). 16 x 28 staged at
+// 16 warps measured 5 % above L1 at 20 (N = 448). Other shapes stage only at full warps.
 int comp_stage_min_warps(const CompTuning &t)
 {
-    if (t.spl == 24 && t.warps_per_block == 24) return 20;
+    if ((t.spl == 24 || t.spl == 20) && t.warps_per_block == 24) return 20;
     if (t.group == 16 && t.spl == 28 && t.warps_per_block == 20) return 16;
     return t.warps_per_block;
 }
